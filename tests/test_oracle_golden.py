@@ -1,0 +1,59 @@
+"""The CPU oracle reproduces the reference's own golden application logs."""
+import json
+import os
+
+import numpy as np
+
+from oracle.oracle import Operator, solve
+from tests.cases import heat_unidirectional, vortex
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_logs.json")))
+
+
+def test_heat_unidirectional_log():
+    """Newton + GMRES(Jacobi) time loop; norms printed to 6 digits must agree exactly."""
+    mesh, T = heat_unidirectional()
+    op = Operator(mesh, "heat", rho_cp=1.0, dt=1e-4, k=1.0)
+    zero = np.zeros(mesh.ndofs)
+    got = []
+    for _ in range(5):
+        T_old = T.copy()
+        for _newton in range(10):  # NewtonRaphsonSolver::solve, newton_raphson_solver.cpp:22-80
+            rhs = np.zeros(mesh.ndofs)
+            op.create_rhs(rhs, T, T_old, zero)
+            d = np.zeros(mesh.ndofs)
+            solve(op, d, rhs, "gmres", inv_diag=op.inverse_diagonal(), rel_tol=1e-12)
+            if np.linalg.norm(rhs) < 5e-9 and np.linalg.norm(d) < 1e-10:
+                break
+            T += d
+        got.append("%.5e" % op.l2_norm(T))
+    assert got == GOLD["heat_unidirectional_2d_q1"]["values"]
+
+
+def _vortex_norms(dim):
+    mesh, phi, mask, vel = vortex(dim)
+    op = Operator(mesh, "advdiff", cmask=mask, dt=0.01, theta=0.5, eps=0.0, vel=vel)
+    nobc = op.with_(cmask=None)
+    out = []
+    for _ in range(5):
+        old = phi.copy()
+        bc = np.where(mask == 1, -1.0, 0.0)  # create_rhs_and_apply_dirichlet_matrixfree
+        rhs = -nobc.vmult(bc)
+        nobc.create_rhs(rhs, old)
+        rhs[mask == 1] = 0.0
+        x = old.copy()
+        solve(op, x, rhs, "gmres", inv_diag=op.inverse_diagonal(), rel_tol=1e-12)
+        x[mask == 1] = -1.0
+        phi = x
+        out.append(op.l2_norm(phi))
+    return np.array(out)
+
+
+def test_vortex_logs():
+    """Reproduced to 7 significant digits (the logs print 11); the remaining 4e-8 relative gap is
+    not a solver effect: a dense direct solve of the same discrete system agrees with GMRES here
+    to 11 digits."""
+    for dim, key in ((3, "advdiff_vortex_mf_3d_q1"), (2, "advdiff_vortex_mf_2d_q1")):
+        ref = np.array([float(v) for v in GOLD[key]["values"]])
+        got = _vortex_norms(dim)
+        assert np.max(np.abs(got - ref) / ref) < 5e-8, (got, ref)

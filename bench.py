@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""Benchmark of the matrix-free heat operator apply (and the CG solves) on B200.
+
+Headline: heat-operator apply throughput in GDoF/s on the "FP64 variable-coefficient heat
+operator at scale" workload: 64^3 hexahedra on the unit cube, FE_Q(4) / QGauss(5), 257^3 =
+16,974,593 DoFs, M/dt + div(k grad) with dt = 1e-3, rho c_p = 1, per-cell k = exp(z),
+z ~ N(0, 0.5^2) (seed 2), homogeneous Dirichlet on all faces, source vector U[-1,1] (seed 1).
+One step = one operator apply (vmult) over that vector.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--no-solve]
+
+Multi-GPU: the apply does not shard in this build (one GPU per problem); N ranks run N
+independent replicas ("replicas only"), value = all DoFs processed / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(workload="heat_apply_q4_64cube_fp64", degree=4, cells=64, dofs=257 ** 3, n_cells=64 ** 3,
+                dt=1e-3, rho_cp=1.0, k="exp(N(0,0.5^2)) per cell, seed 2", src="U[-1,1] seed 1",
+                dirichlet="homogeneous, all faces", quadrature="QGauss(5)")
+METRIC = "heat_op_apply_gdofs"
+UNIT = "GDoF/s"
+# algorithmic bytes per apply: read src (N), write dst (N), read k (N_c), 8 bytes each
+ALGO_BYTES = 8 * (2 * 257 ** 3 + 64 ** 3)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_inputs():
+    from meltpooldg_b200.inputs import normal_cells, uniform_dofs
+    from meltpooldg_b200.operators import Mesh
+
+    mesh = Mesh(4, (64, 64, 64), dirichlet_faces=63)
+    kc = np.exp(normal_cells(mesh, seed=2, sigma=0.5))
+    src = uniform_dofs(mesh, seed=1)
+    return mesh, kc, src
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(WORKLOAD["workload"])
+    except Exception:
+        return None
+
+
+def cpu_baseline(mesh, kc, src, seconds=15.0):
+    """The oracle (CPU restatement of the reference apply) on the same workload, all host threads."""
+    from oracle.oracle import Mesh as OMesh
+    from oracle.oracle import Operator as OOp
+    from oracle.oracle import num_threads
+
+    om = OMesh(4, (64, 64, 64))
+    op = OOp(om, "heat", cmask=om.face_mask(63), rho_cp=1.0, dt=1e-3, k_cell=kc)
+    op.vmult(src)  # warm-up
+    times = []
+    t_end = time.perf_counter() + seconds
+    while time.perf_counter() < t_end or len(times) < 2:
+        t0 = time.perf_counter()
+        op.vmult(src)
+        times.append(time.perf_counter() - t0)
+        if len(times) >= 50:
+            break
+    t = statistics.median(times)
+    return {"value": mesh.ndofs / t / 1e9, "unit": UNIT, "cores": num_threads(), "kind": "port",
+            "sample": f"{len(times)} full applies of the workload (median), oracle C++ restatement, OpenMP"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    from oracle.oracle import Mesh as OMesh
+    from oracle.oracle import Operator as OOp
+    from oracle.oracle import num_threads
+
+    mesh, kc, src = make_inputs()
+    om = OMesh(4, (64, 64, 64))
+    op = OOp(om, "heat", cmask=om.face_mask(63), rho_cp=1.0, dt=1e-3, k_cell=kc)
+    for _ in range(max(args.warmup, 1)):
+        op.vmult(src)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        op.vmult(src)
+    t = (time.perf_counter() - t0) / args.steps
+    val = mesh.ndofs / t / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(WORKLOAD, parallelism="cpu"),
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": num_threads(), "kind": "port",
+                             "sample": f"{args.steps} full applies of the workload, oracle C++ restatement "
+                                       "(the reference needs deal.II, absent on this image)"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_solves(torch, stream):
+    """CG solve time to 1e-8: FP64 Jacobi-CG vs FP32-inner/FP64-outer defect correction on the
+    128^3 FE_Q(2) problem (dt 1e-3, k = exp(N(0,0.5^2)) seed 3, b = U[-1,1] seed 3)."""
+    from meltpooldg_b200.inputs import normal_cells, uniform_dofs
+    from meltpooldg_b200.operators import HeatDiffuseOperator, LinearSolver, LinearSolverData, Mesh
+
+    mesh = Mesh(2, (128, 128, 128), dirichlet_faces=63)
+    kc = np.exp(normal_cells(mesh, seed=3, sigma=0.5))
+    b = uniform_dofs(mesh, seed=3, cmask=mesh_mask(mesh))
+    op = HeatDiffuseOperator(mesh, rho_cp=1.0, dt=1e-3, conductivity_cells=kc, stream=stream.cuda_stream)
+    bd = torch.tensor(b, device="cuda")
+    out = {"workload": "heat_cg_q2_128cube", "dofs": mesh.ndofs, "tol": 1e-8}
+    res = {}
+    for mode in ("fp64", "mixed", "fp64", "mixed"):
+        x = torch.zeros_like(bd)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if mode == "fp64":
+            st = LinearSolver.solve(op, x, bd, LinearSolverData("CG", "Diagonal", rel_tolerance=1e-8))
+            its = st.iterations
+        else:
+            st = LinearSolver.solve_mixed(op, x, bd, outer_rel_tol=1e-8, inner_rel_tol=1e-4)
+            its = st.inner_iterations
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[mode] = (e0.elapsed_time(e1), its, x)
+    # error of both against a tightly converged FP64 solve
+    xr = torch.zeros_like(bd)
+    LinearSolver.solve(op, xr, bd, LinearSolverData("CG", "Diagonal", rel_tolerance=1e-12))
+    nr = torch.linalg.norm(xr).item()
+    for mode in ("fp64", "mixed"):
+        ms, its, x = res[mode]
+        r = torch.empty_like(bd)
+        op.residual(r, bd, x)
+        out[mode] = {"ms": ms, "iterations": its,
+                     "rel_residual": torch.linalg.norm(r).item() / torch.linalg.norm(bd).item(),
+                     "rel_error_vs_fp64_1e-12": torch.linalg.norm(x - xr).item() / nr}
+    out["speedup_mixed_vs_fp64"] = res["fp64"][0] / res["mixed"][0]
+    return out
+
+
+def mesh_mask(mesh):
+    nx, ny, nz = mesh.n
+    m = np.zeros((nz, ny, nx), np.uint8)
+    m[0], m[-1], m[:, 0], m[:, -1], m[:, :, 0], m[:, :, -1] = 1, 1, 1, 1, 1, 1
+    return m.ravel()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    ws, rank, local = dist_env()
+    import torch
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from meltpooldg_b200.build import build
+
+    if rank == 0 or ws == 1:
+        build()
+    if ws > 1:
+        torch.distributed.barrier()
+    from meltpooldg_b200.operators import HeatDiffuseOperator
+
+    mesh, kc, src = make_inputs()
+    stream = torch.cuda.current_stream()
+    op = HeatDiffuseOperator(mesh, rho_cp=1.0, dt=1e-3, conductivity_cells=kc, stream=stream.cuda_stream)
+    x = torch.tensor(src, device="cuda")
+    y = torch.empty_like(x)
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        op.vmult(y, x)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        op.vmult(y, x)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    errs = op.device_errors()
+
+    # end-to-end: host buffers through the C ABI (H2D + apply + D2H inside the timed region)
+    hsrc = torch.tensor(src).pin_memory()
+    hdst = torch.empty_like(hsrc).pin_memory()
+    for _ in range(2):
+        op.vmult_host(hdst.numpy(), hsrc.numpy())
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ke = max(5, args.steps // 5)
+    barrier()
+    torch.cuda.synchronize()
+    e2.record(stream)
+    for _ in range(ke):
+        op.vmult_host(hdst.numpy(), hsrc.numpy())
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3) / ke
+
+    t = torch.tensor([ms, ms_e2e], device="cuda", dtype=torch.float64)
+    if ws > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms, ms_e2e = t.tolist()
+
+    solve = None
+    if not args.no_solve and rank == 0:
+        try:
+            solve = run_solves(torch, stream)
+        except Exception as exc:  # report, never hide
+            solve = {"error": repr(exc)}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+            cpu = cpu_baseline(mesh, kc, src)
+        except Exception as exc:
+            cpu = {"error": repr(exc)}
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        achieved = ALGO_BYTES / (ms * 1e-3) / 1e9
+        traffic = committed_traffic()
+        line = {
+            "metric": METRIC, "value": ws * mesh.ndofs / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(WORKLOAD, parallelism=f"replicas{ws}",
+                           l2="inputs larger than L2: src + dst = 272 MB > 126 MB per step"),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": ALGO_BYTES},
+            "e2e": {"value": ws * mesh.ndofs / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
+                    "h2d_bytes_per_step": 8 * mesh.ndofs, "d2h_bytes_per_step": 8 * mesh.ndofs,
+                    "ms_per_step": ms_e2e},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+            "device_wait_errors": errs,
+            "cpu_baseline": cpu,
+            "solve": solve,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,198 @@
+/*
+ * mpdg_gpu.h -- C ABI of the B200 (sm_100a) matrix-free operator library.
+ *
+ * Drop-in boundary for MeltPoolDG's matrix-free hot path.  Each entry point replaces one member
+ * of the reference interface (paths inside the MeltPoolDG source tree):
+ *
+ *   OperatorMatrixFree<dim,number>            include/meltpooldg/core/operator_base.hpp:189-283
+ *     vmult(dst, src)                         :239-243   -> mpdg_op_vmult / _f32 / _host
+ *     create_rhs(dst, src)                    :208-212   -> mpdg_op_create_rhs
+ *     compute_inverse_diagonal_from_matrixfree(diag) :268-272 -> mpdg_op_compute_inverse_diagonal
+ *   OperatorBase::reset_time_increment(dt)    :41-46     -> mpdg_op_reset_time_increment
+ *   OperatorBase::reset_dof_index(idx)        :31-35     -> mpdg_op_reset_dof_index
+ *   HeatDiffuseMultiPhaseOperator             source/heat/heat_diffuse_operator.cpp:38-80 (ctor)
+ *   AdvectionDiffusionOperator                source/level_set/advection_diffusion_operator.cpp
+ *   LinearSolver::solve                       include/meltpooldg/linear_algebra/linear_solver.hpp:26-134
+ *                                                        -> mpdg_solve
+ *   JacobiPreconditioner                      include/meltpooldg/linear_algebra/preconditioner_jacobi.hpp:25-89
+ *                                                        -> MPDG_PRECOND_JACOBI in mpdg_solve
+ *
+ * Conventions
+ *  - Vectors are in lexicographic lattice order (x fastest) over the (k m + 1)^3 Gauss-Lobatto
+ *    support points of a structured box mesh of axis-aligned hexahedra.  deal.II's DoF numbering
+ *    is mapped onto it once by the caller.
+ *  - Pointers are DEVICE pointers unless the function name ends in _host.
+ *  - vmult zeroes dst; Dirichlet-constrained entries of src are read as 0 and those of dst stay 0
+ *    (deal.II MatrixFree semantics).  create_rhs accumulates into dst, reads its inputs plainly
+ *    and skips constrained rows.  The inverse diagonal has 1 on constrained rows.
+ *  - Every call is stream-ordered on the handle's stream; one host thread per handle.
+ *  - Functions return MPDG_OK (0) or an error code; mpdg_last_error() describes the last error of
+ *    the calling thread.
+ */
+#ifndef MPDG_GPU_H
+#define MPDG_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MPDG_API __attribute__((visibility("default")))
+#else
+#define MPDG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum mpdg_status
+{
+  MPDG_OK                = 0,
+  MPDG_ERR_ARG           = 1, /* invalid argument                                          */
+  MPDG_ERR_CUDA          = 2, /* CUDA runtime error                                        */
+  MPDG_ERR_NOT_CONVERGED = 3, /* SolverControl::NoConvergence (linear_solver.hpp:124-129)   */
+  MPDG_ERR_ZERO_DT       = 4, /* ExcZeroTimeIncrement (include/meltpooldg/core/exceptions.hpp:6) */
+  MPDG_ERR_TIMEOUT       = 5, /* a bounded device-side wait gave up                        */
+  MPDG_ERR_UNSUPPORTED   = 6, /* configuration not provided by this library                */
+  MPDG_ERR_NOMEM         = 7  /* device allocation failed                                  */
+};
+
+enum mpdg_op_kind
+{
+  MPDG_HEAT    = 0, /* (rho c_p/dt) M + div(k grad), source/heat/heat_diffuse_operator.cpp      */
+  MPDG_ADVDIFF = 1  /* M/dt + theta (v.grad + eps K), source/level_set/advection_diffusion_operator.cpp */
+};
+
+enum mpdg_solver_kind
+{
+  MPDG_CG    = 0, /* dealii::SolverCG                          */
+  MPDG_GMRES = 1  /* dealii::SolverGMRES, right preconditioning */
+};
+
+enum mpdg_precond_kind
+{
+  MPDG_PRECOND_IDENTITY = 0,
+  MPDG_PRECOND_JACOBI   = 1
+};
+
+typedef struct mpdg_mesh_desc
+{
+  int32_t        degree;          /* FE_Q degree: heat 1..4, advection-diffusion 1..2 */
+  int32_t        cells[3];        /* cells per direction                                */
+  double         origin[3];       /* lower corner of the box                            */
+  double         length[3];       /* box edge lengths                                   */
+  uint32_t       dirichlet_faces; /* homogeneous Dirichlet on whole faces: bit 2d = low face of
+                                     dim d, bit 2d+1 = high face                         */
+  const uint8_t *dirichlet_mask;  /* optional HOST array of n_dofs flags (nonzero = constrained),
+                                     added to the faces; NULL for none                   */
+} mpdg_mesh_desc;
+
+typedef struct mpdg_op_params
+{
+  int32_t       kind;               /* mpdg_op_kind                                            */
+  int32_t       reserved;
+  /* heat */
+  double        rho_cp;             /* density * specific heat capacity                        */
+  double        dt;                 /* time increment (must be > 0)                            */
+  double        conductivity;       /* k when conductivity_cells == NULL                       */
+  const double *conductivity_cells; /* optional HOST array of n_cells per-cell conductivities
+                                       (lexicographic cells, x fastest)                      */
+  /* advection-diffusion */
+  double        theta;              /* one-step-theta: 1 implicit Euler, 0.5 Crank-Nicolson    */
+  double        diffusivity;        /* eps                                                      */
+  double        velocity[12];       /* affine velocity v(x) = velocity[0..2] + G x with
+                                       G = velocity[3..11] row-major                          */
+} mpdg_op_params;
+
+typedef struct mpdg_solver_params
+{
+  int32_t solver;   /* mpdg_solver_kind                                           */
+  int32_t precond;  /* mpdg_precond_kind                                          */
+  int32_t max_it;   /* ReductionControl max_steps (LinearSolverData default 10000) */
+  int32_t restart;  /* GMRES basis size (default 30)                               */
+  double  abs_tol;  /* ReductionControl tolerance (default 1e-20)                  */
+  double  rel_tol;  /* ReductionControl reduction (default 1e-12)                  */
+} mpdg_solver_params;
+
+typedef struct mpdg_solve_info
+{
+  int32_t iterations;       /* SolverControl::last_step()                               */
+  int32_t status;           /* MPDG_OK or MPDG_ERR_NOT_CONVERGED                        */
+  double  initial_residual; /* |b - A x0|                                                */
+  double  final_residual;   /* last checked residual                                     */
+  double *history;          /* optional HOST buffer for residuals 0..iterations (may be NULL) */
+  int32_t history_capacity; /* entries available in history                              */
+  int32_t inner_iterations; /* mixed precision: total inner FP32 iterations              */
+} mpdg_solve_info;
+
+typedef struct mpdg_mixed_params
+{
+  double  outer_rel_tol;   /* FP64 defect correction: |b - A x| <= outer_rel_tol |b|     */
+  double  inner_rel_tol;   /* FP32 Jacobi-CG (or GMRES) reduction per outer step           */
+  int32_t max_outer;
+  int32_t max_inner;
+  int32_t solver;          /* mpdg_solver_kind of the inner solver                         */
+  int32_t restart;         /* inner GMRES basis size                                       */
+} mpdg_mixed_params;
+
+typedef struct mpdg_op mpdg_op;
+
+/* Operator lifetime -- HeatDiffuseMultiPhaseOperator / AdvectionDiffusionOperator constructors */
+MPDG_API int     mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op **out);
+MPDG_API int     mpdg_op_destroy(mpdg_op *op);
+MPDG_API int64_t mpdg_op_n_dofs(const mpdg_op *op);
+MPDG_API int64_t mpdg_op_n_cells(const mpdg_op *op);
+MPDG_API int     mpdg_op_set_stream(mpdg_op *op, void *cuda_stream);
+
+/* OperatorBase::reset_time_increment (operator_base.hpp:41-46); dt <= 0 -> MPDG_ERR_ZERO_DT */
+MPDG_API int mpdg_op_reset_time_increment(mpdg_op *op, double dt);
+/* OperatorBase::reset_dof_index (operator_base.hpp:31-35): 1 = with Dirichlet constraints
+   (dof_idx, default), 0 = without (dof_no_bc_idx, used by the Dirichlet lifting of
+   include/meltpooldg/linear_algebra/utilities_matrixfree.hpp:33-100) */
+MPDG_API int mpdg_op_reset_dof_index(mpdg_op *op, int with_dirichlet);
+/* replace the per-cell conductivity (heat); k_cells has n_cells entries (device pointer) */
+MPDG_API int mpdg_op_set_conductivity(mpdg_op *op, const double *k_cells);
+
+/* OperatorMatrixFree::vmult (operator_base.hpp:239-243): dst = A src (FP64 / FP32) */
+MPDG_API int mpdg_op_vmult(mpdg_op *op, double *dst, const double *src);
+MPDG_API int mpdg_op_vmult_f32(mpdg_op *op, float *dst, const float *src);
+/* vmult with host buffers: host->device copy, apply, device->host copy (end-to-end call) */
+MPDG_API int mpdg_op_vmult_host(mpdg_op *op, double *dst_host, const double *src_host);
+/* dst += scale A src (no zeroing) */
+MPDG_API int mpdg_op_vmult_add(mpdg_op *op, double *dst, const double *src, double scale);
+/* r = b - A x */
+MPDG_API int mpdg_op_residual(mpdg_op *op, double *r, const double *b, const double *x);
+
+/* OperatorMatrixFree::compute_inverse_diagonal_from_matrixfree (operator_base.hpp:268-272) */
+MPDG_API int mpdg_op_compute_inverse_diagonal(mpdg_op *op, double *diag);
+MPDG_API int mpdg_op_compute_inverse_diagonal_f32(mpdg_op *op, float *diag);
+
+/* OperatorMatrixFree::create_rhs (operator_base.hpp:208-212), accumulating into dst.
+   heat (heat_diffuse_operator.cpp:393-529, 783-806):
+     dst += -[(rho c_p/dt)(T - T_old) - q] phi - k grad T . grad phi    (a = T, b = T_old, c = q)
+   advection-diffusion (advection_diffusion_operator.cpp:274-358):
+     dst += (u_old/dt - (1-theta) v.grad u_old) phi - (1-theta) eps grad u_old . grad phi (a = u_old) */
+MPDG_API int mpdg_op_create_rhs(mpdg_op *op, double *dst, const double *a, const double *b, const double *c);
+
+/* LinearSolver::solve (linear_solver.hpp:26-134) on the operator: FP64, device x (initial guess
+   in, solution out) and b.  Returns MPDG_ERR_NOT_CONVERGED like SolverControl::NoConvergence. */
+MPDG_API int mpdg_solve(mpdg_op *op, double *x, const double *b, const mpdg_solver_params *params, mpdg_solve_info *info);
+/* The same solve entirely in FP32 (operator, vectors; dot products accumulated in FP64) */
+MPDG_API int mpdg_solve_f32(mpdg_op *op, float *x, const float *b, const mpdg_solver_params *params, mpdg_solve_info *info);
+
+/* FP32-inner / FP64-outer defect correction (no reference counterpart: the reference instantiates
+   double only, heat_diffuse_operator.cpp:1214-1216).  Outer: r = b - A64 x in FP64, stop when
+   |r| <= outer_rel_tol |b|; inner: FP32 operator and vectors with Jacobi preconditioning solve
+   A32 e = r to inner_rel_tol; x += e in FP64. */
+MPDG_API int mpdg_solve_mixed(mpdg_op *op, double *x, const double *b, const mpdg_mixed_params *params, mpdg_solve_info *info);
+
+/* Number of error words raised by bounded device waits since the last call (and reset). */
+MPDG_API int mpdg_op_device_errors(mpdg_op *op);
+
+/* Description of the last error on the calling thread. */
+MPDG_API const char *mpdg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPDG_GPU_H */

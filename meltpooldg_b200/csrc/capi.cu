@@ -1,0 +1,896 @@
+// C ABI (include/mpdg_gpu.h) and the host-side solver loops.
+//
+// The solver loops restate the algorithms the reference calls through
+// include/meltpooldg/linear_algebra/linear_solver.hpp:26-134:
+//   * dealii::SolverCG with the Jacobi preconditioner (preconditioner_jacobi.hpp:51-69) and
+//     ReductionControl(max_it, abs_tol, rel_tol): the scalar recurrences run on the device
+//     (CGState, vec.cu) so the host enqueues batches of iterations and only polls the state;
+//   * dealii::SolverGMRES with right preconditioning (linear_solver.hpp:112-118), classical
+//     Gram-Schmidt with one fused dot pass and one fused update pass per iteration, Givens
+//     rotations and the least-squares update on the host in FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/mpdg_gpu.h"
+#include "kernels.h"
+
+using namespace mpdg;
+
+namespace
+{
+  thread_local std::string g_last_error = "no error";
+
+  int
+  fail(int code, const std::string &msg)
+  {
+    g_last_error = msg;
+    return code;
+  }
+
+  int
+  cuda_fail(cudaError_t e, const char *where)
+  {
+    return fail(MPDG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+  }
+
+#define MPDG_CUDA(...)                                                                                         \
+  do                                                                                                           \
+    {                                                                                                          \
+      cudaError_t e__ = (__VA_ARGS__);                                                                         \
+      if (e__ != cudaSuccess)                                                                                  \
+        return cuda_fail(e__, #__VA_ARGS__);                                                                   \
+    }                                                                                                          \
+  while (0)
+
+  // host-side ReductionControl (GMRES)
+  struct Control
+  {
+    int    max_it;
+    double abs_tol, rel_tol, reduced = 0.0;
+    int
+    check(int step, double v)
+    {
+      if (step == 0)
+        reduced = v * rel_tol;
+      if (v <= reduced)
+        return 1;
+      if (v <= abs_tol)
+        return 1;
+      if (step >= max_it || std::isnan(v))
+        return 2;
+      return 0;
+    }
+  };
+} // namespace
+
+struct mpdg_op
+{
+  int       kind   = MPDG_HEAT;
+  int       degree = 2;
+  int       m[3]{};
+  double    origin[3]{}, length[3]{}, h[3]{};
+  uint32_t  faces  = 0;
+  uint8_t  *d_mask = nullptr;
+  bool      with_bc = true;
+  double    rho_cp = 1.0, dt = 1.0, k = 1.0;
+  double   *d_k64 = nullptr;
+  float    *d_k32 = nullptr;
+  double    theta = 1.0, eps = 0.0, vel[12]{};
+  int       brick[3]{}, nbr[3]{};
+  long long ndofs = 0, ncells = 0;
+  unsigned *d_sync = nullptr; // [0] ticket, [1] done, [2] reducer counter, [3..] flags
+  int      *d_err  = nullptr;
+  unsigned  epoch  = 0;
+  double   *d_red  = nullptr; // reducer partials
+  double   *d_scal = nullptr; // 64 scalars
+  CGState  *d_cg   = nullptr;
+  CGState  *h_cg   = nullptr; // pinned mirror
+  double   *h_scal = nullptr; // pinned scalars
+  cudaStream_t stream = nullptr;
+  std::map<std::string, std::pair<void *, size_t>> ws;
+
+  GridDesc
+  grid() const
+  {
+    GridDesc g;
+    for (int d = 0; d < 3; ++d)
+      {
+        g.m[d]   = m[d];
+        g.nbr[d] = nbr[d];
+        g.n[d]   = degree * m[d] + 1;
+      }
+    g.faces = with_bc ? faces : 0u;
+    g.cmask = with_bc ? d_mask : nullptr;
+    return g;
+  }
+  SyncDesc
+  sync()
+  {
+    if (++epoch == 0)
+      ++epoch;
+    SyncDesc s;
+    s.ticket = d_sync;
+    s.done   = d_sync + 1;
+    s.flags  = d_sync + 3;
+    s.epoch  = epoch;
+    s.error  = d_err;
+    return s;
+  }
+  Reducer
+  reducer() const
+  {
+    return Reducer{d_red, d_sync + 2};
+  }
+  template <typename T>
+  T *
+  vec(const std::string &name, size_t count = 0)
+  {
+    const size_t bytes = sizeof(T) * (count ? count : (size_t)ndofs);
+    auto         it    = ws.find(name);
+    if (it != ws.end() && it->second.second >= bytes)
+      return static_cast<T *>(it->second.first);
+    if (it != ws.end())
+      {
+        cudaFree(it->second.first);
+        ws.erase(it);
+      }
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess)
+      return nullptr;
+    ws[name] = {p, bytes};
+    return static_cast<T *>(p);
+  }
+  template <typename T>
+  const T *
+  kcell() const;
+};
+
+template <>
+const double *
+mpdg_op::kcell<double>() const
+{
+  return d_k64;
+}
+template <>
+const float *
+mpdg_op::kcell<float>() const
+{
+  return d_k32;
+}
+
+namespace
+{
+  HeatGeom
+  heat_geom(const mpdg_op *op, double mass_scale)
+  {
+    HeatGeom g;
+    g.mass_coef = mass_scale * op->h[0] * op->h[1] * op->h[2];
+    g.cx        = op->h[1] * op->h[2] / op->h[0];
+    g.cy        = op->h[0] * op->h[2] / op->h[1];
+    g.cz        = op->h[0] * op->h[1] / op->h[2];
+    return g;
+  }
+
+  AdvParams
+  adv_params(const mpdg_op *op, double theta_override, bool use_override)
+  {
+    AdvParams p;
+    const double th = use_override ? theta_override : op->theta;
+    p.inv_dt        = 1.0 / op->dt;
+    p.theta_adv     = th;
+    p.theta_dif     = th * op->eps;
+    for (int i = 0; i < 12; ++i)
+      p.vel[i] = op->vel[i];
+    for (int d = 0; d < 3; ++d)
+      {
+        p.origin[d] = op->origin[d];
+        p.h[d]      = op->h[d];
+      }
+    return p;
+  }
+
+  // Generic apply.  mode: OutMode; 'which' selects the physics variant:
+  //   0 tangent, 1 mass only (heat, coefficient mass_scale), 2 stiffness only (heat, scale on k),
+  //   3 advection with theta replaced by theta - 1 (create_rhs)
+  template <typename T>
+  int
+  apply(mpdg_op *op, int mode, double scale, T *dst, const T *src, const T *b, int mask_src, int which = 0,
+        const int *skip = nullptr)
+  {
+    if (op->kind == MPDG_HEAT)
+      {
+        HeatLaunch<T> h;
+        h.degree = op->degree;
+        h.mode   = mode;
+        h.scale  = scale;
+        h.geo    = heat_geom(op, which == 2 ? 0.0 : (which == 1 ? 1.0 : op->rho_cp / op->dt));
+        h.grid   = op->grid();
+        h.sync   = op->sync();
+        h.kconst = which == 1 ? 0.0 : op->k;
+        h.kcell  = which == 1 ? nullptr : op->kcell<T>();
+        h.src    = src;
+        h.dst    = dst;
+        h.b      = b;
+        h.mask_src = mask_src;
+        h.skip     = skip;
+        MPDG_CUDA(heat_apply<T>(h, op->stream));
+      }
+    else
+      {
+        AdvLaunch<T> h;
+        h.degree   = op->degree;
+        h.mode     = mode;
+        h.scale    = scale;
+        h.p        = adv_params(op, op->theta - 1.0, which == 3);
+        h.grid     = op->grid();
+        h.sync     = op->sync();
+        h.src      = src;
+        h.dst      = dst;
+        h.b        = b;
+        h.mask_src = mask_src;
+        h.skip     = skip;
+        MPDG_CUDA(adv_apply<T>(h, op->stream));
+      }
+    return MPDG_OK;
+  }
+
+  template <typename T>
+  int
+  inverse_diagonal(mpdg_op *op, T *diag)
+  {
+    const GridDesc g = op->grid();
+    if (op->kind == MPDG_HEAT)
+      {
+        MPDG_CUDA(heat_diagonal<T>(g, op->degree, heat_geom(op, op->rho_cp / op->dt), op->k, op->kcell<T>(), diag,
+                                   true, 1.0e-10, op->stream));
+      }
+    else
+      {
+        const int n3  = (op->degree + 1) * (op->degree + 1) * (op->degree + 1);
+        T        *buf = op->vec<T>(sizeof(T) == 8 ? "celldiag64" : "celldiag32", (size_t)op->ncells * n3);
+        if (!buf)
+          return fail(MPDG_ERR_NOMEM, "cell diagonal buffer");
+        MPDG_CUDA(adv_diagonal<T>(g, op->degree, adv_params(op, 0, false), diag, buf, op->stream));
+        MPDG_CUDA(vec_absmax<T>(diag, op->ndofs, op->d_scal, op->reducer(), op->stream));
+        MPDG_CUDA(vec_invert_rel<T>(diag, op->d_scal, op->ndofs, op->stream));
+      }
+    return MPDG_OK;
+  }
+
+  int
+  check_op(const mpdg_op *op)
+  {
+    if (!op)
+      return fail(MPDG_ERR_ARG, "null operator handle");
+    return MPDG_OK;
+  }
+
+  // ---------------------------------------------------------------------------------------------
+  // Preconditioned CG (dealii::SolverCG semantics), all scalars on the device.
+  template <typename T>
+  int
+  cg_solve(mpdg_op *op, T *x, const T *b, const T *invd, int max_it, double abs_tol, double rel_tol,
+           mpdg_solve_info *info, const char *tag)
+  {
+    const long long n = op->ndofs;
+    const std::string t(tag);
+    T *r = op->vec<T>(t + "r"), *p = op->vec<T>(t + "p"), *v = op->vec<T>(t + "v");
+    if (!r || !p || !v)
+      return fail(MPDG_ERR_NOMEM, "CG work vectors");
+    double *hist = op->vec<double>(t + "hist", (size_t)max_it + 2);
+    if (!hist)
+      return fail(MPDG_ERR_NOMEM, "CG history");
+    CGState st{};
+    st.abs_tol = abs_tol;
+    st.rel_tol = rel_tol;
+    st.max_it  = max_it;
+    *op->h_cg  = st;
+    MPDG_CUDA(cudaMemcpyAsync(op->d_cg, op->h_cg, sizeof(CGState), cudaMemcpyHostToDevice, op->stream));
+    // r = b - A x
+    if (int e = apply<T>(op, (int)OutMode::BPlus, -1.0, r, x, b, 1))
+      return e;
+    MPDG_CUDA(cg_init<T>(r, invd, p, op->d_cg, hist, op->reducer(), n, op->stream));
+    int batch = 4;
+    for (;;)
+      {
+        for (int k = 0; k < batch; ++k)
+          {
+            MPDG_CUDA(cg_update_p<T>(r, invd, p, op->d_cg, n, op->stream));
+            if (int e = apply<T>(op, (int)OutMode::Set, 1.0, v, p, nullptr, 1, 0, &op->d_cg->done))
+              return e;
+            MPDG_CUDA(cg_alpha<T>(p, v, op->d_cg, op->reducer(), n, op->stream));
+            MPDG_CUDA(cg_update_xr<T>(x, r, p, v, invd, op->d_cg, hist, op->reducer(), n, op->stream));
+          }
+        MPDG_CUDA(cudaMemcpyAsync(op->h_cg, op->d_cg, sizeof(CGState), cudaMemcpyDeviceToHost, op->stream));
+        MPDG_CUDA(cudaStreamSynchronize(op->stream));
+        if (op->h_cg->done)
+          break;
+        batch = std::min(batch * 2, 64);
+      }
+    const CGState &f = *op->h_cg;
+    if (info)
+      {
+        info->iterations       = f.it;
+        info->status           = f.done == 1 ? MPDG_OK : MPDG_ERR_NOT_CONVERGED;
+        info->initial_residual = f.res0;
+        info->final_residual   = f.res;
+        if (info->history && info->history_capacity > 0)
+          {
+            const int cnt = std::min(info->history_capacity, f.it + 1);
+            MPDG_CUDA(cudaMemcpy(info->history, hist, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+          }
+      }
+    int dev_err = 0;
+    MPDG_CUDA(cudaMemcpy(&dev_err, op->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (dev_err)
+      return fail(MPDG_ERR_TIMEOUT, "a bounded device wait gave up during the CG solve");
+    if (f.done != 1)
+      return fail(MPDG_ERR_NOT_CONVERGED, "CG did not converge in " + std::to_string(f.it) + " iterations");
+    return MPDG_OK;
+  }
+
+  // ---------------------------------------------------------------------------------------------
+  // Right-preconditioned restarted GMRES (dealii::SolverGMRES with right_preconditioning = true).
+  template <typename T>
+  int
+  gmres_solve(mpdg_op *op, T *x, const T *b, const T *invd, int max_it, double abs_tol, double rel_tol, int restart,
+              mpdg_solve_info *info, const char *tag)
+  {
+    const long long   n = op->ndofs;
+    const std::string t(tag);
+    const int         m = std::max(1, std::min(restart, 31));
+    std::vector<T *>  V(m + 1);
+    for (int i = 0; i <= m; ++i)
+      {
+        V[i] = op->vec<T>(t + "V" + std::to_string(i));
+        if (!V[i])
+          return fail(MPDG_ERR_NOMEM, "GMRES basis");
+      }
+    T *z = op->vec<T>(t + "z");
+    if (!z)
+      return fail(MPDG_ERR_NOMEM, "GMRES work vector");
+    double             *d_h = op->d_scal; // [0..m+1]
+    std::vector<double> H((m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), y(m);
+    std::vector<double> hist;
+    Control             ctl{max_it, abs_tol, rel_tol};
+    int                 it = 0, state = 0;
+    double              res0 = 0.0, res = 0.0;
+    bool                first = true;
+    const Reducer       red   = op->reducer();
+    auto fetch = [&](int cnt) -> int {
+      MPDG_CUDA(cudaMemcpyAsync(op->h_scal, d_h, sizeof(double) * cnt, cudaMemcpyDeviceToHost, op->stream));
+      MPDG_CUDA(cudaStreamSynchronize(op->stream));
+      return MPDG_OK;
+    };
+    for (;;)
+      {
+        if (int e = apply<T>(op, (int)OutMode::BPlus, -1.0, V[0], x, b, 1))
+          return e;
+        const T *v0 = V[0];
+        MPDG_CUDA(vec_multidot<T>(&v0, &v0, 1, n, d_h, red, op->stream));
+        if (int e = fetch(1))
+          return e;
+        const double beta = std::sqrt(op->h_scal[0]);
+        if (first)
+          {
+            res0  = beta;
+            first = false;
+            hist.push_back(beta);
+          }
+        res   = beta;
+        state = ctl.check(it, beta);
+        if (state != 0)
+          break;
+        MPDG_CUDA(vec_axpby<T>(V[0], 1.0 / beta, V[0], 0.0, nullptr, n, op->stream));
+        std::fill(g.begin(), g.end(), 0.0);
+        std::fill(H.begin(), H.end(), 0.0);
+        g[0]  = beta;
+        int j = 0;
+        for (; j < m; ++j)
+          {
+            ++it;
+            const T *zin = V[j];
+            if (invd)
+              {
+                MPDG_CUDA(vec_scale<T>(z, V[j], invd, n, op->stream));
+                zin = z;
+              }
+            if (int e = apply<T>(op, (int)OutMode::Set, 1.0, V[j + 1], zin, nullptr, 1))
+              return e;
+            std::vector<const T *> Vc(V.begin(), V.begin() + j + 1);
+            MPDG_CUDA(vec_dots_against<T>(V[j + 1], Vc.data(), j + 1, n, d_h, red, op->stream));
+            MPDG_CUDA(vec_orth_update<T>(V[j + 1], Vc.data(), d_h, j + 1, n, d_h + j + 1, red, op->stream));
+            if (int e = fetch(j + 2))
+              return e;
+            const double hn = std::sqrt(std::max(0.0, op->h_scal[j + 1]));
+            for (int i = 0; i <= j; ++i)
+              H[i * m + j] = op->h_scal[i];
+            H[(j + 1) * m + j] = hn;
+            if (hn > 0.0)
+              MPDG_CUDA(vec_axpby<T>(V[j + 1], 1.0 / hn, V[j + 1], 0.0, nullptr, n, op->stream));
+            for (int i = 0; i < j; ++i)
+              {
+                const double t0 = H[i * m + j], t1 = H[(i + 1) * m + j];
+                H[i * m + j]       = cs[i] * t0 + sn[i] * t1;
+                H[(i + 1) * m + j] = -sn[i] * t0 + cs[i] * t1;
+              }
+            const double a = H[j * m + j], c = H[(j + 1) * m + j];
+            const double r = std::hypot(a, c);
+            cs[j]          = a / r;
+            sn[j]          = c / r;
+            H[j * m + j]       = r;
+            H[(j + 1) * m + j] = 0.0;
+            g[j + 1]           = -sn[j] * g[j];
+            g[j]               = cs[j] * g[j];
+            res                = std::abs(g[j + 1]);
+            hist.push_back(res);
+            state = ctl.check(it, res);
+            if (state != 0 || hn == 0.0)
+              {
+                ++j;
+                break;
+              }
+          }
+        for (int i = j - 1; i >= 0; --i)
+          {
+            double s = g[i];
+            for (int kk = i + 1; kk < j; ++kk)
+              s -= H[i * m + kk] * y[kk];
+            y[i] = s / H[i * m + i];
+          }
+        std::memcpy(op->h_scal, y.data(), sizeof(double) * j);
+        MPDG_CUDA(cudaMemcpyAsync(d_h, op->h_scal, sizeof(double) * j, cudaMemcpyHostToDevice, op->stream));
+        MPDG_CUDA(vec_fill<T>(z, T(0), n, op->stream));
+        std::vector<const T *> Vc(V.begin(), V.begin() + j);
+        MPDG_CUDA(vec_multiaxpy<T>(z, Vc.data(), d_h, j, n, 1.0, op->stream));
+        if (invd)
+          MPDG_CUDA(vec_scale<T>(z, z, invd, n, op->stream));
+        MPDG_CUDA(vec_axpby<T>(x, 1.0, x, 1.0, z, n, op->stream));
+        MPDG_CUDA(cudaStreamSynchronize(op->stream));
+        if (state != 0)
+          break;
+      }
+    if (info)
+      {
+        info->iterations       = it;
+        info->status           = state == 1 ? MPDG_OK : MPDG_ERR_NOT_CONVERGED;
+        info->initial_residual = res0;
+        info->final_residual   = res;
+        if (info->history && info->history_capacity > 0)
+          {
+            const int cnt = std::min<int>(info->history_capacity, (int)hist.size());
+            std::memcpy(info->history, hist.data(), sizeof(double) * cnt);
+          }
+      }
+    if (state != 1)
+      return fail(MPDG_ERR_NOT_CONVERGED, "GMRES did not converge in " + std::to_string(it) + " iterations");
+    return MPDG_OK;
+  }
+
+  template <typename T>
+  int
+  solve_typed(mpdg_op *op, T *x, const T *b, const mpdg_solver_params *prm, mpdg_solve_info *info, const char *tag)
+  {
+    if (!prm || !x || !b)
+      return fail(MPDG_ERR_ARG, "null argument to solve");
+    T *invd = nullptr;
+    if (prm->precond == MPDG_PRECOND_JACOBI)
+      {
+        invd = op->vec<T>(std::string(tag) + "invd");
+        if (!invd)
+          return fail(MPDG_ERR_NOMEM, "inverse diagonal");
+        // JacobiPreconditioner::update (preconditioner_jacobi.hpp:65-69) once per solve
+        if (int e = inverse_diagonal<T>(op, invd))
+          return e;
+      }
+    const int max_it = prm->max_it > 0 ? prm->max_it : 10000;
+    if (prm->solver == MPDG_CG)
+      return cg_solve<T>(op, x, b, invd, max_it, prm->abs_tol, prm->rel_tol, info, tag);
+    if (prm->solver == MPDG_GMRES)
+      return gmres_solve<T>(op, x, b, invd, max_it, prm->abs_tol, prm->rel_tol, prm->restart > 0 ? prm->restart : 30,
+                            info, tag);
+    return fail(MPDG_ERR_ARG, "unknown solver kind");
+  }
+} // namespace
+
+extern "C" {
+
+const char *
+mpdg_last_error(void)
+{
+  return g_last_error.c_str();
+}
+
+int
+mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op **out)
+{
+  if (!mesh || !params || !out)
+    return fail(MPDG_ERR_ARG, "null argument to mpdg_op_create");
+  *out = nullptr;
+  if (params->kind != MPDG_HEAT && params->kind != MPDG_ADVDIFF)
+    return fail(MPDG_ERR_ARG, "unknown operator kind");
+  if (params->kind == MPDG_HEAT && (mesh->degree < 1 || mesh->degree > 4))
+    return fail(MPDG_ERR_UNSUPPORTED, "heat operator: FE_Q degree must be 1..4");
+  if (params->kind == MPDG_ADVDIFF && (mesh->degree < 1 || mesh->degree > 2))
+    return fail(MPDG_ERR_UNSUPPORTED, "advection-diffusion operator: FE_Q degree must be 1..2");
+  for (int d = 0; d < 3; ++d)
+    if (mesh->cells[d] < 1 || !(mesh->length[d] > 0.0))
+      return fail(MPDG_ERR_ARG, "mesh cells and lengths must be positive");
+  if (!(params->dt > 0.0))
+    return fail(MPDG_ERR_ZERO_DT, "time increment must be positive (ExcZeroTimeIncrement)");
+  const long long n0 = (long long)mesh->degree * mesh->cells[0] + 1, n1 = (long long)mesh->degree * mesh->cells[1] + 1,
+                  n2 = (long long)mesh->degree * mesh->cells[2] + 1;
+  // lattice indices are 32-bit in the kernels
+  if (n0 * n1 * n2 >= (1LL << 31))
+    return fail(MPDG_ERR_UNSUPPORTED, "an operator holds fewer than 2^31 DoFs");
+
+  mpdg_op *op = new mpdg_op();
+  op->kind    = params->kind;
+  op->degree  = mesh->degree;
+  for (int d = 0; d < 3; ++d)
+    {
+      op->m[d]      = mesh->cells[d];
+      op->origin[d] = mesh->origin[d];
+      op->length[d] = mesh->length[d];
+      op->h[d]      = mesh->length[d] / mesh->cells[d];
+    }
+  op->faces  = mesh->dirichlet_faces & 63u;
+  op->rho_cp = params->rho_cp;
+  op->dt     = params->dt;
+  op->k      = params->conductivity;
+  op->theta  = params->theta;
+  op->eps    = params->diffusivity;
+  for (int i = 0; i < 12; ++i)
+    op->vel[i] = params->velocity[i];
+  if (op->kind == MPDG_HEAT)
+    heat_brick_shape<double>(op->degree, op->brick);
+  else
+    adv_brick_shape<double>(op->degree, op->brick);
+  for (int d = 0; d < 3; ++d)
+    op->nbr[d] = (op->m[d] + op->brick[d] - 1) / op->brick[d];
+  op->ndofs             = n0 * n1 * n2;
+  op->ncells            = (long long)op->m[0] * op->m[1] * op->m[2];
+  const long long nbrk  = (long long)op->nbr[0] * op->nbr[1] * op->nbr[2];
+  auto            clean = [&](int code, const std::string &msg) {
+    mpdg_op_destroy(op);
+    return fail(code, msg);
+  };
+  if (cudaMalloc(&op->d_sync, sizeof(unsigned) * (3 + nbrk)) != cudaSuccess ||
+      cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&op->d_red, sizeof(double) * RED_BLOCKS * 40) != cudaSuccess ||
+      cudaMalloc(&op->d_scal, sizeof(double) * 64) != cudaSuccess ||
+      cudaMalloc(&op->d_cg, sizeof(CGState)) != cudaSuccess ||
+      cudaMallocHost(&op->h_cg, sizeof(CGState)) != cudaSuccess ||
+      cudaMallocHost(&op->h_scal, sizeof(double) * 64) != cudaSuccess)
+    return clean(MPDG_ERR_NOMEM, "device allocation in mpdg_op_create");
+  if (cudaMemset(op->d_sync, 0, sizeof(unsigned) * (3 + nbrk)) != cudaSuccess ||
+      cudaMemset(op->d_err, 0, sizeof(int)) != cudaSuccess)
+    return clean(MPDG_ERR_CUDA, "cudaMemset in mpdg_op_create");
+  if (mesh->dirichlet_mask)
+    {
+      if (cudaMalloc(&op->d_mask, op->ndofs) != cudaSuccess)
+        return clean(MPDG_ERR_NOMEM, "Dirichlet mask");
+      if (cudaMemcpy(op->d_mask, mesh->dirichlet_mask, op->ndofs, cudaMemcpyHostToDevice) != cudaSuccess)
+        return clean(MPDG_ERR_CUDA, "Dirichlet mask copy");
+    }
+  if (op->kind == MPDG_HEAT && params->conductivity_cells)
+    {
+      std::vector<float> k32(op->ncells);
+      for (long long c = 0; c < op->ncells; ++c)
+        k32[c] = (float)params->conductivity_cells[c];
+      if (cudaMalloc(&op->d_k64, sizeof(double) * op->ncells) != cudaSuccess ||
+          cudaMalloc(&op->d_k32, sizeof(float) * op->ncells) != cudaSuccess)
+        return clean(MPDG_ERR_NOMEM, "conductivity field");
+      if (cudaMemcpy(op->d_k64, params->conductivity_cells, sizeof(double) * op->ncells, cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+          cudaMemcpy(op->d_k32, k32.data(), sizeof(float) * op->ncells, cudaMemcpyHostToDevice) != cudaSuccess)
+        return clean(MPDG_ERR_CUDA, "conductivity copy");
+    }
+  (void)tables(op->degree); // build the 1-D tables once
+  *out = op;
+  return MPDG_OK;
+}
+
+int
+mpdg_op_destroy(mpdg_op *op)
+{
+  if (!op)
+    return MPDG_OK;
+  if (op->stream)
+    cudaStreamSynchronize(op->stream);
+  else
+    cudaDeviceSynchronize();
+  for (auto &kv : op->ws)
+    cudaFree(kv.second.first);
+  cudaFree(op->d_sync);
+  cudaFree(op->d_err);
+  cudaFree(op->d_red);
+  cudaFree(op->d_scal);
+  cudaFree(op->d_cg);
+  cudaFree(op->d_mask);
+  cudaFree(op->d_k64);
+  cudaFree(op->d_k32);
+  if (op->h_cg)
+    cudaFreeHost(op->h_cg);
+  if (op->h_scal)
+    cudaFreeHost(op->h_scal);
+  delete op;
+  return MPDG_OK;
+}
+
+int64_t
+mpdg_op_n_dofs(const mpdg_op *op)
+{
+  return op ? op->ndofs : -1;
+}
+
+int64_t
+mpdg_op_n_cells(const mpdg_op *op)
+{
+  return op ? op->ncells : -1;
+}
+
+int
+mpdg_op_set_stream(mpdg_op *op, void *stream)
+{
+  if (int e = check_op(op))
+    return e;
+  op->stream = static_cast<cudaStream_t>(stream);
+  return MPDG_OK;
+}
+
+int
+mpdg_op_reset_time_increment(mpdg_op *op, double dt)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!(dt > 0.0))
+    return fail(MPDG_ERR_ZERO_DT, "time increment must be positive (ExcZeroTimeIncrement)");
+  op->dt = dt;
+  return MPDG_OK;
+}
+
+int
+mpdg_op_reset_dof_index(mpdg_op *op, int with_dirichlet)
+{
+  if (int e = check_op(op))
+    return e;
+  op->with_bc = with_dirichlet != 0;
+  return MPDG_OK;
+}
+
+int
+mpdg_op_set_conductivity(mpdg_op *op, const double *k_cells)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_HEAT || !k_cells)
+    return fail(MPDG_ERR_ARG, "conductivity applies to the heat operator");
+  if (!op->d_k64)
+    {
+      if (cudaMalloc(&op->d_k64, sizeof(double) * op->ncells) != cudaSuccess ||
+          cudaMalloc(&op->d_k32, sizeof(float) * op->ncells) != cudaSuccess)
+        return fail(MPDG_ERR_NOMEM, "conductivity field");
+    }
+  MPDG_CUDA(cudaMemcpyAsync(op->d_k64, k_cells, sizeof(double) * op->ncells, cudaMemcpyDeviceToDevice, op->stream));
+  MPDG_CUDA(vec_convert<float, double>(op->d_k32, op->d_k64, op->ncells, op->stream));
+  return MPDG_OK;
+}
+
+int
+mpdg_op_vmult(mpdg_op *op, double *dst, const double *src)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!dst || !src || dst == src)
+    return fail(MPDG_ERR_ARG, "vmult needs distinct non-null dst and src");
+  return apply<double>(op, (int)OutMode::Set, 1.0, dst, src, nullptr, 1);
+}
+
+int
+mpdg_op_vmult_f32(mpdg_op *op, float *dst, const float *src)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!dst || !src || dst == src)
+    return fail(MPDG_ERR_ARG, "vmult needs distinct non-null dst and src");
+  return apply<float>(op, (int)OutMode::Set, 1.0, dst, src, nullptr, 1);
+}
+
+int
+mpdg_op_vmult_add(mpdg_op *op, double *dst, const double *src, double scale)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!dst || !src || dst == src)
+    return fail(MPDG_ERR_ARG, "vmult_add needs distinct non-null dst and src");
+  return apply<double>(op, (int)OutMode::Add, scale, dst, src, nullptr, 1);
+}
+
+int
+mpdg_op_residual(mpdg_op *op, double *r, const double *b, const double *x)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!r || !b || !x || r == x)
+    return fail(MPDG_ERR_ARG, "residual needs non-null r, b, x with r != x");
+  return apply<double>(op, (int)OutMode::BPlus, -1.0, r, x, b, 1);
+}
+
+int
+mpdg_op_vmult_host(mpdg_op *op, double *dst_host, const double *src_host)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!dst_host || !src_host)
+    return fail(MPDG_ERR_ARG, "null host buffer");
+  double *ds = op->vec<double>("host_src"), *dd = op->vec<double>("host_dst");
+  if (!ds || !dd)
+    return fail(MPDG_ERR_NOMEM, "staging vectors");
+  const size_t bytes = sizeof(double) * op->ndofs;
+  MPDG_CUDA(cudaMemcpyAsync(ds, src_host, bytes, cudaMemcpyHostToDevice, op->stream));
+  if (int e = apply<double>(op, (int)OutMode::Set, 1.0, dd, ds, nullptr, 1))
+    return e;
+  MPDG_CUDA(cudaMemcpyAsync(dst_host, dd, bytes, cudaMemcpyDeviceToHost, op->stream));
+  MPDG_CUDA(cudaStreamSynchronize(op->stream));
+  return MPDG_OK;
+}
+
+int
+mpdg_op_compute_inverse_diagonal(mpdg_op *op, double *diag)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!diag)
+    return fail(MPDG_ERR_ARG, "null diagonal");
+  return inverse_diagonal<double>(op, diag);
+}
+
+int
+mpdg_op_compute_inverse_diagonal_f32(mpdg_op *op, float *diag)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!diag)
+    return fail(MPDG_ERR_ARG, "null diagonal");
+  return inverse_diagonal<float>(op, diag);
+}
+
+int
+mpdg_op_create_rhs(mpdg_op *op, double *dst, const double *a, const double *b, const double *c)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!(op->dt > 0.0))
+    return fail(MPDG_ERR_ZERO_DT, "time increment must be positive (ExcZeroTimeIncrement)");
+  if (!dst || !a)
+    return fail(MPDG_ERR_ARG, "create_rhs needs dst and its first input");
+  if (op->kind == MPDG_HEAT)
+    {
+      // v = (rho c_p/dt)(T_old - T) + q ; dst += M v - K_k T   (plain reads, free rows)
+      double *v = op->vec<double>("rhs_tmp");
+      if (!v)
+        return fail(MPDG_ERR_NOMEM, "rhs work vector");
+      const double s = op->rho_cp / op->dt;
+      MPDG_CUDA(vec_axpby<double>(v, -s, a, b ? s : 0.0, b, op->ndofs, op->stream));
+      if (c)
+        MPDG_CUDA(vec_axpby<double>(v, 1.0, v, 1.0, c, op->ndofs, op->stream));
+      if (int e = apply<double>(op, (int)OutMode::Add, 1.0, dst, v, nullptr, 0, 1))
+        return e;
+      return apply<double>(op, (int)OutMode::Add, -1.0, dst, a, nullptr, 0, 2);
+    }
+  return apply<double>(op, (int)OutMode::Add, 1.0, dst, a, nullptr, 0, 3);
+}
+
+int
+mpdg_solve(mpdg_op *op, double *x, const double *b, const mpdg_solver_params *params, mpdg_solve_info *info)
+{
+  if (int e = check_op(op))
+    return e;
+  return solve_typed<double>(op, x, b, params, info, "s64_");
+}
+
+int
+mpdg_solve_f32(mpdg_op *op, float *x, const float *b, const mpdg_solver_params *params, mpdg_solve_info *info)
+{
+  if (int e = check_op(op))
+    return e;
+  return solve_typed<float>(op, x, b, params, info, "s32_");
+}
+
+int
+mpdg_solve_mixed(mpdg_op *op, double *x, const double *b, const mpdg_mixed_params *prm, mpdg_solve_info *info)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!x || !b || !prm)
+    return fail(MPDG_ERR_ARG, "null argument to mpdg_solve_mixed");
+  const long long n   = op->ndofs;
+  double         *r64 = op->vec<double>("mx_r64");
+  float          *r32 = op->vec<float>("mx_r32"), *e32 = op->vec<float>("mx_e32"), *invd32 = op->vec<float>("mx_invd32");
+  double         *invd64 = op->vec<double>("mx_invd64");
+  if (!r64 || !r32 || !e32 || !invd32 || !invd64)
+    return fail(MPDG_ERR_NOMEM, "mixed-precision work vectors");
+  // Jacobi diagonal computed in FP64 and rounded once
+  if (int e = inverse_diagonal<double>(op, invd64))
+    return e;
+  MPDG_CUDA(vec_convert<float, double>(invd32, invd64, n, op->stream));
+  const double *bb = b;
+  MPDG_CUDA(vec_multidot<double>(&bb, &bb, 1, n, op->d_scal, op->reducer(), op->stream));
+  MPDG_CUDA(cudaMemcpy(op->h_scal, op->d_scal, sizeof(double), cudaMemcpyDeviceToHost));
+  const double bnorm = std::sqrt(op->h_scal[0]);
+  const double tol   = prm->outer_rel_tol * bnorm;
+  int          inner_total = 0, outer = 0, status = MPDG_ERR_NOT_CONVERGED;
+  double       res = 0.0, res0 = -1.0;
+  std::vector<double> hist;
+  for (outer = 0; outer <= prm->max_outer; ++outer)
+    {
+      if (int e = apply<double>(op, (int)OutMode::BPlus, -1.0, r64, x, b, 1))
+        return e;
+      const double *rr = r64;
+      MPDG_CUDA(vec_multidot<double>(&rr, &rr, 1, n, op->d_scal, op->reducer(), op->stream));
+      MPDG_CUDA(cudaMemcpyAsync(op->h_scal, op->d_scal, sizeof(double), cudaMemcpyDeviceToHost, op->stream));
+      MPDG_CUDA(cudaStreamSynchronize(op->stream));
+      res = std::sqrt(op->h_scal[0]);
+      if (res0 < 0)
+        res0 = res;
+      hist.push_back(res);
+      if (res <= tol)
+        {
+          status = MPDG_OK;
+          break;
+        }
+      if (outer == prm->max_outer)
+        break;
+      MPDG_CUDA(vec_convert<float, double>(r32, r64, n, op->stream));
+      MPDG_CUDA(vec_fill<float>(e32, 0.0f, n, op->stream));
+      mpdg_solve_info in{};
+      int             rc;
+      if (prm->solver == MPDG_GMRES)
+        rc = gmres_solve<float>(op, e32, r32, invd32, prm->max_inner, 0.0, prm->inner_rel_tol,
+                                prm->restart > 0 ? prm->restart : 30, &in, "mi32_");
+      else
+        rc = cg_solve<float>(op, e32, r32, invd32, prm->max_inner, 0.0, prm->inner_rel_tol, &in, "mi32_");
+      if (rc != MPDG_OK && rc != MPDG_ERR_NOT_CONVERGED)
+        return rc;
+      inner_total += in.iterations;
+      MPDG_CUDA(vec_add_f32_to_f64(x, e32, n, op->stream));
+    }
+  if (info)
+    {
+      info->iterations       = outer;
+      info->inner_iterations = inner_total;
+      info->status           = status;
+      info->initial_residual = res0;
+      info->final_residual   = res;
+      if (info->history && info->history_capacity > 0)
+        {
+          const int cnt = std::min<int>(info->history_capacity, (int)hist.size());
+          std::memcpy(info->history, hist.data(), sizeof(double) * cnt);
+        }
+    }
+  if (status != MPDG_OK)
+    return fail(MPDG_ERR_NOT_CONVERGED, "mixed-precision defect correction did not converge");
+  return MPDG_OK;
+}
+
+int
+mpdg_op_device_errors(mpdg_op *op)
+{
+  if (!op)
+    return -1;
+  int v = 0;
+  if (cudaMemcpy(&v, op->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  cudaMemset(op->d_err, 0, sizeof(int));
+  return v;
+}
+
+} // extern "C"

@@ -1,0 +1,597 @@
+// Heat operator kernels: matrix-free apply (fast diagonalisation, see sumfac.cuh) and the
+// DoF-parallel diagonal.  Reference: source/heat/heat_diffuse_operator.cpp
+//   vmult                      :179-197  (MatrixFree::loop, zero_dst = true)
+//   tangent_local_cell_operation :1029-1079 (val = rho c_p/dt u, grad = k grad u)
+//   compute_inverse_diagonal_from_matrixfree :271-284 (|d| > 1e-10 ? 1/d : 1)
+//
+// Work decomposition: one CTA per brick of cells (brick.cuh).  For k <= 2 one thread holds a whole
+// cell (n^3 <= 27 values) in registers.  For k >= 3 a cell is split over two threads in different
+// warps by the reflection parity of its z-modes: the "odd" thread transforms the floor(n/2) odd
+// z-planes (u_l - u_{n-1-l}) and leaves its result in shared memory, the "even" thread transforms
+// the ceil(n/2) even z-planes (u_l + u_{n-1-l}, u_mid) and combines both into the nodal output.
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <set>
+
+#include "brick.cuh"
+#include "kernels.h"
+#include "sumfac.cuh"
+
+namespace mpdg
+{
+  // 1-D fast-diagonalisation tables per degree in constant memory (uploaded once per device):
+  // [WE (ne*ne) | WO (no*no) | lambda (n)]
+  constexpr int FD_TAB = 32;
+  __constant__ double c_fd_d[5][FD_TAB];
+  __constant__ float  c_fd_f[5][FD_TAB];
+
+  template <typename T>
+  __device__ __forceinline__ const T *
+  fd_table(int K)
+  {
+    if constexpr (sizeof(T) == 8)
+      return c_fd_d[K];
+    else
+      return c_fd_f[K];
+  }
+
+  template <typename T, int N>
+  struct HeatArgs
+  {
+    T          cx, cy, cz; // stiffness geometry factors (hy hz / hx, ...)
+    GridDesc   g;
+    SyncDesc   s;
+    T          alpha;  // scale * rho c_p / dt * hx hy hz
+    T          kscale; // scale (multiplies the conductivity)
+    T          kconst; // conductivity when kcell == nullptr
+    const T   *kcell;  // per-cell conductivity
+    const T   *src;
+    T         *dst;
+    const T   *b;      // BPlus mode: dst = b + A src (may alias dst)
+    int        mask_src;
+    const int *skip;   // return at once when *skip != 0 (a solve has finished)
+  };
+
+  template <int K, typename T>
+  struct HeatBrickShape;
+  template <typename T>
+  struct HeatBrickShape<1, T>
+  {
+    static constexpr int BX = 8, BY = 8, BZ = 4;
+  };
+  template <typename T>
+  struct HeatBrickShape<2, T>
+  {
+    static constexpr int BX = 8, BY = 8, BZ = 4;
+  };
+  template <typename T>
+  struct HeatBrickShape<3, T>
+  {
+    static constexpr int BX = 4, BY = 4, BZ = 4;
+  };
+  template <typename T>
+  struct HeatBrickShape<4, T>
+  {
+    static constexpr int BX = 4, BY = 4, BZ = 4;
+  };
+
+  template <int K, typename T>
+  struct HeatLayout
+  {
+    static constexpr int  N = K + 1, NE = (N + 1) / 2, NO = N / 2;
+    using S                 = HeatBrickShape<K, T>;
+    static constexpr bool TWO = (N >= 4);
+    static constexpr int  NC  = S::BX * S::BY * S::BZ;
+    static constexpr int  NT  = TWO ? 2 * NC : NC;
+    using BR                  = Brick<K, S::BX, S::BY, S::BZ, NT>;
+    static constexpr int  SH  = N * N * N - K * K * K;
+    static constexpr int  ODD = TWO ? NO * N * N : 0;
+    static constexpr size_t bytes = sizeof(T) * ((size_t)BR::NPTS + (size_t)(ODD + SH) * NC);
+  };
+
+  template <int K, typename T, OutMode MODE>
+  __global__ void __launch_bounds__(HeatLayout<K, T>::NT)
+  heat_apply_kernel(const __grid_constant__ HeatArgs<T, K + 1> a)
+  {
+    using L          = HeatLayout<K, T>;
+    using BR         = typename L::BR;
+    constexpr int N  = K + 1, NE = L::NE, NO = L::NO;
+    constexpr int NC = L::NC, PX = BR::PX, PY = BR::PY;
+    constexpr int BX = BR::BX, BY = BR::BY, BZ = BR::BZ;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *const s_src   = reinterpret_cast<T *>(smem_raw); // staging; output accumulation later
+    T *const s_dst   = s_src;
+    T *const s_odd   = s_src + BR::NPTS;                // two-pass scratch (column per cell)
+    T *const s_shell = s_src + BR::NPTS + L::ODD * NC;  // published shell points (column per cell)
+    __shared__ unsigned s_ticket;
+    if (a.skip != nullptr && *a.skip != 0)
+      return;
+
+    BR br;
+    if (!brick_begin<BR, T, MODE>(br, a.g, a.s, a.dst, a.b, &s_ticket))
+      return;
+    brick_stage(br, a.src, a.mask_src != 0, s_src);
+
+    const int  cell = threadIdx.x % NC;       // cell of the brick handled by this thread
+    const int  role = threadIdx.x / NC;       // 0: whole cell / even z-modes, 1: odd z-modes
+    const int  tx = cell % BX, ty = (cell / BX) % BY, tz = cell / (BX * BY);
+    const int  cx = br.c0[0] + tx, cy = br.c0[1] + ty, cz = br.c0[2] + tz;
+    const bool valid = cx < a.g.m[0] && cy < a.g.m[1] && cz < a.g.m[2];
+    const int  lox = tx == 0 ? 0 : 1, loy = ty == 0 ? 0 : 1, loz = tz == 0 ? 0 : 1;
+    const int  base = (K * tz) * PY * PX + (K * ty) * PX + K * tx;
+    T          kc   = T(0);
+    if (valid)
+      {
+        const long long c = (long long)cx + (long long)a.g.m[0] * ((long long)cy + (long long)a.g.m[1] * cz);
+        kc                = a.kscale * (a.kcell ? a.kcell[c] : a.kconst);
+      }
+    const T  alpha = a.alpha;
+    const T *tb    = fd_table<T>(K);
+    const T *we    = tb;
+    const T *wo    = tb + NE * NE;
+    const T *lam   = tb + NE * NE + NO * NO;
+    const T  kcx = kc * a.cx, kcy = kc * a.cy, kcz = kc * a.cz;
+    // multiply P modal planes (modal z index z0 + c) by alpha + k_c (cx lam_a + cy lam_b + cz lam_c)
+    auto scale_planes = [&](T *v, const int P, const int z0) {
+#pragma unroll
+      for (int c = 0; c < N; ++c)
+        if (c < P)
+          {
+            const T tz = fma(kcz, lam[z0 + c], alpha);
+#pragma unroll
+            for (int b = 0; b < N; ++b)
+              {
+                const T tyz = fma(kcy, lam[b], tz);
+#pragma unroll
+                for (int aa = 0; aa < N; ++aa)
+                  v[(c * N + b) * N + aa] *= fma(kcx, lam[aa], tyz);
+              }
+          }
+    };
+    // owned points go to the brick accumulator, shell points to this cell's shell column
+    auto emit = [&](const int i, const int j, const int l, const T v) {
+      const bool owned = (i >= lox) && (j >= loy) && (l >= loz);
+      T *p = owned ? s_dst + (base + l * PY * PX + j * PX + i) : s_shell + (shell_index<N>(i, j, l) * NC + cell);
+      *p   = v;
+    };
+
+    if constexpr (!L::TWO)
+      {
+        T u[N * N * N];
+        if (valid)
+          {
+#pragma unroll
+            for (int l = 0; l < N; ++l)
+#pragma unroll
+              for (int j = 0; j < N; ++j)
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                  u[(l * N + j) * N + i] = s_src[base + l * PY * PX + j * PX + i];
+            xy_planes<T, N, N, true>(u, we, wo);
+#pragma unroll
+            for (int q = 0; q < N * N; ++q)
+              fwd_line<T, N, N * N>(u, q, we, wo);
+            scale_planes(u, N, 0);
+#pragma unroll
+            for (int q = 0; q < N * N; ++q)
+              bwd_line<T, N, N * N>(u, q, we, wo);
+            xy_planes<T, N, N, false>(u, we, wo);
+          }
+        __syncthreads(); // all reads of s_src done: s_dst may overlay it
+        if (valid)
+          {
+#pragma unroll
+            for (int l = 0; l < N; ++l)
+#pragma unroll
+              for (int j = 0; j < N; ++j)
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                  emit(i, j, l, u[(l * N + j) * N + i]);
+          }
+      }
+    else
+      {
+        T e[NE * N * N];
+        if (valid && role == 1)
+          {
+            // odd z-modes: o_k = u_k - u_{N-1-k}; result O_k to the scratch column of this cell
+            T *v = e; // reuse the register array (NO <= NE planes)
+#pragma unroll
+            for (int k = 0; k < NO; ++k)
+#pragma unroll
+              for (int j = 0; j < N; ++j)
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                  v[(k * N + j) * N + i] = s_src[base + k * PY * PX + j * PX + i] -
+                                           s_src[base + (N - 1 - k) * PY * PX + j * PX + i];
+#pragma unroll
+            for (int q = 0; q < N * N; ++q)
+              {
+                T t[NO];
+#pragma unroll
+                for (int m = 0; m < NO; ++m)
+                  {
+                    T s = wo[m * NO] * v[q];
+#pragma unroll
+                    for (int k = 1; k < NO; ++k)
+                      s = fma(wo[m * NO + k], v[k * N * N + q], s);
+                    t[m] = s;
+                  }
+#pragma unroll
+                for (int m = 0; m < NO; ++m)
+                  v[m * N * N + q] = t[m];
+              }
+            xy_planes<T, N, NO, true>(v, we, wo);
+            scale_planes(v, NO, NE);
+            xy_planes<T, N, NO, false>(v, we, wo);
+#pragma unroll
+            for (int q = 0; q < N * N; ++q)
+              {
+                T t[NO];
+#pragma unroll
+                for (int k = 0; k < NO; ++k)
+                  {
+                    T s = wo[k] * v[q];
+#pragma unroll
+                    for (int m = 1; m < NO; ++m)
+                      s = fma(wo[m * NO + k], v[m * N * N + q], s);
+                    t[k] = s;
+                  }
+#pragma unroll
+                for (int k = 0; k < NO; ++k)
+                  s_odd[(k * N * N + q) * NC + cell] = t[k];
+              }
+          }
+        else if (valid)
+          {
+            // even z-modes: e_k = u_k + u_{N-1-k}, e_mid = u_mid; kept in registers
+#pragma unroll
+            for (int k = 0; k < NE; ++k)
+#pragma unroll
+              for (int j = 0; j < N; ++j)
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                  {
+                    const T lo = s_src[base + k * PY * PX + j * PX + i];
+                    e[(k * N + j) * N + i] =
+                      (k < N / 2) ? lo + s_src[base + (N - 1 - k) * PY * PX + j * PX + i] : lo;
+                  }
+#pragma unroll
+            for (int q = 0; q < N * N; ++q)
+              {
+                T t[NE];
+#pragma unroll
+                for (int m = 0; m < NE; ++m)
+                  {
+                    T s = we[m * NE] * e[q];
+#pragma unroll
+                    for (int k = 1; k < NE; ++k)
+                      s = fma(we[m * NE + k], e[k * N * N + q], s);
+                    t[m] = s;
+                  }
+#pragma unroll
+                for (int m = 0; m < NE; ++m)
+                  e[m * N * N + q] = t[m];
+              }
+            xy_planes<T, N, NE, true>(e, we, wo);
+            scale_planes(e, NE, 0);
+            xy_planes<T, N, NE, false>(e, we, wo);
+#pragma unroll
+            for (int q = 0; q < N * N; ++q)
+              {
+                T t[NE];
+#pragma unroll
+                for (int k = 0; k < NE; ++k)
+                  {
+                    T s = we[k] * e[q];
+#pragma unroll
+                    for (int m = 1; m < NE; ++m)
+                      s = fma(we[m * NE + k], e[m * N * N + q], s);
+                    t[k] = s;
+                  }
+#pragma unroll
+                for (int k = 0; k < NE; ++k)
+                  e[k * N * N + q] = t[k];
+              }
+          }
+        __syncthreads(); // s_src dead, odd results complete
+        if (valid && role == 0)
+          {
+#pragma unroll
+            for (int k = 0; k < N / 2; ++k)
+#pragma unroll
+              for (int j = 0; j < N; ++j)
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                  {
+                    const T E = e[(k * N + j) * N + i];
+                    const T O = s_odd[((k * N + j) * N + i) * NC + cell];
+                    emit(i, j, k, E + O);
+                    emit(i, j, N - 1 - k, E - O);
+                  }
+            if constexpr (N % 2 == 1)
+#pragma unroll
+              for (int j = 0; j < N; ++j)
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                  emit(i, j, N / 2, e[((N / 2) * N + j) * N + i]);
+          }
+      }
+    __syncthreads();
+
+    // ---- add the shells of in-brick upper neighbours into the owned points
+    if (valid && role == 0)
+      {
+        const bool ux = tx + 1 < BX && cx + 1 < a.g.m[0];
+        const bool uy = ty + 1 < BY && cy + 1 < a.g.m[1];
+        const bool uz = tz + 1 < BZ && cz + 1 < a.g.m[2];
+#pragma unroll
+        for (int l = 0; l < N; ++l)
+#pragma unroll
+          for (int j = 0; j < N; ++j)
+#pragma unroll
+            for (int i = 0; i < N; ++i)
+              {
+                if (i != K && j != K && l != K)
+                  continue;
+                T sum = T(0);
+#pragma unroll
+                for (int s = 1; s < 8; ++s)
+                  {
+                    const int sx = s & 1, sy = (s >> 1) & 1, sz = (s >> 2) & 1;
+                    if ((sx && i != K) || (sy && j != K) || (sz && l != K))
+                      continue;
+                    const bool ok = (!sx || ux) && (!sy || uy) && (!sz || uz);
+                    const int  nb = cell + sx + sy * BX + sz * BX * BY;
+                    const T    v  = s_shell[shell_index<N>(sx ? 0 : i, sy ? 0 : j, sz ? 0 : l) * NC + (ok ? nb : cell)];
+                    sum += ok ? v : T(0);
+                  }
+                const bool owned = (i >= lox) && (j >= loy) && (l >= loz);
+                if (owned)
+                  s_dst[base + l * PY * PX + j * PX + i] += sum;
+              }
+      }
+    __syncthreads();
+    brick_end<BR, T, MODE>(br, a.g, a.s, s_dst, a.dst, a.b);
+  }
+
+  // ---- diagonal: closed-form per-cell entries gathered per DoF (deterministic, no atomics)
+  template <typename T>
+  struct DiagArgs
+  {
+    GridDesc g;
+    int      K;
+    T        alpha, cx, cy, cz; // mass coefficient and stiffness geometry factors
+    T        kconst;
+    const T *kcell;
+    T        mdiag[8], kdiag[8]; // 1-D M_ii, K_ii
+    T        threshold;          // |d| > threshold ? 1/d : 1
+    T       *diag;
+    int      invert;
+  };
+
+  template <typename T>
+  __global__ void
+  heat_diag_kernel(const __grid_constant__ DiagArgs<T> a)
+  {
+    const long long ndofs = (long long)a.g.n[0] * a.g.n[1] * a.g.n[2];
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < ndofs;
+         idx += (long long)gridDim.x * blockDim.x)
+      {
+        const int I = (int)(idx % a.g.n[0]), J = (int)((idx / a.g.n[0]) % a.g.n[1]),
+                  L = (int)(idx / ((long long)a.g.n[0] * a.g.n[1]));
+        T d;
+        if (is_constrained(a.g, I, J, L, idx))
+          d = T(1);
+        else
+          {
+            int       cs[3][2], ls[3][2], nc[3];
+            const int P[3] = {I, J, L};
+            for (int dd = 0; dd < 3; ++dd)
+              {
+                nc[dd]      = 0;
+                const int q = P[dd] / a.K, r = P[dd] % a.K;
+                if (r == 0)
+                  {
+                    if (q - 1 >= 0)
+                      {
+                        cs[dd][nc[dd]] = q - 1;
+                        ls[dd][nc[dd]] = a.K;
+                        ++nc[dd];
+                      }
+                    if (q < a.g.m[dd])
+                      {
+                        cs[dd][nc[dd]] = q;
+                        ls[dd][nc[dd]] = 0;
+                        ++nc[dd];
+                      }
+                  }
+                else
+                  {
+                    cs[dd][0] = q;
+                    ls[dd][0] = r;
+                    nc[dd]    = 1;
+                  }
+              }
+            d = T(0);
+            for (int z = 0; z < nc[2]; ++z)
+              for (int y = 0; y < nc[1]; ++y)
+                for (int x = 0; x < nc[0]; ++x)
+                  {
+                    const long long cell =
+                      (long long)cs[0][x] + (long long)a.g.m[0] * ((long long)cs[1][y] + (long long)a.g.m[1] * cs[2][z]);
+                    const T kc = a.kcell ? a.kcell[cell] : a.kconst;
+                    const T mx = a.mdiag[ls[0][x]], my = a.mdiag[ls[1][y]], mz = a.mdiag[ls[2][z]];
+                    const T kx = a.kdiag[ls[0][x]], ky = a.kdiag[ls[1][y]], kz = a.kdiag[ls[2][z]];
+                    d += a.alpha * mx * my * mz + kc * (a.cx * kx * my * mz + a.cy * mx * ky * mz + a.cz * mx * my * kz);
+                  }
+          }
+        if (a.invert)
+          d = (fabs(d) > a.threshold) ? T(1) / d : T(1);
+        a.diag[idx] = d;
+      }
+  }
+
+  // ------------------------------------------------------------------------------------------
+  // host launchers
+
+  // Upload the 1-D tables of every degree once per device.
+  static cudaError_t
+  upload_fd_tables()
+  {
+    static std::mutex          mtx;
+    static std::set<int>       done;
+    int                        dev = 0;
+    cudaError_t                e   = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+      return e;
+    std::lock_guard<std::mutex> lock(mtx);
+    if (done.count(dev))
+      return cudaSuccess;
+    double hd[5][FD_TAB] = {};
+    float  hf[5][FD_TAB] = {};
+    for (int K = 1; K <= 4; ++K)
+      {
+        const Tables1D &t = tables(K);
+        int             o = 0;
+        for (int i = 0; i < t.ne * t.ne; ++i)
+          hd[K][o++] = t.WE[i];
+        for (int i = 0; i < t.no * t.no; ++i)
+          hd[K][o++] = t.WO[i];
+        for (int i = 0; i < t.n; ++i)
+          hd[K][o++] = t.lam[i];
+        for (int i = 0; i < o; ++i)
+          hf[K][i] = (float)hd[K][i];
+      }
+    if ((e = cudaMemcpyToSymbol(c_fd_d, hd, sizeof(hd))) != cudaSuccess)
+      return e;
+    if ((e = cudaMemcpyToSymbol(c_fd_f, hf, sizeof(hf))) != cudaSuccess)
+      return e;
+    done.insert(dev);
+    return cudaSuccess;
+  }
+
+  template <int K, typename T, OutMode MODE>
+  static cudaError_t
+  launch_apply(const HeatLaunch<T> &h, cudaStream_t stream)
+  {
+    using L = HeatLayout<K, T>;
+    HeatArgs<T, K + 1> a;
+    cudaError_t        ue = upload_fd_tables();
+    if (ue != cudaSuccess)
+      return ue;
+    a.cx       = (T)h.geo.cx;
+    a.cy       = (T)h.geo.cy;
+    a.cz       = (T)h.geo.cz;
+    a.g        = h.grid;
+    a.s        = h.sync;
+    a.alpha    = (T)(h.scale * h.geo.mass_coef);
+    a.kscale   = (T)h.scale;
+    a.kconst   = (T)h.kconst;
+    a.kcell    = h.kcell;
+    a.src      = h.src;
+    a.dst      = h.dst;
+    a.b        = h.b;
+    a.mask_src = h.mask_src;
+    a.skip     = h.skip;
+    auto kern  = heat_apply_kernel<K, T, MODE>;
+    static thread_local bool attr_done = false;
+    if (!attr_done)
+      {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
+        if (e != cudaSuccess)
+          return e;
+        attr_done = true;
+      }
+    const unsigned nbricks = (unsigned)h.grid.nbr[0] * h.grid.nbr[1] * h.grid.nbr[2];
+    kern<<<nbricks, L::BR::NT, L::bytes, stream>>>(a);
+    return cudaGetLastError();
+  }
+
+  template <typename T>
+  static void
+  brick_shape(int K, int &bx, int &by, int &bz)
+  {
+    switch (K)
+      {
+        case 1: bx = HeatBrickShape<1, T>::BX; by = HeatBrickShape<1, T>::BY; bz = HeatBrickShape<1, T>::BZ; break;
+        case 2: bx = HeatBrickShape<2, T>::BX; by = HeatBrickShape<2, T>::BY; bz = HeatBrickShape<2, T>::BZ; break;
+        case 3: bx = HeatBrickShape<3, T>::BX; by = HeatBrickShape<3, T>::BY; bz = HeatBrickShape<3, T>::BZ; break;
+        default: bx = HeatBrickShape<4, T>::BX; by = HeatBrickShape<4, T>::BY; bz = HeatBrickShape<4, T>::BZ; break;
+      }
+  }
+
+  template <typename T>
+  void
+  heat_brick_shape(int K, int shape[3])
+  {
+    brick_shape<T>(K, shape[0], shape[1], shape[2]);
+  }
+
+  template <int K, typename T>
+  static cudaError_t
+  dispatch_mode(const HeatLaunch<T> &h, cudaStream_t s)
+  {
+    switch (h.mode)
+      {
+        case 0: return launch_apply<K, T, OutMode::Set>(h, s);
+        case 1: return launch_apply<K, T, OutMode::Add>(h, s);
+        default: return launch_apply<K, T, OutMode::BPlus>(h, s);
+      }
+  }
+
+  template <typename T>
+  cudaError_t
+  heat_apply(const HeatLaunch<T> &h, cudaStream_t s)
+  {
+    switch (h.degree)
+      {
+        case 1: return dispatch_mode<1, T>(h, s);
+        case 2: return dispatch_mode<2, T>(h, s);
+        case 3: return dispatch_mode<3, T>(h, s);
+        case 4: return dispatch_mode<4, T>(h, s);
+        default: return cudaErrorInvalidValue;
+      }
+  }
+
+  template <typename T>
+  cudaError_t
+  heat_diagonal(const GridDesc &g, int K, const HeatGeom &geo, double kconst, const T *kcell, T *diag,
+                bool invert, double threshold, cudaStream_t s)
+  {
+    if (K < 1 || K > 7)
+      return cudaErrorInvalidValue;
+    DiagArgs<T>     a;
+    const Tables1D &t = tables(K);
+    a.g               = g;
+    a.K               = K;
+    a.alpha           = (T)geo.mass_coef;
+    a.cx              = (T)geo.cx;
+    a.cy              = (T)geo.cy;
+    a.cz              = (T)geo.cz;
+    a.kconst          = (T)kconst;
+    a.kcell           = kcell;
+    for (int i = 0; i < 8; ++i)
+      {
+        a.mdiag[i] = i <= K ? (T)t.M[i * t.n + i] : T(0);
+        a.kdiag[i] = i <= K ? (T)t.K[i * t.n + i] : T(0);
+      }
+    a.threshold = (T)threshold;
+    a.diag      = diag;
+    a.invert    = invert ? 1 : 0;
+    const long long n = (long long)g.n[0] * g.n[1] * g.n[2];
+    const int       blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    heat_diag_kernel<T><<<blocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+  }
+
+  template cudaError_t heat_apply<double>(const HeatLaunch<double> &, cudaStream_t);
+  template cudaError_t heat_apply<float>(const HeatLaunch<float> &, cudaStream_t);
+  template cudaError_t heat_diagonal<double>(const GridDesc &, int, const HeatGeom &, double, const double *, double *,
+                                             bool, double, cudaStream_t);
+  template cudaError_t heat_diagonal<float>(const GridDesc &, int, const HeatGeom &, double, const float *, float *,
+                                            bool, double, cudaStream_t);
+  template void heat_brick_shape<double>(int, int[3]);
+  template void heat_brick_shape<float>(int, int[3]);
+} // namespace mpdg

@@ -1,0 +1,164 @@
+// Internal launch interfaces of the CUDA kernels (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "brick.cuh"
+#include "tables.h"
+
+namespace mpdg
+{
+  // Geometry factors of the uniform box mesh (hx, hy, hz per cell).
+  struct HeatGeom
+  {
+    double mass_coef; // multiplies M(x)M(x)M (rho c_p / dt * hx hy hz for the tangent)
+    double cx, cy, cz; // hy hz / hx, hx hz / hy, hx hy / hz
+  };
+
+  template <typename T>
+  struct HeatLaunch
+  {
+    int         degree   = 2;
+    int         mode     = 0;   // OutMode
+    double      scale    = 1.0; // dst (+)= scale * A src
+    HeatGeom    geo{};
+    GridDesc    grid{};
+    SyncDesc    sync{};
+    double      kconst   = 1.0;
+    const T    *kcell    = nullptr;
+    const T    *src      = nullptr;
+    T          *dst      = nullptr;
+    const T    *b        = nullptr;
+    int         mask_src = 1;
+    const int  *skip     = nullptr; // device flag: return at once when nonzero
+  };
+
+  template <typename T>
+  cudaError_t heat_apply(const HeatLaunch<T> &h, cudaStream_t s);
+
+  template <typename T>
+  cudaError_t heat_diagonal(const GridDesc &g, int K, const HeatGeom &geo, double kconst, const T *kcell,
+                            T *diag, bool invert, double threshold, cudaStream_t s);
+
+  template <typename T>
+  void heat_brick_shape(int K, int shape[3]);
+
+  // ---- advection-diffusion (source/level_set/advection_diffusion_operator.cpp)
+  struct AdvParams
+  {
+    double inv_dt;
+    double theta_adv; // multiplies v . grad u
+    double theta_dif; // multiplies eps grad u . grad phi (already times eps)
+    double vel[12];   // v(x) = vel[0..2] + G x, G = vel[3..11] row-major
+    double origin[3];
+    double h[3];
+  };
+
+  template <typename T>
+  struct AdvLaunch
+  {
+    int       degree   = 2;
+    int       mode     = 0;
+    double    scale    = 1.0;
+    AdvParams p{};
+    GridDesc  grid{};
+    SyncDesc  sync{};
+    const T  *src      = nullptr;
+    T        *dst      = nullptr;
+    const T  *b        = nullptr;
+    int       mask_src = 1;
+    const int *skip    = nullptr;
+  };
+
+  template <typename T>
+  cudaError_t adv_apply(const AdvLaunch<T> &h, cudaStream_t s);
+
+  // per-cell diagonal entries gathered per DoF, then optionally inverted with the advection rule
+  template <typename T>
+  cudaError_t adv_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, T *cellbuf, cudaStream_t s);
+
+  template <typename T>
+  void adv_brick_shape(int K, int shape[3]);
+
+  // ---- vectors and reductions (double accumulation for every vector type)
+  constexpr int RED_BLOCKS  = 592; // 4 x 148 SMs
+  constexpr int RED_THREADS = 256;
+
+  struct Reducer
+  {
+    double   *partials; // RED_BLOCKS * 8
+    unsigned *counter;  // last-block ticket
+  };
+
+  // PCG state kept on the device (deal.II SolverCG + ReductionControl semantics)
+  struct CGState
+  {
+    double rho;      // r . z of the current iteration
+    double alpha;
+    double beta;
+    double res0;     // initial residual norm
+    double tol;      // max(abs_tol, rel_tol * res0)
+    double abs_tol;
+    double rel_tol;
+    double res;      // last residual norm
+    int    it;       // completed iterations
+    int    max_it;
+    int    done;     // 0 iterate, 1 converged, 2 failed
+    int    pad;
+  };
+
+  template <typename T>
+  cudaError_t cg_init(const T *r, const T *invd, T *p, CGState *st, double *hist, Reducer red, long long n,
+                      cudaStream_t s);
+  template <typename T>
+  cudaError_t cg_update_p(const T *r, const T *invd, T *p, const CGState *st, long long n, cudaStream_t s);
+  template <typename T>
+  cudaError_t cg_alpha(const T *p, const T *v, CGState *st, Reducer red, long long n, cudaStream_t s);
+  template <typename T>
+  cudaError_t cg_update_xr(T *x, T *r, const T *p, const T *v, const T *invd, CGState *st, double *hist,
+                           Reducer red, long long n, cudaStream_t s);
+
+  // generic helpers
+  template <typename T>
+  cudaError_t vec_fill(T *x, T v, long long n, cudaStream_t s);
+  template <typename Tdst, typename Tsrc>
+  cudaError_t vec_convert(Tdst *dst, const Tsrc *src, long long n, cudaStream_t s);
+  // dst = a*x + b*y (elementwise, any of x / y may be null meaning 0)
+  template <typename T>
+  cudaError_t vec_axpby(T *dst, double a, const T *x, double b, const T *y, long long n, cudaStream_t s);
+  // x64 += (double) e32
+  cudaError_t vec_add_f32_to_f64(double *x, const float *e, long long n, cudaStream_t s);
+  // out[k] = sum_i x_k[i] * y_k[i], k < m <= 8 (deterministic)
+  template <typename T>
+  cudaError_t vec_multidot(const T *const *x, const T *const *y, int m, long long n, double *out_dev, Reducer red,
+                           cudaStream_t s);
+  // h_k = w . v_k (k < m), out[m] = ||w||^2
+  template <typename T>
+  cudaError_t vec_dots_against(const T *w, const T *const *v, int m, long long n, double *out_dev, Reducer red,
+                               cudaStream_t s);
+  // dst = src * invd (Jacobi)
+  template <typename T>
+  cudaError_t vec_scale(T *dst, const T *src, const T *invd, long long n, cudaStream_t s);
+  // x += sum_k c_k v_k (coefficients on the device), then optionally x *= invd first on the sum
+  template <typename T>
+  cudaError_t vec_multiaxpy(T *x, const T *const *v, const double *coef_dev, int m, long long n, double post_scale,
+                            cudaStream_t s);
+  // w -= sum_k h_k v_k and returns ||w||^2 into out_dev (coefficients on the device)
+  template <typename T>
+  cudaError_t vec_orth_update(T *w, const T *const *v, const double *h_dev, int m, long long n, double *out_dev,
+                              Reducer red, cudaStream_t s);
+  // inverse of a diagonal with the heat rule (|d| > thr ? 1/d : 1) in place
+  template <typename T>
+  cudaError_t vec_invert(T *d, double thr, long long n, cudaStream_t s);
+  // max |d| (deterministic) into out_dev
+  template <typename T>
+  cudaError_t vec_absmax(const T *d, long long n, double *out_dev, Reducer red, cudaStream_t s);
+  // d = |d| > 1e-14 max(1, *amax) ? 1/d : 1 (advection rule, amax on the device)
+  template <typename T>
+  cudaError_t vec_invert_rel(T *d, const double *amax_dev, long long n, cudaStream_t s);
+  // set constrained entries (face mask / per-DoF mask) of x to v
+  template <typename T>
+  cudaError_t vec_set_constrained(T *x, T v, const GridDesc &g, cudaStream_t s);
+} // namespace mpdg

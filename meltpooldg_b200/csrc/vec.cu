@@ -1,0 +1,575 @@
+// Vector kernels and deterministic reductions for the Krylov solvers.
+//
+// Every reduction runs on a fixed grid of RED_BLOCKS blocks with a grid-stride loop, reduces in
+// registers/shared memory in a fixed order, writes one partial per block, and the last block to
+// finish (threadfence + ticket) sums the partials in block order.  Results are therefore
+// bit-reproducible run to run.  Sums are accumulated in double for every vector type, so the FP32
+// inner solver keeps FP64 dot products and norms.
+//
+// The PCG kernels carry the scalar recurrences of dealii::SolverCG on the device (CGState): the
+// host enqueues iterations without waiting for the scalars, and every kernel returns at once
+// when the state says the solve has finished.  ReductionControl semantics
+// (include/meltpooldg/linear_algebra/linear_solver.hpp:36): converged when the unpreconditioned
+// residual norm is <= rel_tol * |r_0| or <= abs_tol; failed at max_it or on NaN.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "kernels.h"
+
+namespace mpdg
+{
+  namespace
+  {
+    constexpr int NWARP = RED_THREADS / 32;
+
+    __device__ __forceinline__ double
+    warp_sum(double v)
+    {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, off);
+      return v;
+    }
+
+    __device__ __forceinline__ double
+    warp_max(double v)
+    {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1)
+        v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+      return v;
+    }
+
+    // Block-reduce M values; the last block sums the per-block partials in order and calls fin()
+    // on thread 0 with the totals.  MAX selects a max-reduction instead of a sum.
+    template <int M, bool MAX = false, class Fin>
+    __device__ __forceinline__ void
+    reduce_finish(double (&v)[M], int m_active, Reducer red, Fin fin)
+    {
+      __shared__ double sh[M][NWARP];
+      __shared__ double tot[M];
+      __shared__ bool   last;
+      const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+      for (int k = 0; k < M; ++k)
+        if (k < m_active)
+          {
+            const double w = MAX ? warp_max(v[k]) : warp_sum(v[k]);
+            if (lane == 0)
+              sh[k][warp] = w;
+          }
+      __syncthreads();
+      if (warp == 0)
+        {
+#pragma unroll
+          for (int k = 0; k < M; ++k)
+            if (k < m_active)
+              {
+                double s = lane < NWARP ? sh[k][lane] : (MAX ? -INFINITY : 0.0);
+                s        = MAX ? warp_max(s) : warp_sum(s);
+                if (lane == 0)
+                  red.partials[k * RED_BLOCKS + blockIdx.x] = s;
+              }
+        }
+      if (threadIdx.x == 0)
+        {
+          __threadfence();
+          last = (atomicAdd(red.counter, 1u) == gridDim.x - 1);
+        }
+      __syncthreads();
+      if (!last)
+        return;
+      for (int k = 0; k < m_active; ++k)
+        {
+          double s = MAX ? -INFINITY : 0.0;
+          for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+            {
+              const double p = __ldcg(red.partials + k * RED_BLOCKS + b);
+              s              = MAX ? fmax(s, p) : s + p;
+            }
+          s = MAX ? warp_max(s) : warp_sum(s);
+          if (lane == 0)
+            sh[0][warp] = s;
+          __syncthreads();
+          if (threadIdx.x == 0)
+            {
+              double t = sh[0][0];
+              for (int w = 1; w < NWARP; ++w)
+                t = MAX ? fmax(t, sh[0][w]) : t + sh[0][w];
+              tot[k] = t;
+            }
+          __syncthreads();
+        }
+      if (threadIdx.x == 0)
+        {
+          fin(tot);
+          *red.counter = 0u;
+          __threadfence();
+        }
+    }
+
+    __device__ __forceinline__ int
+    control_check(const CGState &st, int step, double value)
+    {
+      if (value <= st.rel_tol * st.res0)
+        return 1;
+      if (value <= st.abs_tol)
+        return 1;
+      if (step >= st.max_it || isnan(value))
+        return 2;
+      return 0;
+    }
+
+    template <typename T>
+    __global__ void
+    cg_init_kernel(const T *__restrict__ r, const T *__restrict__ invd, CGState *st, double *hist, Reducer red,
+                   long long n)
+    {
+      double v[2] = {0.0, 0.0};
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+          const double ri = (double)r[i];
+          const double zi = invd ? (double)(T)(r[i] * invd[i]) : ri;
+          v[0] += ri * ri;
+          v[1] += ri * zi;
+        }
+      reduce_finish<2>(v, 2, red, [&](double *tot) {
+        const double res = sqrt(tot[0]);
+        st->res0         = res;
+        st->res          = res;
+        st->tol          = fmax(st->abs_tol, st->rel_tol * res);
+        st->rho          = tot[1];
+        st->beta         = 0.0;
+        st->it           = 0;
+        if (hist)
+          hist[0] = res;
+        st->done = control_check(*st, 0, res);
+      });
+    }
+
+    template <typename T>
+    __global__ void
+    cg_update_p_kernel(const T *__restrict__ r, const T *__restrict__ invd, T *__restrict__ p, const CGState *st,
+                       long long n)
+    {
+      if (st->done)
+        return;
+      const T beta = (T)st->beta;
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+          const T z = invd ? r[i] * invd[i] : r[i];
+          p[i]      = (st->it == 0) ? z : z + beta * p[i];
+        }
+    }
+
+    template <typename T>
+    __global__ void
+    cg_alpha_kernel(const T *__restrict__ p, const T *__restrict__ v, CGState *st, Reducer red, long long n)
+    {
+      if (st->done)
+        return;
+      double a[1] = {0.0};
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        a[0] += (double)p[i] * (double)v[i];
+      reduce_finish<1>(a, 1, red, [&](double *tot) { st->alpha = st->rho / tot[0]; });
+    }
+
+    template <typename T>
+    __global__ void
+    cg_update_xr_kernel(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p, const T *__restrict__ v,
+                        const T *__restrict__ invd, CGState *st, double *hist, Reducer red, long long n)
+    {
+      if (st->done)
+        return;
+      const T alpha = (T)st->alpha;
+      double  a[2]  = {0.0, 0.0};
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+          x[i] += alpha * p[i];
+          const T ri = r[i] - alpha * v[i];
+          r[i]       = ri;
+          const T zi = invd ? ri * invd[i] : ri;
+          a[0] += (double)ri * (double)ri;
+          a[1] += (double)ri * (double)zi;
+        }
+      reduce_finish<2>(a, 2, red, [&](double *tot) {
+        const int    it  = st->it + 1;
+        const double res = sqrt(tot[0]);
+        st->it           = it;
+        st->res          = res;
+        if (hist)
+          hist[it] = res;
+        st->done = control_check(*st, it, res);
+        st->beta = tot[1] / st->rho;
+        st->rho  = tot[1];
+      });
+    }
+
+    template <typename T>
+    __global__ void
+    fill_kernel(T *x, T v, long long n)
+    {
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] = v;
+    }
+
+    template <typename Td, typename Ts>
+    __global__ void
+    convert_kernel(Td *d, const Ts *s, long long n)
+    {
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        d[i] = (Td)s[i];
+    }
+
+    template <typename T>
+    __global__ void
+    axpby_kernel(T *d, T a, const T *x, T b, const T *y, long long n)
+    {
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+          T v = T(0);
+          if (x)
+            v = a * x[i];
+          if (y)
+            v = fma(b, y[i], v);
+          d[i] = v;
+        }
+    }
+
+    __global__ void
+    add_f32_kernel(double *x, const float *e, long long n)
+    {
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] += (double)e[i];
+    }
+
+    template <typename T>
+    __global__ void
+    scale_kernel(T *d, const T *s, const T *w, long long n)
+    {
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        d[i] = w ? s[i] * w[i] : s[i];
+    }
+
+    constexpr int MAXV = 32;
+    template <typename T>
+    struct VecList
+    {
+      const T *v[MAXV];
+    };
+
+    template <typename T>
+    struct PairList
+    {
+      const T *x[8];
+      const T *y[8];
+    };
+
+    template <typename T>
+    __global__ void
+    multidot_kernel(const __grid_constant__ PairList<T> L, int m, long long n, double *out, Reducer red)
+    {
+      double a[8] = {};
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+            if (k < m)
+              a[k] += (double)L.x[k][i] * (double)L.y[k][i];
+        }
+      reduce_finish<8>(a, m, red, [&](double *tot) {
+        for (int k = 0; k < m; ++k)
+          out[k] = tot[k];
+      });
+    }
+
+    // x += post * sum_k c_k v_k   (post = scalar); coefficients read from the device
+    template <typename T>
+    __global__ void
+    multiaxpy_kernel(T *x, const __grid_constant__ VecList<T> L, const double *c, int m, long long n, double post)
+    {
+      __shared__ double cs[MAXV];
+      if (threadIdx.x < MAXV)
+        cs[threadIdx.x] = threadIdx.x < m ? c[threadIdx.x] : 0.0;
+      __syncthreads();
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+          double s = 0.0;
+          for (int k = 0; k < m; ++k)
+            s += cs[k] * (double)L.v[k][i];
+          x[i] += (T)(post * s);
+        }
+    }
+
+    // h_k = w . v_k (k < m), plus ||w||^2 as entry m
+    template <typename T>
+    __global__ void
+    dots_against_kernel(const T *w, const __grid_constant__ VecList<T> L, int m, long long n, double *out, Reducer red)
+    {
+      double a[MAXV + 1] = {};
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+          const double wi = (double)w[i];
+#pragma unroll
+          for (int k = 0; k < MAXV; ++k)
+            if (k < m)
+              a[k] += wi * (double)L.v[k][i];
+          a[MAXV] += wi * wi;
+        }
+      // move the norm entry next to the m dots
+      double b[MAXV + 1];
+#pragma unroll
+      for (int k = 0; k <= MAXV; ++k)
+        b[k] = (k < m) ? a[k] : (k == m ? a[MAXV] : 0.0);
+      reduce_finish<MAXV + 1>(b, m + 1, red, [&](double *tot) {
+        for (int k = 0; k <= m; ++k)
+          out[k] = tot[k];
+      });
+    }
+
+    // w -= sum_k h_k v_k; out[0] = ||w||^2
+    template <typename T>
+    __global__ void
+    orth_update_kernel(T *w, const __grid_constant__ VecList<T> L, const double *h, int m, long long n, double *out,
+                       Reducer red)
+    {
+      __shared__ double hs[MAXV];
+      if (threadIdx.x < MAXV)
+        hs[threadIdx.x] = threadIdx.x < m ? h[threadIdx.x] : 0.0;
+      __syncthreads();
+      double a[1] = {0.0};
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+          double s = (double)w[i];
+          for (int k = 0; k < m; ++k)
+            s -= hs[k] * (double)L.v[k][i];
+          const T t = (T)s;
+          w[i]      = t;
+          a[0] += (double)t * (double)t;
+        }
+      reduce_finish<1>(a, 1, red, [&](double *tot) { out[0] = tot[0]; });
+    }
+
+    template <typename T>
+    __global__ void
+    invert_kernel(T *d, T thr, long long n)
+    {
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        d[i] = (fabs(d[i]) > thr) ? T(1) / d[i] : T(1);
+    }
+
+    template <typename T>
+    __global__ void
+    absmax_kernel(const T *d, long long n, double *out, Reducer red)
+    {
+      double a[1] = {0.0};
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        a[0] = fmax(a[0], fabs((double)d[i]));
+      reduce_finish<1, true>(a, 1, red, [&](double *tot) { out[0] = tot[0]; });
+    }
+
+    template <typename T>
+    __global__ void
+    invert_rel_kernel(T *d, const double *amax, long long n)
+    {
+      const double thr = 1.0e-14 * fmax(1.0, *amax);
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        d[i] = (fabs((double)d[i]) > thr) ? T(1) / d[i] : T(1);
+    }
+
+    template <typename T>
+    __global__ void
+    set_constrained_kernel(T *x, T v, const GridDesc g)
+    {
+      const long long n = (long long)g.n[0] * g.n[1] * g.n[2];
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+          const int I = (int)(i % g.n[0]), J = (int)((i / g.n[0]) % g.n[1]), L = (int)(i / ((long long)g.n[0] * g.n[1]));
+          if (is_constrained(g, I, J, L, i))
+            x[i] = v;
+        }
+    }
+
+    inline int
+    stream_blocks(long long n)
+    {
+      const long long b = (n + 255) / 256;
+      return (int)(b < 148LL * 16 ? (b > 0 ? b : 1) : 148LL * 16);
+    }
+  } // namespace
+
+  template <typename T>
+  cudaError_t
+  cg_init(const T *r, const T *invd, T *p, CGState *st, double *hist, Reducer red, long long n, cudaStream_t s)
+  {
+    (void)p;
+    cg_init_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(r, invd, st, hist, red, n);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  cg_update_p(const T *r, const T *invd, T *p, const CGState *st, long long n, cudaStream_t s)
+  {
+    cg_update_p_kernel<T><<<stream_blocks(n), 256, 0, s>>>(r, invd, p, st, n);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  cg_alpha(const T *p, const T *v, CGState *st, Reducer red, long long n, cudaStream_t s)
+  {
+    cg_alpha_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(p, v, st, red, n);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  cg_update_xr(T *x, T *r, const T *p, const T *v, const T *invd, CGState *st, double *hist, Reducer red,
+               long long n, cudaStream_t s)
+  {
+    cg_update_xr_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(x, r, p, v, invd, st, hist, red, n);
+    return cudaGetLastError();
+  }
+
+  template <typename T>
+  cudaError_t
+  vec_fill(T *x, T v, long long n, cudaStream_t s)
+  {
+    fill_kernel<T><<<stream_blocks(n), 256, 0, s>>>(x, v, n);
+    return cudaGetLastError();
+  }
+  template <typename Td, typename Ts>
+  cudaError_t
+  vec_convert(Td *d, const Ts *src, long long n, cudaStream_t s)
+  {
+    convert_kernel<Td, Ts><<<stream_blocks(n), 256, 0, s>>>(d, src, n);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  vec_axpby(T *d, double a, const T *x, double b, const T *y, long long n, cudaStream_t s)
+  {
+    axpby_kernel<T><<<stream_blocks(n), 256, 0, s>>>(d, (T)a, x, (T)b, y, n);
+    return cudaGetLastError();
+  }
+  cudaError_t
+  vec_add_f32_to_f64(double *x, const float *e, long long n, cudaStream_t s)
+  {
+    add_f32_kernel<<<stream_blocks(n), 256, 0, s>>>(x, e, n);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  vec_multidot(const T *const *x, const T *const *y, int m, long long n, double *out, Reducer red, cudaStream_t s)
+  {
+    if (m < 1 || m > 8)
+      return cudaErrorInvalidValue;
+    PairList<T> L{};
+    for (int k = 0; k < m; ++k)
+      {
+        L.x[k] = x[k];
+        L.y[k] = y[k];
+      }
+    multidot_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(L, m, n, out, red);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  vec_scale(T *d, const T *src, const T *w, long long n, cudaStream_t s)
+  {
+    scale_kernel<T><<<stream_blocks(n), 256, 0, s>>>(d, src, w, n);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  vec_multiaxpy(T *x, const T *const *v, const double *c, int m, long long n, double post, cudaStream_t s)
+  {
+    if (m < 1 || m > MAXV)
+      return cudaErrorInvalidValue;
+    VecList<T> L{};
+    for (int k = 0; k < m; ++k)
+      L.v[k] = v[k];
+    multiaxpy_kernel<T><<<stream_blocks(n), 256, 0, s>>>(x, L, c, m, n, post);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  vec_dots_against(const T *w, const T *const *v, int m, long long n, double *out, Reducer red, cudaStream_t s)
+  {
+    if (m < 1 || m > MAXV)
+      return cudaErrorInvalidValue;
+    VecList<T> L{};
+    for (int k = 0; k < m; ++k)
+      L.v[k] = v[k];
+    dots_against_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, m, n, out, red);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  vec_orth_update(T *w, const T *const *v, const double *h, int m, long long n, double *out, Reducer red,
+                  cudaStream_t s)
+  {
+    if (m < 1 || m > MAXV)
+      return cudaErrorInvalidValue;
+    VecList<T> L{};
+    for (int k = 0; k < m; ++k)
+      L.v[k] = v[k];
+    orth_update_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, h, m, n, out, red);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  vec_invert(T *d, double thr, long long n, cudaStream_t s)
+  {
+    invert_kernel<T><<<stream_blocks(n), 256, 0, s>>>(d, (T)thr, n);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  vec_absmax(const T *d, long long n, double *out, Reducer red, cudaStream_t s)
+  {
+    absmax_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(d, n, out, red);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  vec_invert_rel(T *d, const double *amax, long long n, cudaStream_t s)
+  {
+    invert_rel_kernel<T><<<stream_blocks(n), 256, 0, s>>>(d, amax, n);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  vec_set_constrained(T *x, T v, const GridDesc &g, cudaStream_t s)
+  {
+    const long long n = (long long)g.n[0] * g.n[1] * g.n[2];
+    set_constrained_kernel<T><<<stream_blocks(n), 256, 0, s>>>(x, v, g);
+    return cudaGetLastError();
+  }
+
+#define MPDG_INST(T)                                                                                         \
+  template cudaError_t cg_init<T>(const T *, const T *, T *, CGState *, double *, Reducer, long long, cudaStream_t); \
+  template cudaError_t cg_update_p<T>(const T *, const T *, T *, const CGState *, long long, cudaStream_t);      \
+  template cudaError_t cg_alpha<T>(const T *, const T *, CGState *, Reducer, long long, cudaStream_t);          \
+  template cudaError_t cg_update_xr<T>(T *, T *, const T *, const T *, const T *, CGState *, double *, Reducer,  \
+                                       long long, cudaStream_t);                                                \
+  template cudaError_t vec_fill<T>(T *, T, long long, cudaStream_t);                                            \
+  template cudaError_t vec_axpby<T>(T *, double, const T *, double, const T *, long long, cudaStream_t);        \
+  template cudaError_t vec_multidot<T>(const T *const *, const T *const *, int, long long, double *, Reducer,    \
+                                       cudaStream_t);                                                           \
+  template cudaError_t vec_scale<T>(T *, const T *, const T *, long long, cudaStream_t);                        \
+  template cudaError_t vec_multiaxpy<T>(T *, const T *const *, const double *, int, long long, double,          \
+                                        cudaStream_t);                                                          \
+  template cudaError_t vec_dots_against<T>(const T *, const T *const *, int, long long, double *, Reducer,       \
+                                           cudaStream_t);                                                       \
+  template cudaError_t vec_orth_update<T>(T *, const T *const *, const double *, int, long long, double *,      \
+                                          Reducer, cudaStream_t);                                               \
+  template cudaError_t vec_invert<T>(T *, double, long long, cudaStream_t);                                     \
+  template cudaError_t vec_absmax<T>(const T *, long long, double *, Reducer, cudaStream_t);                    \
+  template cudaError_t vec_invert_rel<T>(T *, const double *, long long, cudaStream_t);                         \
+  template cudaError_t vec_set_constrained<T>(T *, T, const GridDesc &, cudaStream_t);
+  MPDG_INST(double)
+  MPDG_INST(float)
+#undef MPDG_INST
+  template cudaError_t vec_convert<float, double>(float *, const double *, long long, cudaStream_t);
+  template cudaError_t vec_convert<double, float>(double *, const float *, long long, cudaStream_t);
+} // namespace mpdg

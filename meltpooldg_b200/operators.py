@@ -1,0 +1,255 @@
+"""Host-side mirror of MeltPoolDG's matrix-free operator / solver interface over the C ABI.
+
+Names and semantics follow the reference:
+  * OperatorMatrixFree (include/meltpooldg/core/operator_base.hpp:189-283): vmult, create_rhs,
+    compute_inverse_diagonal_from_matrixfree, reset_time_increment, reset_dof_index, pre/post/reinit
+  * HeatDiffuseOperator  -> HeatDiffuseMultiPhaseOperator (source/heat/heat_diffuse_operator.cpp)
+  * AdvectionDiffusionOperator (source/level_set/advection_diffusion_operator.cpp)
+  * LinearSolverData / LinearSolver.solve (include/meltpooldg/linear_algebra/linear_solver_data.hpp,
+    linear_solver.hpp:26-134): ReductionControl(max_iterations, abs_tolerance, rel_tolerance);
+    non-convergence raises NoConvergence.
+Vectors are torch tensors on the CUDA device (torch only provides device memory); their entries
+are in lexicographic lattice order.  Every computation runs in libmpdg_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import MpdgError, NoConvergence, ZeroTimeIncrement, check, lib  # noqa: F401
+
+
+@dataclass
+class Mesh:
+    """Structured box of cells[0] x cells[1] x cells[2] axis-aligned hexahedra with FE_Q(degree)."""
+
+    degree: int
+    cells: Sequence[int]
+    origin: Sequence[float] = (0.0, 0.0, 0.0)
+    length: Sequence[float] = (1.0, 1.0, 1.0)
+    dirichlet_faces: int = 0
+    dirichlet_mask: Optional[np.ndarray] = None  # uint8 per DoF (nonzero = constrained)
+
+    @property
+    def n(self):
+        return tuple(self.degree * c + 1 for c in self.cells)
+
+    @property
+    def ndofs(self) -> int:
+        a, b, c = self.n
+        return a * b * c
+
+    @property
+    def ncells(self) -> int:
+        return int(np.prod(self.cells))
+
+    def _desc(self) -> L.MeshDesc:
+        d = L.MeshDesc()
+        d.degree = int(self.degree)
+        for i in range(3):
+            d.cells[i] = int(self.cells[i])
+            d.origin[i] = float(self.origin[i])
+            d.length[i] = float(self.length[i])
+        d.dirichlet_faces = int(self.dirichlet_faces)
+        if self.dirichlet_mask is not None:
+            self._mask = np.ascontiguousarray(self.dirichlet_mask, dtype=np.uint8)
+            if self._mask.size != self.ndofs:
+                raise ValueError("dirichlet_mask must have one entry per DoF")
+            d.dirichlet_mask = self._mask.ctypes.data
+        else:
+            d.dirichlet_mask = None
+        return d
+
+
+def _ptr(t) -> Optional[int]:
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("vectors must be contiguous CUDA tensors")
+    return t.data_ptr()
+
+
+class OperatorMatrixFree:
+    """Common handle logic; see include/meltpooldg/core/operator_base.hpp:189-283."""
+
+    def __init__(self, mesh: Mesh, params: L.OpParams, stream=None):
+        self.mesh = mesh
+        self._params = params
+        h = C.c_void_p()
+        check(lib().mpdg_op_create(C.byref(mesh._desc()), C.byref(params), C.byref(h)))
+        self._h = h
+        if stream is not None:
+            check(lib().mpdg_op_set_stream(self._h, C.c_void_p(stream)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().mpdg_op_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
+            self._h = None
+
+    def set_stream(self, stream_handle: int) -> None:
+        check(lib().mpdg_op_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    @property
+    def n_dofs(self) -> int:
+        return lib().mpdg_op_n_dofs(self._h)
+
+    # OperatorBase
+    def reset_time_increment(self, dt: float) -> None:
+        check(lib().mpdg_op_reset_time_increment(self._h, float(dt)))
+
+    def reset_dof_index(self, with_dirichlet: bool) -> None:
+        check(lib().mpdg_op_reset_dof_index(self._h, 1 if with_dirichlet else 0))
+
+    def pre(self) -> None:  # ghost updates: nothing to do on one device
+        pass
+
+    def post(self) -> None:
+        pass
+
+    def reinit(self) -> None:
+        pass
+
+    # OperatorMatrixFree
+    def vmult(self, dst, src) -> None:
+        import torch
+
+        if src.dtype == torch.float64:
+            check(lib().mpdg_op_vmult(self._h, _ptr(dst), _ptr(src)))
+        elif src.dtype == torch.float32:
+            check(lib().mpdg_op_vmult_f32(self._h, _ptr(dst), _ptr(src)))
+        else:
+            raise TypeError("vmult needs float64 or float32 vectors")
+
+    def vmult_add(self, dst, src, scale: float = 1.0) -> None:
+        check(lib().mpdg_op_vmult_add(self._h, _ptr(dst), _ptr(src), float(scale)))
+
+    def residual(self, r, b, x) -> None:
+        check(lib().mpdg_op_residual(self._h, _ptr(r), _ptr(b), _ptr(x)))
+
+    def vmult_host(self, dst: np.ndarray, src: np.ndarray) -> None:
+        assert dst.dtype == np.float64 and src.dtype == np.float64
+        check(lib().mpdg_op_vmult_host(self._h, dst.ctypes.data, src.ctypes.data))
+
+    def compute_inverse_diagonal_from_matrixfree(self, diag) -> None:
+        import torch
+
+        if diag.dtype == torch.float64:
+            check(lib().mpdg_op_compute_inverse_diagonal(self._h, _ptr(diag)))
+        else:
+            check(lib().mpdg_op_compute_inverse_diagonal_f32(self._h, _ptr(diag)))
+
+    def create_rhs(self, dst, a, b=None, c=None) -> None:
+        check(lib().mpdg_op_create_rhs(self._h, _ptr(dst), _ptr(a), _ptr(b), _ptr(c)))
+
+    def device_errors(self) -> int:
+        return lib().mpdg_op_device_errors(self._h)
+
+
+class HeatDiffuseOperator(OperatorMatrixFree):
+    """(rho c_p/dt) M + div(k grad) -- HeatDiffuseMultiPhaseOperator, single phase, no velocity."""
+
+    def __init__(self, mesh: Mesh, rho_cp: float = 1.0, dt: float = 1.0, conductivity: float = 1.0,
+                 conductivity_cells: Optional[np.ndarray] = None, stream=None):
+        p = L.OpParams()
+        p.kind = L.MPDG_HEAT
+        p.rho_cp, p.dt, p.conductivity = float(rho_cp), float(dt), float(conductivity)
+        if conductivity_cells is not None:
+            self._k = np.ascontiguousarray(conductivity_cells, dtype=np.float64)
+            if self._k.size != mesh.ncells:
+                raise ValueError("conductivity_cells must have one entry per cell")
+            p.conductivity_cells = self._k.ctypes.data
+        super().__init__(mesh, p, stream)
+
+    def set_conductivity(self, k_cells_device) -> None:
+        check(lib().mpdg_op_set_conductivity(self._h, _ptr(k_cells_device)))
+
+
+class AdvectionDiffusionOperator(OperatorMatrixFree):
+    """M/dt + theta (v.grad + eps K) with an affine velocity v(x) = v0 + G x."""
+
+    def __init__(self, mesh: Mesh, dt: float, theta: float = 1.0, diffusivity: float = 0.0,
+                 velocity: Sequence[float] = (0.0,) * 12, stream=None):
+        p = L.OpParams()
+        p.kind = L.MPDG_ADVDIFF
+        p.dt, p.theta, p.diffusivity = float(dt), float(theta), float(diffusivity)
+        for i in range(12):
+            p.velocity[i] = float(velocity[i])
+        super().__init__(mesh, p, stream)
+
+
+@dataclass
+class LinearSolverData:
+    """include/meltpooldg/linear_algebra/linear_solver_data.hpp:37-47 (defaults preserved)."""
+
+    solver_type: str = "GMRES"  # "CG" | "GMRES"
+    preconditioner_type: str = "Identity"  # "Identity" | "Diagonal"
+    max_iterations: int = 10000
+    rel_tolerance: float = 1e-12
+    abs_tolerance: float = 1e-20
+    restart: int = 30
+
+
+@dataclass
+class SolveStats:
+    iterations: int
+    initial_residual: float
+    final_residual: float
+    history: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    inner_iterations: int = 0
+
+
+class LinearSolver:
+    """LinearSolver::solve (include/meltpooldg/linear_algebra/linear_solver.hpp:26-134)."""
+
+    @staticmethod
+    def _params(data: LinearSolverData) -> L.SolverParams:
+        p = L.SolverParams()
+        p.solver = L.MPDG_CG if data.solver_type.upper() == "CG" else L.MPDG_GMRES
+        p.precond = L.MPDG_PRECOND_JACOBI if data.preconditioner_type in ("Diagonal", "Jacobi") else L.MPDG_PRECOND_IDENTITY
+        p.max_it, p.restart = int(data.max_iterations), int(data.restart)
+        p.abs_tol, p.rel_tol = float(data.abs_tolerance), float(data.rel_tolerance)
+        return p
+
+    @staticmethod
+    def solve(op: OperatorMatrixFree, solution, rhs, data: LinearSolverData, history: bool = False) -> SolveStats:
+        import torch
+
+        p = LinearSolver._params(data)
+        info = L.SolveInfo()
+        hist = np.zeros(data.max_iterations + 2) if history else None
+        if hist is not None:
+            info.history = hist.ctypes.data
+            info.history_capacity = hist.size
+        fn = lib().mpdg_solve if solution.dtype == torch.float64 else lib().mpdg_solve_f32
+        rc = fn(op._h, _ptr(solution), _ptr(rhs), C.byref(p), C.byref(info))
+        stats = SolveStats(info.iterations, info.initial_residual, info.final_residual,
+                           hist[: info.iterations + 1] if hist is not None else np.zeros(0))
+        check(rc)
+        return stats
+
+    @staticmethod
+    def solve_mixed(op: HeatDiffuseOperator, solution, rhs, outer_rel_tol: float = 1e-8,
+                    inner_rel_tol: float = 1e-4, max_outer: int = 50, max_inner: int = 10000,
+                    solver: str = "CG", restart: int = 30) -> SolveStats:
+        p = L.MixedParams()
+        p.outer_rel_tol, p.inner_rel_tol = float(outer_rel_tol), float(inner_rel_tol)
+        p.max_outer, p.max_inner = int(max_outer), int(max_inner)
+        p.solver = L.MPDG_CG if solver.upper() == "CG" else L.MPDG_GMRES
+        p.restart = int(restart)
+        info = L.SolveInfo()
+        hist = np.zeros(max_outer + 2)
+        info.history = hist.ctypes.data
+        info.history_capacity = hist.size
+        rc = lib().mpdg_solve_mixed(op._h, _ptr(solution), _ptr(rhs), C.byref(p), C.byref(info))
+        stats = SolveStats(info.iterations, info.initial_residual, info.final_residual,
+                           hist[: info.iterations + 1], info.inner_iterations)
+        check(rc)
+        return stats

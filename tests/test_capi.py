@@ -1,0 +1,60 @@
+"""CPU checks of the C ABI library: it loads and exports every declared entry point."""
+import ctypes
+import os
+import re
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for fn in os.listdir(inc):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(inc, fn)).read()
+            names |= set(re.findall(r"MPDG_API\s+[\w\s\*]+?\b(mpdg_\w+)\s*\(", txt))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert "mpdg_op_vmult" in names and "mpdg_solve" in names and len(names) >= 20
+
+
+def test_library_loads_and_exports_every_symbol():
+    from meltpooldg_b200 import _lib
+    from meltpooldg_b200.build import build
+
+    build()
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_signatures_cover_header():
+    from meltpooldg_b200 import _lib
+
+    bound = {n for n, _, _ in _lib.SIGNATURES + _lib.OPTIONAL}
+    assert declared_symbols() <= bound
+
+
+def test_invalid_arguments_rejected_without_gpu():
+    """Argument checks run before any CUDA call."""
+    from meltpooldg_b200 import _lib
+
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    mesh = _lib.MeshDesc()
+    mesh.degree = 7
+    for d in range(3):
+        mesh.cells[d] = 2
+        mesh.length[d] = 1.0
+    p = _lib.OpParams()
+    p.kind = _lib.MPDG_HEAT
+    p.dt = 1.0
+    assert L.mpdg_op_create(ctypes.byref(mesh), ctypes.byref(p), ctypes.byref(h)) == _lib.MPDG_ERR_UNSUPPORTED
+    mesh.degree = 2
+    p.dt = 0.0
+    assert L.mpdg_op_create(ctypes.byref(mesh), ctypes.byref(p), ctypes.byref(h)) == _lib.MPDG_ERR_ZERO_DT
+    assert b"ExcZeroTimeIncrement" in L.mpdg_last_error()
+    assert L.mpdg_op_vmult(None, None, None) == _lib.MPDG_ERR_ARG

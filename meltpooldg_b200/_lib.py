@@ -9,7 +9,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmpdg_b200.so")
+LIB_PATH = os.environ.get("MPDG_LIB_PATH") or os.path.join(HERE, "libmpdg_b200.so")
 
 MPDG_OK = 0
 MPDG_ERR_ARG = 1

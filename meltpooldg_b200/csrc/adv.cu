@@ -128,8 +128,7 @@ namespace mpdg
     static constexpr int  BX = 8, BY = 8, BZ = (K == 1 ? 8 : 4);
     static constexpr int  NT = BX * BY * BZ;
     using BR                 = Brick<K, BX, BY, BZ, NT>;
-    static constexpr int  SH = N * N * N - K * K * K;
-    static constexpr size_t bytes = sizeof(T) * ((size_t)BR::NPTS + (size_t)SH * BR::NT);
+    static constexpr size_t bytes = sizeof(T) * 2 * (size_t)BR::NPTS; // staged input + accumulator
   };
 
   template <int K, typename T, OutMode MODE>
@@ -141,9 +140,8 @@ namespace mpdg
     constexpr int  N      = K + 1, NT = BR::NT, NP = BR::NPTS, PX = BR::PX, PY = BR::PY;
     constexpr int  BX     = BR::BX, BY = BR::BY;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *const s_src   = reinterpret_cast<T *>(smem_raw);
-    T *const s_dst   = s_src;
-    T *const s_shell = s_src + NP;
+    T *const s_src = reinterpret_cast<T *>(smem_raw);
+    T *const s_dst = s_src + NP;
     __shared__ unsigned s_ticket;
     if (a.skip != nullptr && *a.skip != 0)
       return;
@@ -151,12 +149,13 @@ namespace mpdg
     BR br;
     if (!brick_begin<BR, T, MODE>(br, a.g, a.s, a.dst, a.b, &s_ticket))
       return;
+    for (int p = threadIdx.x; p < NP; p += NT)
+      s_dst[p] = T(0);
     brick_stage(br, a.src, a.mask_src != 0, s_src);
 
     const int  tx = threadIdx.x % BX, ty = (threadIdx.x / BX) % BY, tz = threadIdx.x / (BX * BY);
     const int  cx = br.c0[0] + tx, cy = br.c0[1] + ty, cz = br.c0[2] + tz;
     const bool valid = cx < a.g.m[0] && cy < a.g.m[1] && cz < a.g.m[2];
-    const int  lox = tx == 0 ? 0 : 1, loy = ty == 0 ? 0 : 1, loz = tz == 0 ? 0 : 1;
     const int  base = (K * tz) * PY * PX + (K * ty) * PX + K * tx;
 
     const T *tb  = adv_table<T>(K);
@@ -223,53 +222,14 @@ namespace mpdg
         sweep<T, N, 2, true>(R, tB);
         sweep<T, N, 1, true>(R, tB);
         sweep<T, N, 0, true>(R, tB);
-      }
-    __syncthreads();
-    if (valid)
-      {
+        // cells sharing a lattice point add into the brick accumulator concurrently
 #pragma unroll
         for (int l = 0; l < N; ++l)
 #pragma unroll
           for (int j = 0; j < N; ++j)
 #pragma unroll
             for (int i = 0; i < N; ++i)
-              {
-                const bool owned = (i >= lox) && (j >= loy) && (l >= loz);
-                T *p = owned ? s_dst + (base + l * PY * PX + j * PX + i)
-                             : s_shell + (shell_index<N>(i, j, l) * NT + threadIdx.x);
-                *p = R[(l * N + j) * N + i];
-              }
-      }
-    __syncthreads();
-    if (valid)
-      {
-        const bool ux = tx + 1 < BX && cx + 1 < a.g.m[0];
-        const bool uy = ty + 1 < BY && cy + 1 < a.g.m[1];
-        const bool uz = tz + 1 < BR::BZ && cz + 1 < a.g.m[2];
-#pragma unroll
-        for (int l = 0; l < N; ++l)
-#pragma unroll
-          for (int j = 0; j < N; ++j)
-#pragma unroll
-            for (int i = 0; i < N; ++i)
-              {
-                if (i != K && j != K && l != K)
-                  continue;
-                T sum = T(0);
-#pragma unroll
-                for (int s = 1; s < 8; ++s)
-                  {
-                    const int sx = s & 1, sy = (s >> 1) & 1, sz = (s >> 2) & 1;
-                    if ((sx && i != K) || (sy && j != K) || (sz && l != K))
-                      continue;
-                    const bool ok = (!sx || ux) && (!sy || uy) && (!sz || uz);
-                    const int  nb = threadIdx.x + sx + sy * BX + sz * BX * BY;
-                    const T    v  = s_shell[shell_index<N>(sx ? 0 : i, sy ? 0 : j, sz ? 0 : l) * NT + (ok ? nb : threadIdx.x)];
-                    sum += ok ? v : T(0);
-                  }
-                if ((i >= lox) && (j >= loy) && (l >= loz))
-                  s_dst[base + l * PY * PX + j * PX + i] += sum;
-              }
+              atomicAdd(s_dst + (base + l * PY * PX + j * PX + i), R[(l * N + j) * N + i]);
       }
     __syncthreads();
     brick_end<BR, T, MODE>(br, a.g, a.s, s_dst, a.dst, a.b);

@@ -6,10 +6,9 @@
 //    shared memory with cp.async (all copies in flight at once, zero-fill for points outside the
 //    domain).  Dirichlet-constrained points read as 0 when the operator reads "with constraints"
 //    (deal.II read_dof_values); plain reads otherwise (read_dof_values_plain).
-//  * Ownership: inside a brick every lattice point has exactly one owner cell.  A cell owns its
-//    local points with index in [lo_d, K] per dimension, lo_d = 0 for the first cell of the brick
-//    in d and 1 otherwise.  The other points of a cell (index 0 where lo_d = 1) form its "shell";
-//    it publishes them to shared memory and the owner (a lower neighbour) adds them.
+//  * In-brick reduction: cells add their local outputs into a shared-memory accumulator of the
+//    brick's lattice points (shared-memory atomics; contention is rare because cells only share
+//    the points of common faces).
 //  * Brick faces: a lattice point on the low face of a brick (that has a lower neighbour brick)
 //    belongs to that lower brick; a point on the high face belongs to this brick but also gets
 //    contributions from the upper brick.  Those points are combined with global atomics; all
@@ -220,46 +219,54 @@ namespace mpdg
       }
   }
 
-  // Initialise the owned high-face points of the brick (Set: 0, BPlus: b) and publish the flag.
-  // Only the three high faces are visited (edge points twice, with the same value).
+  // Initialise the face points the brick owns (Set: 0, BPlus: b) and publish the flag.  A brick owns
+  // its high faces (also where they are the domain boundary) and, at the domain's low boundary, its
+  // low faces; low faces shared with a lower brick belong to that brick.  Edge points are visited
+  // up to three times with the same value.
   template <class BR, typename T, OutMode MODE>
   __device__ __forceinline__ void
   brick_init_publish(const BR &br, const SyncDesc &s, T *dst, const T *bvec)
   {
     static_assert(MODE != OutMode::Add, "Add mode needs no initialisation");
     constexpr int F0 = BR::PY * BR::PZ, F1 = BR::PX * BR::PZ, F2 = BR::PX * BR::PY;
-    for (int f = threadIdx.x; f < F0 + F1 + F2; f += BR::NT)
+    for (int f = threadIdx.x; f < 2 * (F0 + F1 + F2); f += BR::NT)
       {
-        int px, py, pz;
-        if (f < F0)
+        const int  side = f / (F0 + F1 + F2); // 0: low faces, 1: high faces
+        const int  q    = f % (F0 + F1 + F2);
+        int        px, py, pz;
+        bool       use;
+        if (q < F0)
           {
-            if (!br.hi_sh[0])
-              continue;
-            px = BR::PX - 1, py = f % BR::PY, pz = f / BR::PY;
+            py  = q % BR::PY;
+            pz  = q / BR::PY;
+            px  = side ? br.nv[0] - 1 : 0;
+            use = side ? true : !br.lo_sh[0];
           }
-        else if (f < F0 + F1)
+        else if (q < F0 + F1)
           {
-            if (!br.hi_sh[1])
-              continue;
-            const int q = f - F0;
-            px = q % BR::PX, py = BR::PY - 1, pz = q / BR::PX;
+            px  = (q - F0) % BR::PX;
+            pz  = (q - F0) / BR::PX;
+            py  = side ? br.nv[1] - 1 : 0;
+            use = side ? true : !br.lo_sh[1];
           }
         else
           {
-            if (!br.hi_sh[2])
-              continue;
-            const int q = f - F0 - F1;
-            px = q % BR::PX, py = q / BR::PX, pz = BR::PZ - 1;
+            px  = (q - F0 - F1) % BR::PX;
+            py  = (q - F0 - F1) / BR::PX;
+            pz  = side ? br.nv[2] - 1 : 0;
+            use = side ? true : !br.lo_sh[2];
           }
-        if (!br.inside(px, py, pz) || br.low_shared(px, py, pz))
+        if (!use || !br.inside(px, py, pz) || br.low_shared(px, py, pz))
           continue;
         const int idx = br.index(px, py, pz);
         dst[idx]      = (MODE == OutMode::BPlus) ? bvec[idx] : T(0);
       }
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0)
-      st_release(s.flags + br.id, s.epoch);
+      {
+        __threadfence();
+        st_release(s.flags + br.id, s.epoch);
+      }
   }
 
   // Stage the brick's lattice points of src into shared memory (row walk, cp.async).

@@ -18,7 +18,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/mpdg_gpu.h"
+#include "mpdg_gpu.h"
 #include "kernels.h"
 
 using namespace mpdg;
@@ -220,6 +220,7 @@ namespace
         h.b      = b;
         h.mask_src = mask_src;
         h.skip     = skip;
+        h.march    = op->d_mask == nullptr;
         MPDG_CUDA(heat_apply<T>(h, op->stream));
       }
     else
@@ -550,7 +551,7 @@ mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op
   for (int i = 0; i < 12; ++i)
     op->vel[i] = params->velocity[i];
   if (op->kind == MPDG_HEAT)
-    heat_brick_shape<double>(op->degree, op->brick);
+    heat_brick_shape<double>(op->degree, op->brick, mesh->dirichlet_mask == nullptr);
   else
     adv_brick_shape<double>(op->degree, op->brick);
   for (int d = 0; d < 3; ++d)

@@ -7,8 +7,10 @@
 // Work decomposition: one CTA per brick of cells (brick.cuh).  For k <= 2 one thread holds a whole
 // cell (n^3 <= 27 values) in registers.  For k >= 3 a cell is split over two threads in different
 // warps by the reflection parity of its z-modes: the "odd" thread transforms the floor(n/2) odd
-// z-planes (u_l - u_{n-1-l}) and leaves its result in shared memory, the "even" thread transforms
-// the ceil(n/2) even z-planes (u_l + u_{n-1-l}, u_mid) and combines both into the nodal output.
+// z-planes (u_l - u_{n-1-l}), the "even" thread the ceil(n/2) even z-planes (u_l + u_{n-1-l},
+// u_mid); each adds its part of the nodal output (out_l = E_l + O_l, out_{n-1-l} = E_l - O_l).
+// Cells add their outputs into a shared-memory accumulator of the brick with shared-memory atomics
+// (no ordering between cells that share lattice points is needed).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -16,6 +18,7 @@
 
 #include "brick.cuh"
 #include "kernels.h"
+#include "march.cuh"
 #include "sumfac.cuh"
 
 namespace mpdg
@@ -85,9 +88,7 @@ namespace mpdg
     static constexpr int  NC  = S::BX * S::BY * S::BZ;
     static constexpr int  NT  = TWO ? 2 * NC : NC;
     using BR                  = Brick<K, S::BX, S::BY, S::BZ, NT>;
-    static constexpr int  SH  = N * N * N - K * K * K;
-    static constexpr int  ODD = TWO ? NO * N * N : 0;
-    static constexpr size_t bytes = sizeof(T) * ((size_t)BR::NPTS + (size_t)(ODD + SH) * NC);
+    static constexpr size_t bytes = sizeof(T) * 2 * (size_t)BR::NPTS; // staged input + accumulator
   };
 
   template <int K, typename T, OutMode MODE>
@@ -98,12 +99,10 @@ namespace mpdg
     using BR         = typename L::BR;
     constexpr int N  = K + 1, NE = L::NE, NO = L::NO;
     constexpr int NC = L::NC, PX = BR::PX, PY = BR::PY;
-    constexpr int BX = BR::BX, BY = BR::BY, BZ = BR::BZ;
+    constexpr int BX = BR::BX, BY = BR::BY;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *const s_src   = reinterpret_cast<T *>(smem_raw); // staging; output accumulation later
-    T *const s_dst   = s_src;
-    T *const s_odd   = s_src + BR::NPTS;                // two-pass scratch (column per cell)
-    T *const s_shell = s_src + BR::NPTS + L::ODD * NC;  // published shell points (column per cell)
+    T *const s_src = reinterpret_cast<T *>(smem_raw); // staged input brick
+    T *const s_dst = s_src + BR::NPTS;                // brick accumulator
     __shared__ unsigned s_ticket;
     if (a.skip != nullptr && *a.skip != 0)
       return;
@@ -111,6 +110,8 @@ namespace mpdg
     BR br;
     if (!brick_begin<BR, T, MODE>(br, a.g, a.s, a.dst, a.b, &s_ticket))
       return;
+    for (int p = threadIdx.x; p < BR::NPTS; p += BR::NT)
+      s_dst[p] = T(0);
     brick_stage(br, a.src, a.mask_src != 0, s_src);
 
     const int  cell = threadIdx.x % NC;       // cell of the brick handled by this thread
@@ -118,7 +119,6 @@ namespace mpdg
     const int  tx = cell % BX, ty = (cell / BX) % BY, tz = cell / (BX * BY);
     const int  cx = br.c0[0] + tx, cy = br.c0[1] + ty, cz = br.c0[2] + tz;
     const bool valid = cx < a.g.m[0] && cy < a.g.m[1] && cz < a.g.m[2];
-    const int  lox = tx == 0 ? 0 : 1, loy = ty == 0 ? 0 : 1, loz = tz == 0 ? 0 : 1;
     const int  base = (K * tz) * PY * PX + (K * ty) * PX + K * tx;
     T          kc   = T(0);
     if (valid)
@@ -149,18 +149,16 @@ namespace mpdg
               }
           }
     };
-    // owned points go to the brick accumulator, shell points to this cell's shell column
-    auto emit = [&](const int i, const int j, const int l, const T v) {
-      const bool owned = (i >= lox) && (j >= loy) && (l >= loz);
-      T *p = owned ? s_dst + (base + l * PY * PX + j * PX + i) : s_shell + (shell_index<N>(i, j, l) * NC + cell);
-      *p   = v;
+    // cells sharing a lattice point add into the brick accumulator concurrently
+    auto add_point = [&](const int i, const int j, const int l, const T v) {
+      atomicAdd(s_dst + (base + l * PY * PX + j * PX + i), v);
     };
 
-    if constexpr (!L::TWO)
+    if (valid)
       {
-        T u[N * N * N];
-        if (valid)
+        if constexpr (!L::TWO)
           {
+            T u[N * N * N];
 #pragma unroll
             for (int l = 0; l < N; ++l)
 #pragma unroll
@@ -177,26 +175,19 @@ namespace mpdg
             for (int q = 0; q < N * N; ++q)
               bwd_line<T, N, N * N>(u, q, we, wo);
             xy_planes<T, N, N, false>(u, we, wo);
-          }
-        __syncthreads(); // all reads of s_src done: s_dst may overlay it
-        if (valid)
-          {
 #pragma unroll
             for (int l = 0; l < N; ++l)
 #pragma unroll
               for (int j = 0; j < N; ++j)
 #pragma unroll
                 for (int i = 0; i < N; ++i)
-                  emit(i, j, l, u[(l * N + j) * N + i]);
+                  add_point(i, j, l, u[(l * N + j) * N + i]);
           }
-      }
-    else
-      {
-        T e[NE * N * N];
-        if (valid && role == 1)
+        else if (role == 1)
           {
-            // odd z-modes: o_k = u_k - u_{N-1-k}; result O_k to the scratch column of this cell
-            T *v = e; // reuse the register array (NO <= NE planes)
+            // odd z-modes: o_k = u_k - u_{N-1-k}; the result O_k adds +O_k to plane k and -O_k to
+            // plane N-1-k of the nodal output
+            T v[NO * N * N];
 #pragma unroll
             for (int k = 0; k < NO; ++k)
 #pragma unroll
@@ -240,12 +231,16 @@ namespace mpdg
                   }
 #pragma unroll
                 for (int k = 0; k < NO; ++k)
-                  s_odd[(k * N * N + q) * NC + cell] = t[k];
+                  {
+                    add_point(q % N, q / N, k, t[k]);
+                    add_point(q % N, q / N, N - 1 - k, -t[k]);
+                  }
               }
           }
-        else if (valid)
+        else
           {
-            // even z-modes: e_k = u_k + u_{N-1-k}, e_mid = u_mid; kept in registers
+            // even z-modes: e_k = u_k + u_{N-1-k}, e_mid = u_mid; E_k goes to planes k and N-1-k
+            T e[NE * N * N];
 #pragma unroll
             for (int k = 0; k < NE; ++k)
 #pragma unroll
@@ -292,68 +287,73 @@ namespace mpdg
                   }
 #pragma unroll
                 for (int k = 0; k < NE; ++k)
-                  e[k * N * N + q] = t[k];
+                  {
+                    add_point(q % N, q / N, k, t[k]);
+                    if (k < N / 2)
+                      add_point(q % N, q / N, N - 1 - k, t[k]);
+                  }
               }
           }
-        __syncthreads(); // s_src dead, odd results complete
-        if (valid && role == 0)
-          {
-#pragma unroll
-            for (int k = 0; k < N / 2; ++k)
-#pragma unroll
-              for (int j = 0; j < N; ++j)
-#pragma unroll
-                for (int i = 0; i < N; ++i)
-                  {
-                    const T E = e[(k * N + j) * N + i];
-                    const T O = s_odd[((k * N + j) * N + i) * NC + cell];
-                    emit(i, j, k, E + O);
-                    emit(i, j, N - 1 - k, E - O);
-                  }
-            if constexpr (N % 2 == 1)
-#pragma unroll
-              for (int j = 0; j < N; ++j)
-#pragma unroll
-                for (int i = 0; i < N; ++i)
-                  emit(i, j, N / 2, e[((N / 2) * N + j) * N + i]);
-          }
-      }
-    __syncthreads();
-
-    // ---- add the shells of in-brick upper neighbours into the owned points
-    if (valid && role == 0)
-      {
-        const bool ux = tx + 1 < BX && cx + 1 < a.g.m[0];
-        const bool uy = ty + 1 < BY && cy + 1 < a.g.m[1];
-        const bool uz = tz + 1 < BZ && cz + 1 < a.g.m[2];
-#pragma unroll
-        for (int l = 0; l < N; ++l)
-#pragma unroll
-          for (int j = 0; j < N; ++j)
-#pragma unroll
-            for (int i = 0; i < N; ++i)
-              {
-                if (i != K && j != K && l != K)
-                  continue;
-                T sum = T(0);
-#pragma unroll
-                for (int s = 1; s < 8; ++s)
-                  {
-                    const int sx = s & 1, sy = (s >> 1) & 1, sz = (s >> 2) & 1;
-                    if ((sx && i != K) || (sy && j != K) || (sz && l != K))
-                      continue;
-                    const bool ok = (!sx || ux) && (!sy || uy) && (!sz || uz);
-                    const int  nb = cell + sx + sy * BX + sz * BX * BY;
-                    const T    v  = s_shell[shell_index<N>(sx ? 0 : i, sy ? 0 : j, sz ? 0 : l) * NC + (ok ? nb : cell)];
-                    sum += ok ? v : T(0);
-                  }
-                const bool owned = (i >= lox) && (j >= loy) && (l >= loz);
-                if (owned)
-                  s_dst[base + l * PY * PX + j * PX + i] += sum;
-              }
       }
     __syncthreads();
     brick_end<BR, T, MODE>(br, a.g, a.s, s_dst, a.dst, a.b);
+  }
+
+  // ---- k <= 2: column-marching apply (march.cuh) with the fast-diagonalisation cell operator
+  template <int K, typename T>
+  struct HeatCellOp
+  {
+    static constexpr int N = K + 1, NE = (N + 1) / 2, NO = N / 2;
+    const HeatArgs<T, N> &a;
+    __device__ __forceinline__ void
+    apply(T *u, bool valid, int cx, int cy, int cz) const
+    {
+      T kc = T(0);
+      if (valid)
+        {
+          const long long c = (long long)cx + (long long)a.g.m[0] * ((long long)cy + (long long)a.g.m[1] * cz);
+          kc                = a.kscale * (a.kcell ? a.kcell[c] : a.kconst);
+        }
+      const T *tb  = fd_table<T>(K);
+      const T *we  = tb;
+      const T *wo  = tb + NE * NE;
+      const T *lam = tb + NE * NE + NO * NO;
+      const T  kcx = kc * a.cx, kcy = kc * a.cy, kcz = kc * a.cz, alpha = a.alpha;
+      xy_planes<T, N, N, true>(u, we, wo);
+#pragma unroll
+      for (int q = 0; q < N * N; ++q)
+        fwd_line<T, N, N * N>(u, q, we, wo);
+#pragma unroll
+      for (int c = 0; c < N; ++c)
+        {
+          const T tz = fma(kcz, lam[c], alpha);
+#pragma unroll
+          for (int b = 0; b < N; ++b)
+            {
+              const T tyz = fma(kcy, lam[b], tz);
+#pragma unroll
+              for (int aa = 0; aa < N; ++aa)
+                u[(c * N + b) * N + aa] *= fma(kcx, lam[aa], tyz);
+            }
+        }
+#pragma unroll
+      for (int q = 0; q < N * N; ++q)
+        bwd_line<T, N, N * N>(u, q, we, wo);
+      xy_planes<T, N, N, false>(u, we, wo);
+    }
+  };
+
+  template <int K, typename T, OutMode MODE>
+  __global__ void __launch_bounds__(MarchShape<K>::NT)
+  heat_march_kernel(const __grid_constant__ HeatArgs<T, K + 1> a)
+  {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned s_ticket;
+    if (a.skip != nullptr && *a.skip != 0)
+      return;
+    HeatCellOp<K, T> op{a};
+    march_body<K, T, MODE>(a.g, a.s, a.src, a.dst, a.b, a.mask_src != 0, op, reinterpret_cast<T *>(smem_raw),
+                           &s_ticket);
   }
 
   // ---- diagonal: closed-form per-cell entries gathered per DoF (deterministic, no atomics)
@@ -495,17 +495,35 @@ namespace mpdg
     a.b        = h.b;
     a.mask_src = h.mask_src;
     a.skip     = h.skip;
-    auto kern  = heat_apply_kernel<K, T, MODE>;
-    static thread_local bool attr_done = false;
-    if (!attr_done)
-      {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
-        if (e != cudaSuccess)
-          return e;
-        attr_done = true;
-      }
     const unsigned nbricks = (unsigned)h.grid.nbr[0] * h.grid.nbr[1] * h.grid.nbr[2];
-    kern<<<nbricks, L::BR::NT, L::bytes, stream>>>(a);
+    if constexpr (K <= 2)
+      if (h.grid.cmask == nullptr && h.march)
+      {
+        using ML  = MarchLayout<K, T>;
+        auto kern = heat_march_kernel<K, T, MODE>;
+        static thread_local bool attr_done = false;
+        if (!attr_done)
+          {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ML::bytes);
+            if (e != cudaSuccess)
+              return e;
+            attr_done = true;
+          }
+        kern<<<nbricks, ML::S::NT, ML::bytes, stream>>>(a);
+        return cudaGetLastError();
+      }
+    {
+        auto kern = heat_apply_kernel<K, T, MODE>;
+        static thread_local bool attr_done = false;
+        if (!attr_done)
+          {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
+            if (e != cudaSuccess)
+              return e;
+            attr_done = true;
+          }
+        kern<<<nbricks, L::BR::NT, L::bytes, stream>>>(a);
+      }
     return cudaGetLastError();
   }
 
@@ -515,8 +533,8 @@ namespace mpdg
   {
     switch (K)
       {
-        case 1: bx = HeatBrickShape<1, T>::BX; by = HeatBrickShape<1, T>::BY; bz = HeatBrickShape<1, T>::BZ; break;
-        case 2: bx = HeatBrickShape<2, T>::BX; by = HeatBrickShape<2, T>::BY; bz = HeatBrickShape<2, T>::BZ; break;
+        case 1: bx = MarchShape<1>::BX; by = MarchShape<1>::BY; bz = MarchShape<1>::BZ; break;
+        case 2: bx = MarchShape<2>::BX; by = MarchShape<2>::BY; bz = MarchShape<2>::BZ; break;
         case 3: bx = HeatBrickShape<3, T>::BX; by = HeatBrickShape<3, T>::BY; bz = HeatBrickShape<3, T>::BZ; break;
         default: bx = HeatBrickShape<4, T>::BX; by = HeatBrickShape<4, T>::BY; bz = HeatBrickShape<4, T>::BZ; break;
       }
@@ -524,9 +542,15 @@ namespace mpdg
 
   template <typename T>
   void
-  heat_brick_shape(int K, int shape[3])
+  heat_brick_shape(int K, int shape[3], bool march)
   {
     brick_shape<T>(K, shape[0], shape[1], shape[2]);
+    if (!march && K <= 2)
+      {
+        shape[0] = K == 1 ? HeatBrickShape<1, T>::BX : HeatBrickShape<2, T>::BX;
+        shape[1] = K == 1 ? HeatBrickShape<1, T>::BY : HeatBrickShape<2, T>::BY;
+        shape[2] = K == 1 ? HeatBrickShape<1, T>::BZ : HeatBrickShape<2, T>::BZ;
+      }
   }
 
   template <int K, typename T>
@@ -592,6 +616,6 @@ namespace mpdg
                                              bool, double, cudaStream_t);
   template cudaError_t heat_diagonal<float>(const GridDesc &, int, const HeatGeom &, double, const float *, float *,
                                             bool, double, cudaStream_t);
-  template void heat_brick_shape<double>(int, int[3]);
-  template void heat_brick_shape<float>(int, int[3]);
+  template void heat_brick_shape<double>(int, int[3], bool);
+  template void heat_brick_shape<float>(int, int[3], bool);
 } // namespace mpdg

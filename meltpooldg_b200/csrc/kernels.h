@@ -33,6 +33,7 @@ namespace mpdg
     const T    *b        = nullptr;
     int         mask_src = 1;
     const int  *skip     = nullptr; // device flag: return at once when nonzero
+    bool        march    = true;    // k <= 2: column-marching kernel (operator without per-DoF mask)
   };
 
   template <typename T>
@@ -43,7 +44,7 @@ namespace mpdg
                             T *diag, bool invert, double threshold, cudaStream_t s);
 
   template <typename T>
-  void heat_brick_shape(int K, int shape[3]);
+  void heat_brick_shape(int K, int shape[3], bool march);
 
   // ---- advection-diffusion (source/level_set/advection_diffusion_operator.cpp)
   struct AdvParams

@@ -134,6 +134,24 @@ typedef struct mpdg_mixed_params
   int32_t restart;         /* inner GMRES basis size                                       */
 } mpdg_mixed_params;
 
+typedef struct mpdg_adjoint_params
+{
+  int32_t n_steps;          /* implicit-Euler steps                                      */
+  int32_t checkpoint_every; /* forward states kept every checkpoint_every steps          */
+  double  cg_rel_tol;       /* relative tolerance of every Jacobi-CG solve               */
+  int32_t cg_max_it;
+  int32_t reserved;
+} mpdg_adjoint_params;
+
+typedef struct mpdg_adjoint_result
+{
+  double  objective;      /* J = 1/2 sum_n |T_n - T*_n|^2 (Euclidean, free DoFs)          */
+  double  grad_amplitude; /* dJ/dA                                                        */
+  int32_t forward_solves; /* including the recomputation between checkpoints             */
+  int32_t adjoint_solves;
+  int64_t cg_iterations;
+} mpdg_adjoint_result;
+
 typedef struct mpdg_op mpdg_op;
 
 /* Operator lifetime -- HeatDiffuseMultiPhaseOperator / AdvectionDiffusionOperator constructors */
@@ -184,6 +202,26 @@ MPDG_API int mpdg_solve_f32(mpdg_op *op, float *x, const float *b, const mpdg_so
    |r| <= outer_rel_tol |b|; inner: FP32 operator and vectors with Jacobi preconditioning solve
    A32 e = r to inner_rel_tol; x += e in FP64. */
 MPDG_API int mpdg_solve_mixed(mpdg_op *op, double *x, const double *b, const mpdg_mixed_params *params, mpdg_solve_info *info);
+
+/* Transient heat problem on a heat operator (rho c_p and dt from the operator, conductivity
+   k = exp(log_k) per cell, overwriting the operator's conductivity):
+     (rho c_p M / dt + K(k)) T_n = rho c_p M T_{n-1} / dt + A M qhat_n,  n = 1..n_steps,  T_0 = 0,
+   i.e. the implicit-Euler step of the heat equation with source A qhat_n read like the heat_source
+   of source/heat/heat_diffuse_operator.cpp:445-447,493-495.  No reference counterpart (the reference
+   has no adjoint).  Device arrays: log_k (n_cells), qhat (n_steps * n_dofs), T_target (n_steps *
+   n_dofs), grad_log_k (n_cells).
+   mpdg_adjoint_heat: J and its gradient by the discrete adjoint (A^T lam_n = (T_n - T*_n) + rho c_p
+   M lam_{n+1} / dt, dJ/dz_c = -sum_n k_c lam_n^T K_c T_n, dJ/dA = sum_n lam_n^T M qhat_n), with the
+   forward states checkpointed every checkpoint_every steps and recomputed between checkpoints.
+   grad_log_k == NULL evaluates J only. */
+MPDG_API int mpdg_adjoint_heat(mpdg_op *op, const double *log_k, const double *qhat, double amplitude,
+                               const double *T_target, const mpdg_adjoint_params *params, double *grad_log_k,
+                               mpdg_adjoint_result *result);
+/* Forward states T_1..T_n_steps of the same problem into T_out (n_steps * n_dofs, device). */
+MPDG_API int mpdg_heat_forward(mpdg_op *op, const double *log_k, const double *qhat, double amplitude,
+                               const mpdg_adjoint_params *params, double *T_out);
+/* Per-cell unit-conductivity stiffness form form_c = lam_c^T K_c T_c (device arrays). */
+MPDG_API int mpdg_heat_cell_stiffness_form(mpdg_op *op, const double *lam, const double *T, double *form);
 
 /* Number of error words raised by bounded device waits since the last call (and reset). */
 MPDG_API int mpdg_op_device_errors(mpdg_op *op);

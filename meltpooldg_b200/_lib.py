@@ -130,12 +130,12 @@ SIGNATURES = [
     ("mpdg_solve_f32", [P, P, P, C.POINTER(SolverParams), C.POINTER(SolveInfo)], C.c_int),
     ("mpdg_solve_mixed", [P, P, P, C.POINTER(MixedParams), C.POINTER(SolveInfo)], C.c_int),
     ("mpdg_op_device_errors", [P], C.c_int),
+    ("mpdg_adjoint_heat", [P, P, P, D, P, C.POINTER(AdjointParams), P, C.POINTER(AdjointResult)], C.c_int),
+    ("mpdg_heat_forward", [P, P, P, D, C.POINTER(AdjointParams), P], C.c_int),
+    ("mpdg_heat_cell_stiffness_form", [P, P, P, P], C.c_int),
     ("mpdg_last_error", [], C.c_char_p),
 ]
-OPTIONAL = [
-    ("mpdg_adjoint_heat", [P, P, P, P, P, C.POINTER(AdjointParams), P, C.POINTER(AdjointResult)], C.c_int),
-    ("mpdg_heat_cell_stiffness_form", [P, P, P, P], C.c_int),
-]
+OPTIONAL = []
 
 _lib = None
 

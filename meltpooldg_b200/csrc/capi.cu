@@ -882,6 +882,209 @@ mpdg_solve_mixed(mpdg_op *op, double *x, const double *b, const mpdg_mixed_param
   return MPDG_OK;
 }
 
+namespace
+{
+  // Forward sweep of the transient heat problem; states n = first+1..last are written to out[]
+  // (out may be null), the last state to Tlast.  J accumulated when target != null.
+  int
+  heat_forward_range(mpdg_op *op, const double *invd, const double *qhat, double amplitude, const double *T_first,
+                     int first, int last, const double *target, double *J, double **out, double *Tlast,
+                     const mpdg_adjoint_params *prm, long long *iters, int *solves)
+  {
+    const long long n   = op->ndofs;
+    double         *v   = op->vec<double>("adj_v"), *rhs = op->vec<double>("adj_rhs");
+    double         *Ta  = op->vec<double>("adj_Ta"), *Tb = op->vec<double>("adj_Tb");
+    if (!v || !rhs || !Ta || !Tb)
+      return fail(MPDG_ERR_NOMEM, "adjoint work vectors");
+    MPDG_CUDA(cudaMemcpyAsync(Ta, T_first, sizeof(double) * n, cudaMemcpyDeviceToDevice, op->stream));
+    for (int step = first + 1; step <= last; ++step)
+      {
+        // rhs = M (rho c_p T_{n-1} / dt + A qhat_n), plain reads, constrained rows 0
+        MPDG_CUDA(vec_axpby<double>(v, op->rho_cp / op->dt, Ta, amplitude, qhat + (size_t)(step - 1) * n, n, op->stream));
+        if (int e = apply<double>(op, (int)OutMode::Set, 1.0, rhs, v, nullptr, 0, 1))
+          return e;
+        MPDG_CUDA(cudaMemcpyAsync(Tb, Ta, sizeof(double) * n, cudaMemcpyDeviceToDevice, op->stream));
+        mpdg_solve_info in{};
+        if (int e = cg_solve<double>(op, Tb, rhs, invd, prm->cg_max_it > 0 ? prm->cg_max_it : 10000, 0.0,
+                                     prm->cg_rel_tol, &in, "adjcg_"))
+          return e;
+        *iters += in.iterations;
+        ++*solves;
+        if (target)
+          {
+            MPDG_CUDA(vec_axpby<double>(v, 1.0, Tb, -1.0, target + (size_t)(step - 1) * n, n, op->stream));
+            MPDG_CUDA(vec_set_constrained<double>(v, 0.0, op->grid(), op->stream));
+            const double *vv = v;
+            MPDG_CUDA(vec_multidot<double>(&vv, &vv, 1, n, op->d_scal, op->reducer(), op->stream));
+            MPDG_CUDA(cudaMemcpyAsync(op->h_scal, op->d_scal, sizeof(double), cudaMemcpyDeviceToHost, op->stream));
+            MPDG_CUDA(cudaStreamSynchronize(op->stream));
+            *J += 0.5 * op->h_scal[0];
+          }
+        if (out && out[step - first - 1])
+          MPDG_CUDA(cudaMemcpyAsync(out[step - first - 1], Tb, sizeof(double) * n, cudaMemcpyDeviceToDevice, op->stream));
+        std::swap(Ta, Tb);
+      }
+    if (Tlast)
+      MPDG_CUDA(cudaMemcpyAsync(Tlast, Ta, sizeof(double) * n, cudaMemcpyDeviceToDevice, op->stream));
+    return MPDG_OK;
+  }
+
+  int
+  adjoint_setup(mpdg_op *op, const double *log_k, double **invd)
+  {
+    if (op->kind != MPDG_HEAT)
+      return fail(MPDG_ERR_ARG, "the adjoint needs a heat operator");
+    if (op->degree > 2)
+      return fail(MPDG_ERR_UNSUPPORTED, "the adjoint supports FE_Q degree 1..2");
+    double *k = op->vec<double>("adj_k", (size_t)op->ncells);
+    *invd     = op->vec<double>("adj_invd");
+    if (!k || !*invd)
+      return fail(MPDG_ERR_NOMEM, "adjoint coefficient vectors");
+    MPDG_CUDA(vec_exp(k, log_k, op->ncells, op->stream));
+    if (int e = mpdg_op_set_conductivity(op, k))
+      return e;
+    return inverse_diagonal<double>(op, *invd);
+  }
+} // namespace
+
+int
+mpdg_heat_forward(mpdg_op *op, const double *log_k, const double *qhat, double amplitude,
+                  const mpdg_adjoint_params *prm, double *T_out)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!log_k || !qhat || !prm || !T_out || prm->n_steps < 1)
+    return fail(MPDG_ERR_ARG, "invalid argument to mpdg_heat_forward");
+  double *invd = nullptr;
+  if (int e = adjoint_setup(op, log_k, &invd))
+    return e;
+  const long long      n = op->ndofs;
+  std::vector<double *> out(prm->n_steps);
+  for (int i = 0; i < prm->n_steps; ++i)
+    out[i] = T_out + (size_t)i * n;
+  double *zero = op->vec<double>("adj_zero");
+  if (!zero)
+    return fail(MPDG_ERR_NOMEM, "adjoint work vector");
+  MPDG_CUDA(vec_fill<double>(zero, 0.0, n, op->stream));
+  long long it = 0;
+  int       solves = 0;
+  double    J      = 0.0;
+  if (int e = heat_forward_range(op, invd, qhat, amplitude, zero, 0, prm->n_steps, nullptr, &J, out.data(), nullptr,
+                                 prm, &it, &solves))
+    return e;
+  MPDG_CUDA(cudaStreamSynchronize(op->stream));
+  return MPDG_OK;
+}
+
+int
+mpdg_adjoint_heat(mpdg_op *op, const double *log_k, const double *qhat, double amplitude, const double *T_target,
+                  const mpdg_adjoint_params *prm, double *grad, mpdg_adjoint_result *res)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!log_k || !qhat || !T_target || !prm || prm->n_steps < 1)
+    return fail(MPDG_ERR_ARG, "invalid argument to mpdg_adjoint_heat");
+  double *invd = nullptr;
+  if (int e = adjoint_setup(op, log_k, &invd))
+    return e;
+  const long long n  = op->ndofs;
+  const int       S  = prm->n_steps;
+  const int       ce = std::max(1, std::min(prm->checkpoint_every > 0 ? prm->checkpoint_every : 5, S));
+  const int       ncp = (S + ce - 1) / ce; // checkpoints T_0, T_ce, ... (segment starts)
+  std::vector<double *> cp(ncp), seg(ce);
+  for (int i = 0; i < ncp; ++i)
+    if (!(cp[i] = op->vec<double>("adj_cp" + std::to_string(i))))
+      return fail(MPDG_ERR_NOMEM, "checkpoint storage");
+  for (int i = 0; i < ce; ++i)
+    if (!(seg[i] = op->vec<double>("adj_seg" + std::to_string(i))))
+      return fail(MPDG_ERR_NOMEM, "segment storage");
+  double *lam = op->vec<double>("adj_lam"), *lamn = op->vec<double>("adj_lamn"), *rhs = op->vec<double>("adj_arhs"),
+         *v = op->vec<double>("adj_av"), *Mq = op->vec<double>("adj_Mq");
+  if (!lam || !lamn || !rhs || !v || !Mq)
+    return fail(MPDG_ERR_NOMEM, "adjoint vectors");
+  long long it = 0;
+  int       fsolves = 0, asolves = 0;
+  double    J       = 0.0;
+  // forward pass: J and the checkpoints T_{s ce}
+  MPDG_CUDA(vec_fill<double>(cp[0], 0.0, n, op->stream));
+  for (int s = 0; s < ncp; ++s)
+    {
+      const int a = s * ce, b = std::min(S, a + ce);
+      if (int e = heat_forward_range(op, invd, qhat, amplitude, cp[s], a, b, T_target, &J, nullptr,
+                                     s + 1 < ncp ? cp[s + 1] : nullptr, prm, &it, &fsolves))
+        return e;
+    }
+  double gA = 0.0;
+  if (grad)
+    {
+      MPDG_CUDA(vec_fill<double>(grad, 0.0, op->ncells, op->stream));
+      MPDG_CUDA(vec_fill<double>(lamn, 0.0, n, op->stream));
+      const HeatGeom geo = heat_geom(op, 0.0);
+      for (int s = ncp - 1; s >= 0; --s)
+        {
+          const int a = s * ce, b = std::min(S, a + ce);
+          // recompute T_{a+1..b} from the checkpoint T_a
+          double dummy = 0.0;
+          if (int e = heat_forward_range(op, invd, qhat, amplitude, cp[s], a, b, nullptr, &dummy, seg.data(), nullptr,
+                                         prm, &it, &fsolves))
+            return e;
+          for (int step = b; step > a; --step)
+            {
+              const double *Tn = seg[step - a - 1];
+              // rhs = rho c_p M lam_{n+1} / dt + (T_n - T*_n) on free rows
+              if (int e = apply<double>(op, (int)OutMode::Set, op->rho_cp / op->dt, rhs, lamn, nullptr, 1, 1))
+                return e;
+              MPDG_CUDA(vec_axpby<double>(v, 1.0, Tn, -1.0, T_target + (size_t)(step - 1) * n, n, op->stream));
+              MPDG_CUDA(vec_set_constrained<double>(v, 0.0, op->grid(), op->stream));
+              MPDG_CUDA(vec_axpby<double>(rhs, 1.0, rhs, 1.0, v, n, op->stream));
+              MPDG_CUDA(cudaMemcpyAsync(lam, lamn, sizeof(double) * n, cudaMemcpyDeviceToDevice, op->stream));
+              mpdg_solve_info in{};
+              if (int e = cg_solve<double>(op, lam, rhs, invd, prm->cg_max_it > 0 ? prm->cg_max_it : 10000, 0.0,
+                                           prm->cg_rel_tol, &in, "adjcg_"))
+                return e;
+              it += in.iterations;
+              ++asolves;
+              // dJ/dz_c -= k_c lam^T K_c T_n   (fused per-cell reduction)
+              MPDG_CUDA(heat_cell_form(op->grid(), op->degree, geo, -1.0, lam, Tn, op->d_k64, op->k, grad, true,
+                                       op->stream));
+              // dJ/dA += lam^T M qhat_n
+              if (int e = apply<double>(op, (int)OutMode::Set, 1.0, Mq, qhat + (size_t)(step - 1) * n, nullptr, 0, 1))
+                return e;
+              const double *x0 = lam, *y0 = Mq;
+              MPDG_CUDA(vec_multidot<double>(&x0, &y0, 1, n, op->d_scal, op->reducer(), op->stream));
+              MPDG_CUDA(cudaMemcpyAsync(op->h_scal, op->d_scal, sizeof(double), cudaMemcpyDeviceToHost, op->stream));
+              MPDG_CUDA(cudaStreamSynchronize(op->stream));
+              gA += op->h_scal[0];
+              std::swap(lam, lamn);
+            }
+        }
+    }
+  MPDG_CUDA(cudaStreamSynchronize(op->stream));
+  if (res)
+    {
+      res->objective      = J;
+      res->grad_amplitude = gA;
+      res->forward_solves = fsolves;
+      res->adjoint_solves = asolves;
+      res->cg_iterations  = it;
+    }
+  return MPDG_OK;
+}
+
+int
+mpdg_heat_cell_stiffness_form(mpdg_op *op, const double *lam, const double *T, double *form)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!lam || !T || !form || op->kind != MPDG_HEAT)
+    return fail(MPDG_ERR_ARG, "invalid argument to mpdg_heat_cell_stiffness_form");
+  if (op->degree > 2)
+    return fail(MPDG_ERR_UNSUPPORTED, "cell forms support FE_Q degree 1..2");
+  MPDG_CUDA(heat_cell_form(op->grid(), op->degree, heat_geom(op, 0.0), 1.0, lam, T, nullptr, 1.0, form, false,
+                           op->stream));
+  return MPDG_OK;
+}
+
 int
 mpdg_op_device_errors(mpdg_op *op)
 {

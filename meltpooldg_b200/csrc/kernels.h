@@ -159,6 +159,11 @@ namespace mpdg
   // d = |d| > 1e-14 max(1, *amax) ? 1/d : 1 (advection rule, amax on the device)
   template <typename T>
   cudaError_t vec_invert_rel(T *d, const double *amax_dev, long long n, cudaStream_t s);
+  // adjoint helpers (adjoint.cu): g_c (+)= scale k_c lam_c^T K_c T_c, and k = exp(z)
+  cudaError_t heat_cell_form(const GridDesc &g, int K, const HeatGeom &geo, double scale, const double *lam,
+                             const double *T, const double *k, double kconst, double *out, bool accumulate,
+                             cudaStream_t s);
+  cudaError_t vec_exp(double *k, const double *z, long long n, cudaStream_t s);
   // set constrained entries (face mask / per-DoF mask) of x to v
   template <typename T>
   cudaError_t vec_set_constrained(T *x, T v, const GridDesc &g, cudaStream_t s);

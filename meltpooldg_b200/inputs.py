@@ -59,3 +59,38 @@ def unit_directions(n: int, count: int, seed: int) -> np.ndarray:
 class _Flat:
     def __init__(self, n: int):
         self.ncells = n
+
+
+def gauss_lobatto_nodes(degree: int) -> np.ndarray:
+    """Support points of FE_Q(degree) on [0, 1] (Gauss-Lobatto nodes, degree <= 4)."""
+    s5, s37 = 1.0 / np.sqrt(5.0), np.sqrt(3.0 / 7.0)
+    table = {1: [-1.0, 1.0], 2: [-1.0, 0.0, 1.0], 3: [-1.0, -s5, s5, 1.0], 4: [-1.0, -s37, 0.0, s37, 1.0]}
+    return 0.5 * (np.asarray(table[degree]) + 1.0)
+
+
+def lattice_coords(mesh):
+    """Support-point coordinates (X, Y, Z) of every DoF in lexicographic order (x fastest)."""
+    cells = getattr(mesh, "cells", None) or mesh.m
+    nodes = gauss_lobatto_nodes(mesh.degree)
+    axes = []
+    for d in range(3):
+        h = mesh.length[d] / cells[d]
+        x = np.empty(mesh.degree * cells[d] + 1)
+        for c in range(cells[d]):
+            x[c * mesh.degree:(c + 1) * mesh.degree + 1] = mesh.origin[d] + h * (c + nodes)
+        axes.append(x)
+    Z, Y, X = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    return X.ravel(), Y.ravel(), Z.ravel()
+
+
+def moving_gaussian(mesh, n_steps: int, dt: float, start=(0.2, 0.5, 0.95), velocity=(30.0, 0.0, 0.0),
+                    width: float = 0.05) -> np.ndarray:
+    """Unit-amplitude moving heat source qhat_n(x) = exp(-2 |x - x0(t_n)|^2 / width^2), t_n = n dt,
+    x0(t) = start + velocity t, sampled at the support points; shape (n_steps, n_dofs)."""
+    X, Y, Z = lattice_coords(mesh)
+    out = np.empty((n_steps, X.size))
+    for s in range(n_steps):
+        t = (s + 1) * dt
+        c = [start[d] + velocity[d] * t for d in range(3)]
+        out[s] = np.exp(-2.0 * ((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) / width ** 2)
+    return out

@@ -223,6 +223,35 @@ MPDG_API int mpdg_heat_forward(mpdg_op *op, const double *log_k, const double *q
 /* Per-cell unit-conductivity stiffness form form_c = lam_c^T K_c T_c (device arrays). */
 MPDG_API int mpdg_heat_cell_stiffness_form(mpdg_op *op, const double *lam, const double *T, double *form);
 
+/* Allocation-free heat vmult.  No counterpart in the reference (the reference allocates through
+   deal.II and never runs on a GPU).  Some callers must not allocate device memory at all: a host
+   application that reserves its whole HBM budget up front in its own pool (where a cudaMalloc can
+   fail or fragment that pool), and latency-bound time loops in which cudaMalloc / cudaFree would
+   synchronise the device.  This entry point computes dst = A src exactly like mpdg_op_vmult on an
+   operator built from the same mesh and parameters, without an operator handle and without any
+   device allocation: the launch bookkeeping (brick ticket, per-brick flags, wait error word) lives
+   in a fixed 256 KiB array in the library's device memory, held by every GPU that loads the
+   library until the process exits.
+     - mesh: Dirichlet faces only (dirichlet_mask must be NULL); FE_Q degree 1..4.
+     - params: kind MPDG_HEAT; params->conductivity_cells must be NULL; a per-cell conductivity is
+       passed as the DEVICE array k_cells_dev (n_cells entries) or NULL for params->conductivity.
+     - dst, src: distinct device arrays of n_dofs entries; cuda_stream: a cudaStream_t of the
+       current device (NULL = legacy default stream).
+     - Meshes that need more than MPDG_NOALLOC_MAX_BRICKS brick flags are rejected with
+       MPDG_ERR_UNSUPPORTED before any GPU work (the brick is 32x4x16 cells at degree 1, 32x4x8 at
+       degree 2, 4x4x4 at degrees 3 and 4; e.g. 160^3 cells of degree 4 still fit).
+     - The first call on a device does the set-up: it looks up the scratch address on the current
+       device and loads the interpolation tables; make that first call before any stream capture.
+     - Every call clears the ticket and flags it uses (stream-ordered, before its kernel).  All calls
+       on a device share the one array, so calls that overlap on the GPU (different streams or host
+       threads without ordering) race and give wrong results: order them.
+     - A bounded device wait that gives up records an error word in the scratch array, which this
+       entry point does not read back. */
+#define MPDG_NOALLOC_SCRATCH_BYTES (256 * 1024)
+#define MPDG_NOALLOC_MAX_BRICKS ((MPDG_NOALLOC_SCRATCH_BYTES - 256) / 4)
+MPDG_API int mpdg_heat_vmult_noalloc(const mpdg_mesh_desc *mesh, const mpdg_op_params *params,
+                                     const double *k_cells_dev, double *dst, const double *src, void *cuda_stream);
+
 /* Number of error words raised by bounded device waits since the last call (and reset). */
 MPDG_API int mpdg_op_device_errors(mpdg_op *op);
 

@@ -1098,3 +1098,12 @@ mpdg_op_device_errors(mpdg_op *op)
 }
 
 } // extern "C"
+
+namespace mpdg
+{
+  int
+  record_failure(int code, const char *msg)
+  {
+    return fail(code, msg);
+  }
+} // namespace mpdg

@@ -159,6 +159,8 @@ namespace mpdg
   // d = |d| > 1e-14 max(1, *amax) ? 1/d : 1 (advection rule, amax on the device)
   template <typename T>
   cudaError_t vec_invert_rel(T *d, const double *amax_dev, long long n, cudaStream_t s);
+  // records an error message for mpdg_last_error() and returns code (capi.cu)
+  int record_failure(int code, const char *msg);
   // adjoint helpers (adjoint.cu): g_c (+)= scale k_c lam_c^T K_c T_c, and k = exp(z)
   cudaError_t heat_cell_form(const GridDesc &g, int K, const HeatGeom &geo, double scale, const double *lam,
                              const double *T, const double *k, double kconst, double *out, bool accumulate,

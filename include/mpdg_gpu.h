@@ -20,7 +20,7 @@
  * Conventions
  *  - Vectors are in lexicographic lattice order (x fastest) over the (k m + 1)^3 Gauss-Lobatto
  *    support points of a structured box mesh of axis-aligned hexahedra.  deal.II's DoF numbering
- *    is mapped onto it once by the caller.
+ *    is mapped onto it once by the caller (one permutation of the DoF indices).
  *  - Pointers are DEVICE pointers unless the function name ends in _host.
  *  - vmult zeroes dst; Dirichlet-constrained entries of src are read as 0 and those of dst stay 0
  *    (deal.II MatrixFree semantics).  create_rhs accumulates into dst, reads its inputs plainly

@@ -121,8 +121,7 @@ namespace mpdg
     // row walk: a thread keeps the x-column px = tid % PX and visits rows tid / PX + k * RSTEP
     static constexpr int ROWS   = PY * PZ;
     static constexpr int RSTEP  = NT / PX;
-    static constexpr int RITER  = (ROWS + RSTEP - 1) / RSTEP;
-    static_assert(RSTEP >= 1, "brick rows wider than the CTA");
+    static constexpr int RITER  = RSTEP > 0 ? (ROWS + RSTEP - 1) / RSTEP : 0;
     int            c0[3];                // first cell of the brick
     int            g0[3];                // first lattice point (K c0)
     int            nv[3];                // lattice points of the brick inside the domain
@@ -274,6 +273,7 @@ namespace mpdg
   __device__ __forceinline__ void
   brick_stage(const BR &br, const T *src, bool mask_src, T *s_src)
   {
+    static_assert(BR::RSTEP >= 1, "brick rows wider than the CTA");
     const int  px  = threadIdx.x % BR::PX;
     const int  r0  = threadIdx.x / BR::PX;
     const bool act = r0 < BR::RSTEP;
@@ -303,6 +303,7 @@ namespace mpdg
   __device__ __forceinline__ void
   brick_output(const BR &br, const T *s_dst, T *dst, const T *bvec)
   {
+    static_assert(BR::RSTEP >= 1, "brick rows wider than the CTA");
     constexpr int U   = 4;
     const int     px  = threadIdx.x % BR::PX;
     const int     r0  = threadIdx.x / BR::PX;

@@ -19,6 +19,7 @@
 #include "brick.cuh"
 #include "kernels.h"
 #include "march.cuh"
+#include "pencil.cuh"
 #include "sumfac.cuh"
 
 namespace mpdg
@@ -356,6 +357,50 @@ namespace mpdg
                            &s_ticket);
   }
 
+  // ---- k >= 3: pencil-marching apply (pencil.cuh); the x lines are scaled by the diagonal of the
+  // fast-diagonalisation basis, a + k_c (cx lam_a + cy lam_b + cz lam_c)
+  template <int K, typename T>
+  struct HeatPencilOp
+  {
+    static constexpr int N = K + 1, NE = (N + 1) / 2, NO = N / 2;
+    const HeatArgs<T, N> &a;
+    __device__ __forceinline__ const T *
+    we() const
+    {
+      return fd_table<T>(K);
+    }
+    __device__ __forceinline__ const T *
+    wo() const
+    {
+      return fd_table<T>(K) + NE * NE;
+    }
+    __device__ __forceinline__ void
+    scale_line(T *x, int cx, int cy, int cz, int b, int c) const
+    {
+      const T        *lam  = fd_table<T>(K) + NE * NE + NO * NO;
+      const long long cell = (long long)cx + (long long)a.g.m[0] * ((long long)cy + (long long)a.g.m[1] * cz);
+      const T         kc   = a.kscale * (a.kcell ? a.kcell[cell] : a.kconst);
+      const T         beta = fma(kc * a.cy, lam[b], fma(kc * a.cz, lam[c], a.alpha));
+      const T         kcx  = kc * a.cx;
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+        x[i] *= fma(kcx, lam[i], beta);
+    }
+  };
+
+  template <int K, typename T, OutMode MODE>
+  __global__ void __launch_bounds__(PencilShape<K>::NT)
+  heat_pencil_kernel(const __grid_constant__ HeatArgs<T, K + 1> a)
+  {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned s_ticket;
+    if (a.skip != nullptr && *a.skip != 0)
+      return;
+    HeatPencilOp<K, T> op{a};
+    pencil_body<K, T, MODE>(a.g, a.s, a.src, a.dst, a.b, a.mask_src != 0, op, reinterpret_cast<T *>(smem_raw),
+                            &s_ticket);
+  }
+
   // ---- diagonal: closed-form per-cell entries gathered per DoF (deterministic, no atomics)
   template <typename T>
   struct DiagArgs
@@ -512,6 +557,22 @@ namespace mpdg
         kern<<<nbricks, ML::S::NT, ML::bytes, stream>>>(a);
         return cudaGetLastError();
       }
+    if constexpr (K >= 3)
+      if (h.grid.cmask == nullptr && h.march)
+      {
+        using PL  = PencilLayout<K, T>;
+        auto kern = heat_pencil_kernel<K, T, MODE>;
+        static thread_local bool attr_done = false;
+        if (!attr_done)
+          {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::bytes);
+            if (e != cudaSuccess)
+              return e;
+            attr_done = true;
+          }
+        kern<<<nbricks, PL::S::NT, PL::bytes, stream>>>(a);
+        return cudaGetLastError();
+      }
     {
         auto kern = heat_apply_kernel<K, T, MODE>;
         static thread_local bool attr_done = false;
@@ -545,6 +606,15 @@ namespace mpdg
   heat_brick_shape(int K, int shape[3], bool march)
   {
     brick_shape<T>(K, shape[0], shape[1], shape[2]);
+    if (march && K >= 3)
+      {
+        shape[0] = PencilShape<3>::BX;
+        shape[1] = PencilShape<3>::BY;
+        shape[2] = PencilShape<3>::BZ;
+        static_assert(PencilShape<3>::BX == PencilShape<4>::BX && PencilShape<3>::BY == PencilShape<4>::BY &&
+                        PencilShape<3>::BZ == PencilShape<4>::BZ,
+                      "one pencil brick shape for k = 3, 4");
+      }
     if (!march && K <= 2)
       {
         shape[0] = K == 1 ? HeatBrickShape<1, T>::BX : HeatBrickShape<2, T>::BX;

@@ -64,10 +64,8 @@ mpdg_heat_vmult_noalloc(const mpdg_mesh_desc *mesh, const mpdg_op_params *params
                         double *dst, const double *src, void *cuda_stream)
 {
   using namespace mpdg;
-  if (!mesh || !params || !dst || !src)
+  if (!mesh || !params)
     return reject(MPDG_ERR_ARG, "null argument to mpdg_heat_vmult_noalloc");
-  if (dst == src)
-    return reject(MPDG_ERR_ARG, "mpdg_heat_vmult_noalloc needs distinct dst and src");
   if (params->kind != MPDG_HEAT)
     return reject(MPDG_ERR_ARG, "mpdg_heat_vmult_noalloc applies the heat operator only");
   if (mesh->degree < 1 || mesh->degree > 4)
@@ -110,6 +108,11 @@ mpdg_heat_vmult_noalloc(const mpdg_mesh_desc *mesh, const mpdg_op_params *params
                     nbrk, (int)MPDG_NOALLOC_MAX_BRICKS, (int)MPDG_NOALLOC_SCRATCH_BYTES);
       return reject(MPDG_ERR_UNSUPPORTED, msg);
     }
+  // the vectors are checked last, so a size that is too large is reported whatever they are
+  if (!dst || !src)
+    return reject(MPDG_ERR_ARG, "null vector passed to mpdg_heat_vmult_noalloc");
+  if (dst == src)
+    return reject(MPDG_ERR_ARG, "mpdg_heat_vmult_noalloc needs distinct dst and src");
 
   unsigned   *scratch = nullptr;
   cudaError_t e       = scratch_of_current_device(&scratch);

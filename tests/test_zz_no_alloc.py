@@ -35,7 +35,8 @@ def call_noalloc(m, p, k_dev, dst, src, stream=None):
     from meltpooldg_b200 import _lib as L
 
     return L.lib().mpdg_heat_vmult_noalloc(C.byref(m), C.byref(p), None if k_dev is None else k_dev.data_ptr(),
-                                           dst.data_ptr(), src.data_ptr(), stream)
+                                           None if dst is None else dst.data_ptr(),
+                                           None if src is None else src.data_ptr(), stream)
 
 
 @pytest.mark.gpu
@@ -68,16 +69,18 @@ def test_noalloc_vmult_matches_vmult_twice(degree, cells, faces, kfield):
 
 @pytest.mark.gpu
 def test_noalloc_rejects_oversized_and_unsupported_inputs():
-    """Every rejected call returns before any GPU work, so the small vectors are never touched."""
+    """Every rejected call returns before any GPU work.  The oversized mesh is passed without
+    vectors: the size check comes before the vector check, so no outcome of this call can launch."""
     import torch
 
     from meltpooldg_b200 import _lib as L
 
     x = torch.zeros(8, dtype=torch.float64, device="cuda")
     y = torch.zeros(8, dtype=torch.float64, device="cuda")
-    # 164^3 cells of degree 4 need 41^3 = 68921 brick flags > MPDG_NOALLOC_MAX_BRICKS (65472)
-    m, p = descs(4, (164, 164, 164), 0b111111)
-    assert call_noalloc(m, p, None, y, x) == L.MPDG_ERR_UNSUPPORTED
+    # 1280^3 cells of degree 1 (< 2^31 DoFs) need far more than MPDG_NOALLOC_MAX_BRICKS (65472) brick
+    # flags for any brick of fewer than 32768 cells
+    m, p = descs(1, (1280, 1280, 1280), 0b111111)
+    assert call_noalloc(m, p, None, None, None) == L.MPDG_ERR_UNSUPPORTED
     assert b"brick flags" in L.lib().mpdg_last_error()
     m, p = descs(5, (4, 4, 4), 0b111111)
     assert call_noalloc(m, p, None, y, x) == L.MPDG_ERR_UNSUPPORTED

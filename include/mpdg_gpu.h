@@ -238,8 +238,9 @@ MPDG_API int mpdg_heat_cell_stiffness_form(mpdg_op *op, const double *lam, const
      - dst, src: distinct device arrays of n_dofs entries; cuda_stream: a cudaStream_t of the
        current device (NULL = legacy default stream).
      - Meshes that need more than MPDG_NOALLOC_MAX_BRICKS brick flags are rejected with
-       MPDG_ERR_UNSUPPORTED before any GPU work (the brick is 32x4x16 cells at degree 1, 32x4x8 at
-       degree 2, 4x4x4 at degrees 3 and 4; e.g. 160^3 cells of degree 4 still fit).
+       MPDG_ERR_UNSUPPORTED before any GPU work and before dst / src are looked at (the brick is
+       32x4x16 cells at degree 1, 32x4x8 at degree 2, 32x2x4 at degrees 3 and 4; e.g. 160^3 cells
+       of degree 4 still fit).
      - The first call on a device does the set-up: it looks up the scratch address on the current
        device and loads the interpolation tables; make that first call before any stream capture.
      - Every call clears the ticket and flags it uses (stream-ordered, before its kernel).  All calls

@@ -374,22 +374,42 @@ namespace mpdg
     {
       return fd_table<T>(K) + NE * NE;
     }
-    __device__ __forceinline__ void
-    scale_line(T *x, int cx, int cy, int cz, int b, int c) const
+    __device__ __forceinline__ const T *
+    lam() const
     {
-      const T        *lam  = fd_table<T>(K) + NE * NE + NO * NO;
+      return fd_table<T>(K) + NE * NE + NO * NO;
+    }
+    __device__ __forceinline__ T
+    alpha() const
+    {
+      return a.alpha;
+    }
+    __device__ __forceinline__ T
+    cxg() const
+    {
+      return a.cx;
+    }
+    __device__ __forceinline__ T
+    cyg() const
+    {
+      return a.cy;
+    }
+    __device__ __forceinline__ T
+    czg() const
+    {
+      return a.cz;
+    }
+    // scaled conductivity of cell (cx, cy, cz)
+    __device__ __forceinline__ T
+    kcell(int cx, int cy, int cz) const
+    {
       const long long cell = (long long)cx + (long long)a.g.m[0] * ((long long)cy + (long long)a.g.m[1] * cz);
-      const T         kc   = a.kscale * (a.kcell ? a.kcell[cell] : a.kconst);
-      const T         beta = fma(kc * a.cy, lam[b], fma(kc * a.cz, lam[c], a.alpha));
-      const T         kcx  = kc * a.cx;
-#pragma unroll
-      for (int i = 0; i < N; ++i)
-        x[i] *= fma(kcx, lam[i], beta);
+      return a.kscale * (a.kcell ? a.kcell[cell] : a.kconst);
     }
   };
 
   template <int K, typename T, OutMode MODE>
-  __global__ void __launch_bounds__(PencilShape<K>::NT)
+  __global__ void __launch_bounds__(PencilShape<K>::NT, PencilShape<K>::MINB)
   heat_pencil_kernel(const __grid_constant__ HeatArgs<T, K + 1> a)
   {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -24,13 +24,28 @@
 #include "brick.cuh"
 #include "sumfac.cuh"
 
+#ifndef MPDG_PENCIL_BY
+#define MPDG_PENCIL_BY 2
+#endif
+#ifndef MPDG_PENCIL_BZ
+#define MPDG_PENCIL_BZ 4
+#endif
+#ifndef MPDG_PENCIL_MINB3
+#define MPDG_PENCIL_MINB3 5
+#endif
+#ifndef MPDG_PENCIL_MINB4
+#define MPDG_PENCIL_MINB4 4
+#endif
+
 namespace mpdg
 {
   template <int K>
   struct PencilShape
   {
     static constexpr int N = K + 1, M = N * N;
-    static constexpr int BX = 32, BY = 2, BZ = 4;
+    static constexpr int BX = 32, BY = MPDG_PENCIL_BY, BZ = MPDG_PENCIL_BZ;
+    // CTAs per SM the register allocation is held to (K = 4: 4 x 128 threads at <= 128 registers)
+    static constexpr int MINB = K == 3 ? MPDG_PENCIL_MINB3 : MPDG_PENCIL_MINB4;
     static constexpr int NT = K * BX;        // threads: x points 0 .. K*BX-1
     static constexpr int TP = K * BX + 1;    // x points of the transposition buffer (odd)
     static constexpr int MP = M | 1;         // face-buffer stride (odd)
@@ -44,11 +59,14 @@ namespace mpdg
     static constexpr int FB    = S::BX * S::MP;         // one face buffer
     static constexpr int ZC    = S::BY * K * S::NT;     // z carries
     static constexpr int XS    = S::M;                  // exchange of the cooperative pencil
-    static constexpr size_t bytes = sizeof(T) * (size_t)(TB + 2 * FB + ZC + XS);
+    static constexpr int KC    = S::BX;                 // conductivity of the row's cells
+    static constexpr int MU    = S::M;                  // cy lam_b + cz lam_c per (y, z) mode
+    static constexpr size_t bytes = sizeof(T) * (size_t)(TB + 2 * FB + ZC + XS + KC + MU);
     using BR = Brick<K, S::BX, S::BY, S::BZ, S::NT>;
   };
 
-  // Op supplies the per-cell diagonal: scale(kc, b, c) -> beta, and kcx; see heat.cu.
+  // Op supplies the fast-diagonalisation tables and the per-cell scaling:
+  //   we(), wo(), lam()  1-D tables;  alpha(), cxg(), cyg(), czg()  geometry;  kcell(cell)  k_c.
   template <int K, typename T, OutMode MODE, class Op>
   __device__ __forceinline__ void
   pencil_body(const GridDesc &g, const SyncDesc &s, const T *src, T *dst, const T *bvec, bool mask_src, const Op &op,
@@ -59,6 +77,7 @@ namespace mpdg
     using BR        = typename LAY::BR;
     constexpr int N = K + 1, M = SH::M, TP = SH::TP, MP = SH::MP, BX = SH::BX, NT = SH::NT;
     T *tb = smem, *e0 = smem + LAY::TB, *e4 = e0 + LAY::FB, *zc = e4 + LAY::FB, *xs = zc + LAY::ZC;
+    T *kcs = xs + LAY::XS, *mus = kcs + LAY::KC;
     const int p = threadIdx.x, lane = p & 31, warp = p >> 5;
     BR        br;
     if (!brick_begin<BR, T, MODE>(br, g, s, dst, bvec, s_ticket))
@@ -66,7 +85,10 @@ namespace mpdg
     if constexpr (MODE != OutMode::Add)
       if (br.has_lower_neighbour())
         brick_wait_lower(br, g, s);
-    const T  *we = op.we(), *wo = op.wo();
+    const T *we = op.we(), *wo = op.wo(), *lam = op.lam();
+    if (p < M)
+      mus[p] = op.cyg() * lam[p % N] + op.czg() * lam[p / N];
+    const T   alpha = op.alpha(), cxg = op.cxg();
     const int ncx = min(BX, g.m[0] - br.c0[0]), ncy = min(SH::BY, g.m[1] - br.c0[1]),
               ncz = min(SH::BZ, g.m[2] - br.c0[2]);
     const int  plast = K * ncx;               // brick's high x face (x point)
@@ -74,13 +96,16 @@ namespace mpdg
     const bool extra = ncx == BX;             // x point K*BX exists and is done cooperatively
     const bool xface = p == 0 || p == plast;
     const bool xcon  = (br.con_lo[0] && p == 0) || (br.con_hi[0] && p == plast);
-    const bool xcon_in = mask_src && xcon;
+    const bool zero_pencil = !xin || (mask_src && xcon);
     const int  qx = p % K, cxp = p / K;       // x point = K cxp + qx
     const int  sy = br.sy, sz = br.sz;
-    const int  xbase = br.g0[0] + p;
+    const int  xbase = br.g0[0] + (xin ? p : plast); // clamped: every load stays inside the lattice
     const bool exl   = extra && warp == 0 && lane < N; // lanes of the cooperative pencil
     const int  xbE   = br.g0[0] + K * BX;
     const bool xconE = br.con_hi[0] && extra;
+    // first x line of this thread and the increments of (cell, mode) per round of NT lines
+    constexpr int DCX = NT / M, DM = NT % M;
+    const int     cx_first = p / M, m_first = p % M;
 
     T ycar[N];
 #pragma unroll
@@ -96,22 +121,42 @@ namespace mpdg
             const int  gy0 = br.g0[1] + K * r;
             const bool jlo = br.con_lo[1] && r == 0, jhi = br.con_hi[1] && r == ncy - 1;
             const int  base = gy0 * sy + gz0 * sz;
+            const int  cy = br.c0[1] + r, cz = br.c0[2] + lz;
             // ---- 1. load and transform the pencil (z lines, then y lines)
             T u[M];
             {
-              const bool ok = xin && !xcon_in;
-              const T   *s0 = src + (xbase + base);
+              const T *s0 = src + (xbase + base);
 #pragma unroll
               for (int l = 0; l < N; ++l)
 #pragma unroll
                 for (int j = 0; j < N; ++j)
-                  {
-                    bool v = ok;
-                    if (mask_src)
-                      v = v && !((j == 0 && jlo) || (j == K && jhi) || (l == 0 && llo) || (l == K && lhi));
-                    u[l * N + j] = v ? s0[j * sy + l * sz] : T(0);
-                  }
+                  u[l * N + j] = s0[j * sy + l * sz];
             }
+            if (p < ncx)
+              kcs[p] = op.kcell(br.c0[0] + p, cy, cz);
+            if (zero_pencil)
+#pragma unroll
+              for (int q = 0; q < M; ++q)
+                u[q] = T(0);
+            if (mask_src)
+              {
+                if (jlo)
+#pragma unroll
+                  for (int l = 0; l < N; ++l)
+                    u[l * N] = T(0);
+                if (jhi)
+#pragma unroll
+                  for (int l = 0; l < N; ++l)
+                    u[l * N + K] = T(0);
+                if (llo)
+#pragma unroll
+                  for (int j = 0; j < N; ++j)
+                    u[j] = T(0);
+                if (lhi)
+#pragma unroll
+                  for (int j = 0; j < N; ++j)
+                    u[K * N + j] = T(0);
+              }
 #pragma unroll
             for (int j = 0; j < N; ++j)
               fwd_line<T, N, N>(u, j, we, wo);
@@ -125,7 +170,7 @@ namespace mpdg
               {
                 // cooperative pencil at x point K*BX: lane j transforms the z line of y point j
                 const int  j  = lane;
-                const bool ok = !(mask_src && xconE) && !(mask_src && ((j == 0 && jlo) || (j == K && jhi)));
+                const bool ok = !(mask_src && (xconE || (j == 0 && jlo) || (j == K && jhi)));
                 T          v[N];
 #pragma unroll
                 for (int l = 0; l < N; ++l)
@@ -154,39 +199,47 @@ namespace mpdg
             __syncthreads();
             // ---- 2. x lines: one (cell, mode) line per thread and round
             {
-              const int cy = br.c0[1] + r, cz = br.c0[2] + lz;
-              for (int L = p; L < ncx * M; L += NT)
+              int cx = cx_first, m = m_first;
+              while (cx < ncx)
                 {
-                  const int cx = L / M, m = L - cx * M, b = m % N, c = m / N;
-                  T         x[N];
+                  T x[N];
 #pragma unroll
                   for (int i = 0; i < N; ++i)
                     x[i] = tb[m * TP + K * cx + i];
                   fwd_line<T, N, 1>(x, 0, we, wo);
-                  op.scale_line(x, br.c0[0] + cx, cy, cz, b, c);
+                  const T kc   = kcs[cx];
+                  const T beta = fma(kc, mus[m], alpha);
+                  const T kcx  = kc * cxg;
+#pragma unroll
+                  for (int i = 0; i < N; ++i)
+                    x[i] *= fma(kcx, lam[i], beta);
                   bwd_line<T, N, 1>(x, 0, we, wo);
 #pragma unroll
                   for (int i = 1; i < K; ++i)
                     tb[m * TP + K * cx + i] = x[i];
                   e0[cx * MP + m] = x[0];
                   e4[cx * MP + m] = x[K];
+                  cx += DCX;
+                  m += DM;
+                  if (m >= M)
+                    {
+                      m -= M;
+                      ++cx;
+                    }
                 }
             }
             __syncthreads();
-            // ---- 3. read back, backward y and z transforms
+            // ---- 3. read back (face points: both adjacent cells), backward y and z transforms
 #pragma unroll
             for (int m = 0; m < M; ++m)
+              u[m] = tb[m * TP + p];
+            if (qx == 0)
               {
-                T v;
-                if (qx != 0)
-                  v = tb[m * TP + p];
-                else
-                  {
-                    v = (cxp < ncx) ? e0[cxp * MP + m] : T(0);
-                    if (cxp > 0)
-                      v += e4[(cxp - 1) * MP + m];
-                  }
-                u[m] = v;
+                const T *f0 = e0 + cxp * MP, *f4 = e4 + (cxp - 1) * MP;
+                const bool h0 = cxp < ncx, h4 = cxp > 0;
+#pragma unroll
+                for (int m = 0; m < M; ++m)
+                  u[m] = (h0 ? f0[m] : T(0)) + (h4 ? f4[m] : T(0));
               }
 #pragma unroll
             for (int c = 0; c < N; ++c)
@@ -225,69 +278,108 @@ namespace mpdg
                   }
               }
             // ---- 4. combine and write the pencil's points
-            if (xin)
+            T *d0 = dst + (xbase + base);
+            if (xin && xface)
               {
-                T *d0 = dst + (xbase + base);
-                if (xface)
+                // brick x face: every point atomically
+#pragma unroll
+                for (int l = 0; l < N; ++l)
+#pragma unroll
+                  for (int j = 0; j < N; ++j)
+                    {
+                      const bool cn =
+                        xcon || (j == 0 && jlo) || (j == K && jhi) || (l == 0 && llo) || (l == K && lhi);
+                      if (!cn)
+                        atomicAdd(d0 + (j * sy + l * sz), u[l * N + j]);
+                    }
+              }
+            else if (xin)
+              {
+                const bool ylast = r == ncy - 1, zlast = lz == ncz - 1;
+                T         *zcr   = zc + r * K * NT + p;
+                if (r > 0)
+#pragma unroll
+                  for (int l = 0; l < N; ++l)
+                    u[l * N] += ycar[l];
+                if (lz > 0)
+#pragma unroll
+                  for (int j = 0; j < K; ++j)
+                    u[j] += zcr[j * NT];
+#pragma unroll
+                for (int l = 0; l < N; ++l)
+                  ycar[l] = u[l * N + K];
+                if (!zlast)
+#pragma unroll
+                  for (int j = 0; j < K; ++j)
+                    zcr[j * NT] = u[K * N + j];
+                auto put = [&](int j, int l) {
+                  const int off = j * sy + l * sz;
+                  const T   v   = u[l * N + j];
+                  if constexpr (MODE == OutMode::Set)
+                    d0[off] = v;
+                  else if constexpr (MODE == OutMode::Add)
+                    d0[off] += v;
+                  else
+                    d0[off] = bvec[xbase + base + off] + v;
+                };
+                auto add = [&](int j, int l) { atomicAdd(d0 + (j * sy + l * sz), u[l * N + j]); };
+                // interior of the pencil's owned block: plain stores
+#pragma unroll
+                for (int l = 1; l < K; ++l)
+#pragma unroll
+                  for (int j = 1; j < K; ++j)
+                    put(j, l);
+                // y = 0 row (l = 1..K-1): low y face of the brick in row 0
+                if (r == 0)
                   {
-                    // brick x face: every point atomically
+                    if (!jlo)
 #pragma unroll
-                    for (int l = 0; l < N; ++l)
-#pragma unroll
-                      for (int j = 0; j < N; ++j)
-                        {
-                          const bool cn = xcon || (j == 0 && jlo) || (j == K && jhi) || (l == 0 && llo) ||
-                                          (l == K && lhi);
-                          if (!cn)
-                            atomicAdd(d0 + (j * sy + l * sz), u[l * N + j]);
-                        }
+                      for (int l = 1; l < K; ++l)
+                        add(0, l);
                   }
                 else
+#pragma unroll
+                  for (int l = 1; l < K; ++l)
+                    put(0, l);
+                // z = 0 plane (j = 1..K-1): low z face of the brick in layer 0
+                if (lz == 0)
                   {
-                    const bool ylast = r == ncy - 1, zlast = lz == ncz - 1;
-                    T         *zcr   = zc + r * K * NT + p;
-                    if (r > 0)
+                    if (!llo)
 #pragma unroll
-                      for (int l = 0; l < N; ++l)
-                        u[l * N] += ycar[l];
-                    if (lz > 0)
+                      for (int j = 1; j < K; ++j)
+                        add(j, 0);
+                  }
+                else
 #pragma unroll
-                      for (int j = 0; j < K; ++j)
-                        u[j] += zcr[j * NT];
+                  for (int j = 1; j < K; ++j)
+                    put(j, 0);
+                // corner line (0, 0)
+                if (r == 0 || lz == 0)
+                  {
+                    if (!jlo && !llo)
+                      add(0, 0);
+                  }
+                else
+                  put(0, 0);
+                // y = K row of the last row: high y face (all l); otherwise carried
+                if (ylast && !jhi)
+                  {
 #pragma unroll
-                    for (int l = 0; l < N; ++l)
-                      ycar[l] = u[l * N + K];
-                    if (!zlast)
+                    for (int l = 1; l < K; ++l)
+                      add(K, l);
+                    if (!llo)
+                      add(K, 0);
+                    if (!lhi)
+                      add(K, K);
+                  }
+                // z = K plane (j < K) of the last layer: high z face; otherwise carried
+                if (zlast && !lhi)
+                  {
 #pragma unroll
-                      for (int j = 0; j < K; ++j)
-                        zcr[j * NT] = u[K * N + j];
-                    // owned points j, l < K; brick faces (low y of row 0, low z of layer 0, high y of
-                    // the last row, high z of the last layer) atomically
-#pragma unroll
-                    for (int l = 0; l < N; ++l)
-#pragma unroll
-                      for (int j = 0; j < N; ++j)
-                        {
-                          if (j == K && !ylast)
-                            continue; // carried to the next row
-                          if (l == K && !zlast && j < K)
-                            continue; // carried to the next layer
-                          const int  off  = j * sy + l * sz;
-                          const T    v    = u[l * N + j];
-                          const bool face = (j == 0 && r == 0) || (l == 0 && lz == 0) || j == K || l == K;
-                          if (face)
-                            {
-                              const bool cn = (j == 0 && jlo) || (j == K && jhi) || (l == 0 && llo) || (l == K && lhi);
-                              if (!cn)
-                                atomicAdd(d0 + off, v);
-                            }
-                          else if constexpr (MODE == OutMode::Set)
-                            d0[off] = v;
-                          else if constexpr (MODE == OutMode::Add)
-                            d0[off] += v;
-                          else
-                            d0[off] = bvec[xbase + base + off] + v;
-                        }
+                    for (int j = 1; j < K; ++j)
+                      add(j, K);
+                    if (!jlo)
+                      add(0, K);
                   }
               }
             __syncthreads();

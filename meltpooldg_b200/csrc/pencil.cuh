@@ -17,7 +17,7 @@
 //      owned by the pencil are written with coalesced plain stores; points on the brick's faces
 //      are combined with global atomics, initialised by their owner through the ticket / flag
 //      handshake of brick.cuh.
-// The last x point of a full brick (x = 32 k) has no thread of its own: lanes 0..k of warp 0 process
+// The last x point of a full brick (x = 32 k) has no thread of its own: lanes 0..k of warp 1 process
 // that pencil cooperatively (one z line and one y line each, exchanged through shared memory).
 #pragma once
 
@@ -100,12 +100,15 @@ namespace mpdg
     const int  qx = p % K, cxp = p / K;       // x point = K cxp + qx
     const int  sy = br.sy, sz = br.sz;
     const int  xbase = br.g0[0] + (xin ? p : plast); // clamped: every load stays inside the lattice
-    const bool exl   = extra && warp == 0 && lane < N; // lanes of the cooperative pencil
+    // the cooperative pencil runs on warp 1, the extra round of x lines on the last warp and the x = 0
+    // face atomics on warp 0, so that no warp carries two of these
+    const bool exl   = extra && warp == 1 && lane < N; // lanes of the cooperative pencil
     const int  xbE   = br.g0[0] + K * BX;
     const bool xconE = br.con_hi[0] && extra;
     // first x line of this thread and the increments of (cell, mode) per round of NT lines
     constexpr int DCX = NT / M, DM = NT % M;
-    const int     cx_first = p / M, m_first = p % M;
+    const int     q_line   = (p + 32) % NT;   // the last warp starts at line 0
+    const int     cx_first = q_line / M, m_first = q_line % M;
 
     T ycar[N];
 #pragma unroll

@@ -45,7 +45,46 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--case", default=None,
+                    help="run one named case for profiling and exit: apply_<degree>_<cells>_<f64|f32> "
+                         "(e.g. apply_2_128_f32) or solve_fp64 / solve_mixed (128^3 FE_Q(2) CG to 1e-8)")
     return ap.parse_args()
+
+
+def run_case(name):
+    """One named case for profiling (no JSON contract): a few applies or one solve, timed with events."""
+    import torch
+
+    from meltpooldg_b200.build import build
+    from meltpooldg_b200.inputs import normal_cells, uniform_dofs
+    from meltpooldg_b200.operators import HeatDiffuseOperator, Mesh
+
+    build()
+    stream = torch.cuda.current_stream()
+    if name.startswith("apply_"):
+        _, deg, cells, prec = name.split("_")
+        mesh = Mesh(int(deg), (int(cells),) * 3, dirichlet_faces=63)
+        kc = np.exp(normal_cells(mesh, seed=2, sigma=0.5))
+        op = HeatDiffuseOperator(mesh, rho_cp=1.0, dt=1e-3, conductivity_cells=kc, stream=stream.cuda_stream)
+        dt = torch.float64 if prec == "f64" else torch.float32
+        x = torch.tensor(uniform_dofs(mesh, seed=1), dtype=dt, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(3):
+            op.vmult(y, x)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(10):
+            op.vmult(y, x)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        us = e0.elapsed_time(e1) / 10 * 1e3
+        print(json.dumps({"case": name, "us_per_apply": us, "gdofs": mesh.ndofs / us / 1e3}), flush=True)
+    elif name in ("solve_fp64", "solve_mixed"):
+        out = run_solves(torch, stream, modes=(name[6:],))
+        print(json.dumps({"case": name, **out}), flush=True)
+    else:
+        raise SystemExit(f"unknown case {name}")
 
 
 def dist_env():
@@ -192,7 +231,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_solves(torch, stream):
+def run_solves(torch, stream, modes=("fp64", "mixed")):
     """CG solve time to 1e-8: FP64 Jacobi-CG vs FP32-inner/FP64-outer defect correction on the
     128^3 FE_Q(2) problem (dt 1e-3, k = exp(N(0,0.5^2)) seed 3, b = U[-1,1] seed 3)."""
     from meltpooldg_b200.inputs import normal_cells, uniform_dofs
@@ -205,7 +244,7 @@ def run_solves(torch, stream):
     bd = torch.tensor(b, device="cuda")
     out = {"workload": "heat_cg_q2_128cube", "dofs": mesh.ndofs, "tol": 1e-8}
     res = {}
-    for mode in ("fp64", "mixed", "fp64", "mixed"):
+    for mode in modes + modes:
         x = torch.zeros_like(bd)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -223,15 +262,59 @@ def run_solves(torch, stream):
     xr = torch.zeros_like(bd)
     LinearSolver.solve(op, xr, bd, LinearSolverData("CG", "Diagonal", rel_tolerance=1e-12))
     nr = torch.linalg.norm(xr).item()
-    for mode in ("fp64", "mixed"):
+    for mode in modes:
         ms, its, x = res[mode]
         r = torch.empty_like(bd)
         op.residual(r, bd, x)
         out[mode] = {"ms": ms, "iterations": its,
                      "rel_residual": torch.linalg.norm(r).item() / torch.linalg.norm(bd).item(),
                      "rel_error_vs_fp64_1e-12": torch.linalg.norm(x - xr).item() / nr}
-    out["speedup_mixed_vs_fp64"] = res["fp64"][0] / res["mixed"][0]
+    if "fp64" in res and "mixed" in res:
+        out["speedup_mixed_vs_fp64"] = res["fp64"][0] / res["mixed"][0]
     return out
+
+
+def run_adjoint(torch, stream, fd_dirs=3):
+    """Adjoint of the transient heat problem: 48^3 FE_Q(2) cells, 20 implicit-Euler steps (dt 1e-3,
+    T0 = 0, homogeneous Dirichlet), moving Gaussian source A exp(-2|x - x0(t)|^2 / 0.05^2), A = 100,
+    x0(t) = (0.2 + 30 t, 0.5, 0.95); log k ~ N(0, 0.3^2) (seed 5), target from seed 6; checkpoints
+    every 5 steps.  Times J + dJ/dz (110,592 cells) + dJ/dA, and checks the gradient against central
+    differences (h = 1e-6) on a few random directions (seed 7)."""
+    from meltpooldg_b200.adjoint import TransientHeatAdjoint
+    from meltpooldg_b200.inputs import moving_gaussian, normal_cells, unit_directions
+    from meltpooldg_b200.operators import HeatDiffuseOperator, Mesh
+
+    mesh = Mesh(2, (48, 48, 48), dirichlet_faces=63)
+    steps, dt, amp = 20, 1e-3, 100.0
+    op = HeatDiffuseOperator(mesh, rho_cp=1.0, dt=dt, conductivity=1.0, stream=stream.cuda_stream)
+    adj = TransientHeatAdjoint(op, steps, checkpoint_every=5, cg_rel_tol=1e-12)
+    q = torch.tensor(moving_gaussian(mesh, steps, dt), device="cuda")
+    z = torch.tensor(normal_cells(mesh, seed=5, sigma=0.3), device="cuda")
+    zt = torch.tensor(normal_cells(mesh, seed=6, sigma=0.3), device="cuda")
+    target = torch.empty((steps, mesh.ndofs), dtype=torch.float64, device="cuda")
+    adj.forward(zt, q, amp, target)
+    grad = torch.empty(mesh.ncells, dtype=torch.float64, device="cuda")
+    times = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        J, gA, st = adj.objective_and_gradient(z, q, amp, target, grad)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    g = grad.cpu().numpy()
+    worst, h = 0.0, 1e-6
+    for d in unit_directions(mesh.ncells, fd_dirs, seed=7):
+        dd = torch.tensor(d, device="cuda")
+        jp, _, _ = adj.objective_and_gradient(z + h * dd, q, amp, target)
+        jm, _, _ = adj.objective_and_gradient(z - h * dd, q, amp, target)
+        fd = (jp - jm) / (2 * h)
+        worst = max(worst, abs(fd - float(g @ d)) / max(abs(fd), 1e-300))
+    return {"workload": "heat_adjoint_q2_48cube_20steps", "parameters": mesh.ncells + 1, "objective": J,
+            "ms_objective_and_gradient": min(times), "forward_solves": st.forward_solves,
+            "adjoint_solves": st.adjoint_solves, "cg_iterations": st.cg_iterations,
+            "fd_directions": fd_dirs, "fd_max_rel_err": worst}
 
 
 def mesh_mask(mesh):
@@ -243,6 +326,9 @@ def mesh_mask(mesh):
 
 def main():
     args = parse()
+    if args.case:
+        run_case(args.case)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -279,6 +365,12 @@ def main():
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
+    # untimed soak of the same apply (~0.5 s) so that the clock samples cover the GPU under this load
+    t_soak = time.perf_counter()
+    while time.perf_counter() - t_soak < 0.5:
+        for _ in range(20):
+            op.vmult(y, x)
+        torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -319,6 +411,12 @@ def main():
             solve = run_solves(torch, stream)
         except Exception as exc:  # report, never hide
             solve = {"error": repr(exc)}
+    adjoint = None
+    if not args.no_solve and rank == 0:
+        try:
+            adjoint = run_adjoint(torch, stream)
+        except Exception as exc:  # report, never hide
+            adjoint = {"error": repr(exc)}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
@@ -347,6 +445,7 @@ def main():
             "device_wait_errors": errs,
             "cpu_baseline": cpu,
             "solve": solve,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:

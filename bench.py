@@ -80,6 +80,8 @@ def run_case(name):
         torch.cuda.synchronize()
         us = e0.elapsed_time(e1) / 10 * 1e3
         print(json.dumps({"case": name, "us_per_apply": us, "gdofs": mesh.ndofs / us / 1e3}), flush=True)
+    elif name == "advection":
+        print(json.dumps({"case": name, **run_advection(torch, stream)}), flush=True)
     elif name in ("solve_fp64", "solve_mixed"):
         out = run_solves(torch, stream, modes=(name[6:],))
         print(json.dumps({"case": name, **out}), flush=True)
@@ -274,6 +276,51 @@ def run_solves(torch, stream, modes=("fp64", "mixed")):
     return out
 
 
+def run_advection(torch, stream, steps=10):
+    """Level-set advection-diffusion: 96^3 FE_Q(2) cells (7,189,057 DoFs) on the unit cube, M/dt + u.grad +
+    eps Laplacian with dt = 5e-3, eps = 1e-3, theta = 1 (implicit Euler), rigid rotation
+    u = (-(y - 0.5), x - 0.5, 0), natural boundaries; phi0 = 0.5 (1 - tanh((|x - (0.5, 0.75, 0.5)| - 0.25) / 0.01)).
+    10 steps of Jacobi-GMRES(30) to 1e-10 in FP64, then again with the FP32 operator inside an FP64
+    defect correction; reports both times and the difference of the final fields."""
+    from meltpooldg_b200.inputs import lattice_coords
+    from meltpooldg_b200.operators import AdvectionDiffusionOperator, LinearSolver, LinearSolverData, Mesh
+
+    mesh = Mesh(2, (96, 96, 96))
+    vel = [0.5, -0.5, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0]
+    op = AdvectionDiffusionOperator(mesh, dt=5e-3, theta=1.0, diffusivity=1e-3, velocity=vel,
+                                    stream=stream.cuda_stream)
+    X, Y, Z = lattice_coords(mesh)
+    phi0 = 0.5 * (1.0 - np.tanh((np.sqrt((X - 0.5) ** 2 + (Y - 0.75) ** 2 + (Z - 0.5) ** 2) - 0.25) / 0.01))
+    out = {"workload": "advdiff_q2_96cube_10steps", "dofs": mesh.ndofs, "tol": 1e-10}
+    finals = {}
+    for mode in ("fp64", "mixed", "fp64", "mixed"):
+        phi = torch.tensor(phi0, device="cuda")
+        rhs = torch.empty_like(phi)
+        its = 0
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            rhs.zero_()
+            op.create_rhs(rhs, phi)
+            x = phi.clone()
+            if mode == "fp64":
+                st = LinearSolver.solve(op, x, rhs, LinearSolverData("GMRES", "Diagonal", rel_tolerance=1e-10))
+                its += st.iterations
+            else:
+                st = LinearSolver.solve_mixed(op, x, rhs, outer_rel_tol=1e-10, inner_rel_tol=1e-4, solver="GMRES")
+                its += st.inner_iterations
+            phi = x
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[mode] = {"ms": e0.elapsed_time(e1), "iterations": its}
+        finals[mode] = phi
+    out["rel_diff_mixed_vs_fp64"] = (torch.linalg.norm(finals["mixed"] - finals["fp64"]) /
+                                     torch.linalg.norm(finals["fp64"])).item()
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
+    return out
+
+
 def run_adjoint(torch, stream, fd_dirs=3):
     """Adjoint of the transient heat problem: 48^3 FE_Q(2) cells, 20 implicit-Euler steps (dt 1e-3,
     T0 = 0, homogeneous Dirichlet), moving Gaussian source A exp(-2|x - x0(t)|^2 / 0.05^2), A = 100,
@@ -411,6 +458,12 @@ def main():
             solve = run_solves(torch, stream)
         except Exception as exc:  # report, never hide
             solve = {"error": repr(exc)}
+    advection = None
+    if not args.no_solve and rank == 0:
+        try:
+            advection = run_advection(torch, stream)
+        except Exception as exc:  # report, never hide
+            advection = {"error": repr(exc)}
     adjoint = None
     if not args.no_solve and rank == 0:
         try:
@@ -445,6 +498,7 @@ def main():
             "device_wait_errors": errs,
             "cpu_baseline": cpu,
             "solve": solve,
+            "advection": advection,
             "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)

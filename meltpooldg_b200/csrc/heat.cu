@@ -344,8 +344,21 @@ namespace mpdg
     }
   };
 
+#ifndef MPDG_MARCH_MINB_F64
+#define MPDG_MARCH_MINB_F64 5
+#endif
+#ifndef MPDG_MARCH_MINB_F32
+#define MPDG_MARCH_MINB_F32 7
+#endif
+  // CTAs per SM the register allocation of the column-marching kernel is held to
+  template <typename T>
+  struct MarchMinBlocks
+  {
+    static constexpr int value = sizeof(T) == 8 ? MPDG_MARCH_MINB_F64 : MPDG_MARCH_MINB_F32;
+  };
+
   template <int K, typename T, OutMode MODE>
-  __global__ void __launch_bounds__(MarchShape<K>::NT)
+  __global__ void __launch_bounds__(MarchShape<K>::NT, MarchMinBlocks<T>::value)
   heat_march_kernel(const __grid_constant__ HeatArgs<T, K + 1> a)
   {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -561,7 +574,7 @@ namespace mpdg
     a.mask_src = h.mask_src;
     a.skip     = h.skip;
     const unsigned nbricks = (unsigned)h.grid.nbr[0] * h.grid.nbr[1] * h.grid.nbr[2];
-    if constexpr (K <= 2)
+    if constexpr (K <= 2 && !(K == 2 && MPDG_PENCIL_K2))
       if (h.grid.cmask == nullptr && h.march)
       {
         using ML  = MarchLayout<K, T>;
@@ -577,7 +590,7 @@ namespace mpdg
         kern<<<nbricks, ML::S::NT, ML::bytes, stream>>>(a);
         return cudaGetLastError();
       }
-    if constexpr (K >= 3)
+    if constexpr (K >= 3 || (K == 2 && MPDG_PENCIL_K2))
       if (h.grid.cmask == nullptr && h.march)
       {
         using PL  = PencilLayout<K, T>;
@@ -626,7 +639,7 @@ namespace mpdg
   heat_brick_shape(int K, int shape[3], bool march)
   {
     brick_shape<T>(K, shape[0], shape[1], shape[2]);
-    if (march && K >= 3)
+    if (march && (K >= 3 || (K == 2 && MPDG_PENCIL_K2)))
       {
         shape[0] = PencilShape<3>::BX;
         shape[1] = PencilShape<3>::BY;

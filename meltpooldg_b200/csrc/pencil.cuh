@@ -30,8 +30,14 @@
 #ifndef MPDG_PENCIL_BZ
 #define MPDG_PENCIL_BZ 4
 #endif
+#ifndef MPDG_PENCIL_MINB2
+#define MPDG_PENCIL_MINB2 12
+#endif
 #ifndef MPDG_PENCIL_MINB3
 #define MPDG_PENCIL_MINB3 5
+#endif
+#ifndef MPDG_PENCIL_K2
+#define MPDG_PENCIL_K2 0
 #endif
 #ifndef MPDG_PENCIL_MINB4
 #define MPDG_PENCIL_MINB4 4
@@ -45,7 +51,7 @@ namespace mpdg
     static constexpr int N = K + 1, M = N * N;
     static constexpr int BX = 32, BY = MPDG_PENCIL_BY, BZ = MPDG_PENCIL_BZ;
     // CTAs per SM the register allocation is held to (K = 4: 4 x 128 threads at <= 128 registers)
-    static constexpr int MINB = K == 3 ? MPDG_PENCIL_MINB3 : MPDG_PENCIL_MINB4;
+    static constexpr int MINB = K == 2 ? MPDG_PENCIL_MINB2 : (K == 3 ? MPDG_PENCIL_MINB3 : MPDG_PENCIL_MINB4);
     static constexpr int NT = K * BX;        // threads: x points 0 .. K*BX-1
     static constexpr int TP = K * BX + 1;    // x points of the transposition buffer (odd)
     static constexpr int MP = M | 1;         // face-buffer stride (odd)

@@ -53,6 +53,16 @@ namespace mpdg
     int      *error;  // set to a nonzero code when a bounded wait gives up
   };
 
+  // Optional fused dot product of an apply dst = A src: the kernel sums src^T A src cell by cell and
+  // the last CTA sets *alpha = *rho / (sum) -- the step length of a CG iteration whose search
+  // direction is src.  Disabled when part == nullptr.
+  struct DotSink
+  {
+    double       *part  = nullptr; // one partial per brick
+    double       *alpha = nullptr;
+    const double *rho   = nullptr;
+  };
+
   constexpr unsigned SPIN_LIMIT    = 1u << 22; // x 32 ns sleeps: ~0.1-0.2 s
   constexpr int      ERR_FLAG_WAIT = 1;
   constexpr int      ERR_TICKET    = 2;
@@ -211,6 +221,59 @@ namespace mpdg
         __threadfence();
         if (atomicAdd(s.done, 1u) == gridDim.x - 1)
           {
+            *s.ticket = 0u;
+            *s.done   = 0u;
+            __threadfence();
+          }
+      }
+  }
+
+  // Sum of one double per thread over the CTA in a fixed order (valid in thread 0); scratch holds
+  // NT / 32 doubles and is reusable on return.
+  template <int NT>
+  __device__ __forceinline__ double
+  cta_sum(double v, double *scratch)
+  {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0)
+      scratch[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int w = 0; w < NT / 32; ++w)
+        t += scratch[w];
+    __syncthreads();
+    return t;
+  }
+
+  // release_ticket with the fused dot: every CTA stores the sum of its bricks' cell forms, the last
+  // CTA to finish adds the partials in brick order (deterministic) and sets the step length.
+  template <int NT>
+  __device__ __forceinline__ void
+  release_ticket_dot(const SyncDesc &s, const DotSink &d, unsigned id, double local, double *scratch,
+                     unsigned *s_flag)
+  {
+    const double t = cta_sum<NT>(local, scratch);
+    if (threadIdx.x == 0)
+      {
+        d.part[id] = t;
+        __threadfence();
+        *s_flag = atomicAdd(s.done, 1u) == gridDim.x - 1 ? 1u : 0u;
+      }
+    __syncthreads();
+    if (*s_flag)
+      {
+        __threadfence();
+        double acc = 0.0;
+        for (unsigned i = threadIdx.x; i < gridDim.x; i += NT)
+          acc += __ldcg(d.part + i);
+        const double tot = cta_sum<NT>(acc, scratch);
+        if (threadIdx.x == 0)
+          {
+            *d.alpha  = *d.rho / tot;
             *s.ticket = 0u;
             *s.done   = 0u;
             __threadfence();

@@ -89,6 +89,7 @@ struct mpdg_op
   int      *d_err  = nullptr;
   unsigned  epoch  = 0;
   double   *d_red  = nullptr; // reducer partials
+  double   *d_part = nullptr; // one partial per brick for the fused CG dot product (heat)
   double   *d_scal = nullptr; // 64 scalars
   CGState  *d_cg   = nullptr;
   CGState  *h_cg   = nullptr; // pinned mirror
@@ -202,7 +203,7 @@ namespace
   template <typename T>
   int
   apply(mpdg_op *op, int mode, double scale, T *dst, const T *src, const T *b, int mask_src, int which = 0,
-        const int *skip = nullptr)
+        const int *skip = nullptr, const DotSink *dot = nullptr)
   {
     if (op->kind == MPDG_HEAT)
       {
@@ -221,6 +222,8 @@ namespace
         h.mask_src = mask_src;
         h.skip     = skip;
         h.march    = op->d_mask == nullptr;
+        if (dot)
+          h.dot = *dot;
         MPDG_CUDA(heat_apply<T>(h, op->stream));
       }
     else
@@ -298,15 +301,24 @@ namespace
     if (int e = apply<T>(op, (int)OutMode::BPlus, -1.0, r, x, b, 1))
       return e;
     MPDG_CUDA(cg_init<T>(r, invd, p, op->d_cg, hist, op->reducer(), n, op->stream));
+    // heat operators without a per-DoF mask fuse p^T A p into the apply and set alpha on the device
+    const bool fused = op->kind == MPDG_HEAT && op->d_part != nullptr &&
+                       heat_apply_fuses_dot(op->degree, op->d_mask != nullptr, true);
+    DotSink    sink;
+    sink.part  = op->d_part;
+    sink.alpha = &op->d_cg->alpha;
+    sink.rho   = &op->d_cg->rho;
     int batch = 4;
     for (;;)
       {
         for (int k = 0; k < batch; ++k)
           {
             MPDG_CUDA(cg_update_p<T>(r, invd, p, op->d_cg, n, op->stream));
-            if (int e = apply<T>(op, (int)OutMode::Set, 1.0, v, p, nullptr, 1, 0, &op->d_cg->done))
+            if (int e = apply<T>(op, (int)OutMode::Set, 1.0, v, p, nullptr, 1, 0, &op->d_cg->done,
+                                 fused ? &sink : nullptr))
               return e;
-            MPDG_CUDA(cg_alpha<T>(p, v, op->d_cg, op->reducer(), n, op->stream));
+            if (!fused)
+              MPDG_CUDA(cg_alpha<T>(p, v, op->d_cg, op->reducer(), n, op->stream));
             MPDG_CUDA(cg_update_xr<T>(x, r, p, v, invd, op->d_cg, hist, op->reducer(), n, op->stream));
           }
         MPDG_CUDA(cudaMemcpyAsync(op->h_cg, op->d_cg, sizeof(CGState), cudaMemcpyDeviceToHost, op->stream));
@@ -571,6 +583,8 @@ mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op
       cudaMallocHost(&op->h_cg, sizeof(CGState)) != cudaSuccess ||
       cudaMallocHost(&op->h_scal, sizeof(double) * 64) != cudaSuccess)
     return clean(MPDG_ERR_NOMEM, "device allocation in mpdg_op_create");
+  if (op->kind == MPDG_HEAT && cudaMalloc(&op->d_part, sizeof(double) * nbrk) != cudaSuccess)
+    return clean(MPDG_ERR_NOMEM, "fused dot partials");
   if (cudaMemset(op->d_sync, 0, sizeof(unsigned) * (3 + nbrk)) != cudaSuccess ||
       cudaMemset(op->d_err, 0, sizeof(int)) != cudaSuccess)
     return clean(MPDG_ERR_CUDA, "cudaMemset in mpdg_op_create");
@@ -613,6 +627,7 @@ mpdg_op_destroy(mpdg_op *op)
   cudaFree(op->d_sync);
   cudaFree(op->d_err);
   cudaFree(op->d_red);
+  cudaFree(op->d_part);
   cudaFree(op->d_scal);
   cudaFree(op->d_cg);
   cudaFree(op->d_mask);

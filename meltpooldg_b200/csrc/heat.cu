@@ -13,6 +13,7 @@
 // (no ordering between cells that share lattice points is needed).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <mutex>
 #include <set>
 
@@ -55,6 +56,7 @@ namespace mpdg
     const T   *b;      // BPlus mode: dst = b + A src (may alias dst)
     int        mask_src;
     const int *skip;   // return at once when *skip != 0 (a solve has finished)
+    DotSink    dot;    // fused src^T A src (CG step length), see brick.cuh
   };
 
   template <int K, typename T>
@@ -306,9 +308,11 @@ namespace mpdg
   {
     static constexpr int N = K + 1, NE = (N + 1) / 2, NO = N / 2;
     const HeatArgs<T, N> &a;
-    __device__ __forceinline__ void
+    template <bool DOT>
+    __device__ __forceinline__ double
     apply(T *u, bool valid, int cx, int cy, int cz) const
     {
+      T form = T(0);
       T kc = T(0);
       if (valid)
         {
@@ -334,13 +338,20 @@ namespace mpdg
               const T tyz = fma(kcy, lam[b], tz);
 #pragma unroll
               for (int aa = 0; aa < N; ++aa)
-                u[(c * N + b) * N + aa] *= fma(kcx, lam[aa], tyz);
+                {
+                  const T d = fma(kcx, lam[aa], tyz);
+                  T      &v = u[(c * N + b) * N + aa];
+                  if constexpr (DOT)
+                    form = fma(d * v, v, form);
+                  v *= d;
+                }
             }
         }
 #pragma unroll
       for (int q = 0; q < N * N; ++q)
         bwd_line<T, N, N * N>(u, q, we, wo);
       xy_planes<T, N, N, false>(u, we, wo);
+      return (double)form;
     }
   };
 
@@ -357,17 +368,18 @@ namespace mpdg
     static constexpr int value = sizeof(T) == 8 ? MPDG_MARCH_MINB_F64 : MPDG_MARCH_MINB_F32;
   };
 
-  template <int K, typename T, OutMode MODE>
+  template <int K, typename T, OutMode MODE, bool DOT>
   __global__ void __launch_bounds__(MarchShape<K>::NT, MarchMinBlocks<T>::value)
   heat_march_kernel(const __grid_constant__ HeatArgs<T, K + 1> a)
   {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned s_ticket;
+    __shared__ double   s_red[MarchShape<K>::NT / 32];
     if (a.skip != nullptr && *a.skip != 0)
       return;
     HeatCellOp<K, T> op{a};
-    march_body<K, T, MODE>(a.g, a.s, a.src, a.dst, a.b, a.mask_src != 0, op, reinterpret_cast<T *>(smem_raw),
-                           &s_ticket);
+    march_body<K, T, MODE, HeatCellOp<K, T>, DOT>(a.g, a.s, a.src, a.dst, a.b, a.mask_src != 0, op,
+                                                  reinterpret_cast<T *>(smem_raw), &s_ticket, a.dot, s_red);
   }
 
   // ---- k >= 3: pencil-marching apply (pencil.cuh); the x lines are scaled by the diagonal of the
@@ -421,17 +433,18 @@ namespace mpdg
     }
   };
 
-  template <int K, typename T, OutMode MODE>
+  template <int K, typename T, OutMode MODE, bool DOT>
   __global__ void __launch_bounds__(PencilShape<K>::NT, PencilShape<K>::MINB)
   heat_pencil_kernel(const __grid_constant__ HeatArgs<T, K + 1> a)
   {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned s_ticket;
+    __shared__ double   s_red[PencilShape<K>::NT / 32];
     if (a.skip != nullptr && *a.skip != 0)
       return;
     HeatPencilOp<K, T> op{a};
-    pencil_body<K, T, MODE>(a.g, a.s, a.src, a.dst, a.b, a.mask_src != 0, op, reinterpret_cast<T *>(smem_raw),
-                            &s_ticket);
+    pencil_body<K, T, MODE, HeatPencilOp<K, T>, DOT>(a.g, a.s, a.src, a.dst, a.b, a.mask_src != 0, op,
+                                                     reinterpret_cast<T *>(smem_raw), &s_ticket, a.dot, s_red);
   }
 
   // ---- diagonal: closed-form per-cell entries gathered per DoF (deterministic, no atomics)
@@ -550,6 +563,24 @@ namespace mpdg
     return cudaSuccess;
   }
 
+  // Dynamic shared memory above 48 KB is opted into once per kernel and device.
+  template <class F>
+  static cudaError_t
+  ensure_smem(F kern, size_t bytes, std::atomic<unsigned long long> &devices)
+  {
+    int         dev = 0;
+    cudaError_t e   = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+      return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (devices.load() & bit)
+      return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess)
+      devices.fetch_or(bit);
+    return e;
+  }
+
   template <int K, typename T, OutMode MODE>
   static cudaError_t
   launch_apply(const HeatLaunch<T> &h, cudaStream_t stream)
@@ -573,39 +604,54 @@ namespace mpdg
     a.b        = h.b;
     a.mask_src = h.mask_src;
     a.skip     = h.skip;
+    a.dot      = h.dot;
     const unsigned nbricks = (unsigned)h.grid.nbr[0] * h.grid.nbr[1] * h.grid.nbr[2];
-    if constexpr (K <= 2 && !(K == 2 && MPDG_PENCIL_K2))
+    if constexpr (K <= 2)
       if (h.grid.cmask == nullptr && h.march)
-      {
-        using ML  = MarchLayout<K, T>;
-        auto kern = heat_march_kernel<K, T, MODE>;
-        static thread_local bool attr_done = false;
-        if (!attr_done)
-          {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ML::bytes);
-            if (e != cudaSuccess)
-              return e;
-            attr_done = true;
-          }
-        kern<<<nbricks, ML::S::NT, ML::bytes, stream>>>(a);
-        return cudaGetLastError();
-      }
-    if constexpr (K >= 3 || (K == 2 && MPDG_PENCIL_K2))
+        {
+          using ML = MarchLayout<K, T>;
+          static std::atomic<unsigned long long> dev_plain{0}, dev_dot{0};
+          if constexpr (MODE == OutMode::Set)
+            if (h.dot.part != nullptr)
+              {
+                auto        kern = heat_march_kernel<K, T, MODE, true>;
+                cudaError_t e    = ensure_smem(kern, ML::bytes, dev_dot);
+                if (e != cudaSuccess)
+                  return e;
+                kern<<<nbricks, ML::S::NT, ML::bytes, stream>>>(a);
+                return cudaGetLastError();
+              }
+          auto        kern = heat_march_kernel<K, T, MODE, false>;
+          cudaError_t e    = ensure_smem(kern, ML::bytes, dev_plain);
+          if (e != cudaSuccess)
+            return e;
+          kern<<<nbricks, ML::S::NT, ML::bytes, stream>>>(a);
+          return cudaGetLastError();
+        }
+    if constexpr (K >= 3)
       if (h.grid.cmask == nullptr && h.march)
-      {
-        using PL  = PencilLayout<K, T>;
-        auto kern = heat_pencil_kernel<K, T, MODE>;
-        static thread_local bool attr_done = false;
-        if (!attr_done)
-          {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::bytes);
-            if (e != cudaSuccess)
-              return e;
-            attr_done = true;
-          }
-        kern<<<nbricks, PL::S::NT, PL::bytes, stream>>>(a);
-        return cudaGetLastError();
-      }
+        {
+          using PL = PencilLayout<K, T>;
+          static std::atomic<unsigned long long> dev_plain{0}, dev_dot{0};
+          if constexpr (MODE == OutMode::Set)
+            if (h.dot.part != nullptr)
+              {
+                auto        kern = heat_pencil_kernel<K, T, MODE, true>;
+                cudaError_t e    = ensure_smem(kern, PL::bytes, dev_dot);
+                if (e != cudaSuccess)
+                  return e;
+                kern<<<nbricks, PL::S::NT, PL::bytes, stream>>>(a);
+                return cudaGetLastError();
+              }
+          auto        kern = heat_pencil_kernel<K, T, MODE, false>;
+          cudaError_t e    = ensure_smem(kern, PL::bytes, dev_plain);
+          if (e != cudaSuccess)
+            return e;
+          kern<<<nbricks, PL::S::NT, PL::bytes, stream>>>(a);
+          return cudaGetLastError();
+        }
+    if (h.dot.part != nullptr)
+      return cudaErrorInvalidValue; // the brick kernel has no fused dot (heat_apply_fuses_dot is false)
     {
         auto kern = heat_apply_kernel<K, T, MODE>;
         static thread_local bool attr_done = false;
@@ -639,7 +685,7 @@ namespace mpdg
   heat_brick_shape(int K, int shape[3], bool march)
   {
     brick_shape<T>(K, shape[0], shape[1], shape[2]);
-    if (march && (K >= 3 || (K == 2 && MPDG_PENCIL_K2)))
+    if (march && K >= 3)
       {
         shape[0] = PencilShape<3>::BX;
         shape[1] = PencilShape<3>::BY;
@@ -666,6 +712,12 @@ namespace mpdg
         case 1: return launch_apply<K, T, OutMode::Add>(h, s);
         default: return launch_apply<K, T, OutMode::BPlus>(h, s);
       }
+  }
+
+  bool
+  heat_apply_fuses_dot(int K, bool has_dof_mask, bool march)
+  {
+    return K >= 1 && K <= 4 && !has_dof_mask && march;
   }
 
   template <typename T>

@@ -33,8 +33,12 @@ namespace mpdg
     const T    *b        = nullptr;
     int         mask_src = 1;
     const int  *skip     = nullptr; // device flag: return at once when nonzero
-    bool        march    = true;    // k <= 2: column-marching kernel (operator without per-DoF mask)
+    bool        march    = true;    // column-marching / pencil kernels (operator without per-DoF mask)
+    DotSink     dot{};              // fused src^T A src -> CG step length (Set mode, heat_apply_fuses_dot)
   };
+
+  // whether the apply kernel chosen for these settings can fuse the CG dot product (DotSink)
+  bool heat_apply_fuses_dot(int K, bool has_dof_mask, bool march);
 
   template <typename T>
   cudaError_t heat_apply(const HeatLaunch<T> &h, cudaStream_t s);

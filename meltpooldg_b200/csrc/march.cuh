@@ -67,11 +67,14 @@ namespace mpdg
   }
 
   // The marching body.  Cell operator: Op::apply(u, valid, cx, cy, cz) in place on (k+1)^3 values.
-  template <int K, typename T, OutMode MODE, class Op>
+  // With DOT the cell operator returns the cell's form src_c^T A_c src_c and the sum over the brick
+  // goes to the fused dot product (release_ticket_dot).
+  template <int K, typename T, OutMode MODE, class Op, bool DOT = false>
   __device__ __forceinline__ void
   march_body(const GridDesc &g, const SyncDesc &s, const T *src, T *dst, const T *bvec, bool mask_src, const Op &op,
-             T *smem, unsigned *s_ticket)
+             T *smem, unsigned *s_ticket, const DotSink &dot = DotSink{}, double *s_red = nullptr)
   {
+    double dsum = 0.0;
     using LAY       = MarchLayout<K, T>;
     using BR        = typename LAY::BR;
     constexpr int N = K + 1, PX = LAY::PX, PY = LAY::PY, BZ = LAY::S::BZ;
@@ -119,7 +122,10 @@ namespace mpdg
 #pragma unroll
             for (int i = 0; i < N; ++i)
               u[(l * N + j) * N + i] = vxy ? cur[(l * PY + K * warp + j) * PX + K * lane + i] : T(0);
-        op.apply(u, vxy, cx, cy, cz);
+        if constexpr (DOT)
+          dsum += op.template apply<true>(u, vxy, cx, cy, cz);
+        else
+          op.template apply<false>(u, vxy, cx, cy, cz);
         // x: lane t adds lane t-1's x = K face; only the last lane keeps its own
 #pragma unroll
         for (int q = 0; q < N * N; ++q)
@@ -215,7 +221,9 @@ namespace mpdg
           }
         __syncthreads();
       }
-    if constexpr (MODE != OutMode::Add)
+    if constexpr (DOT)
+      release_ticket_dot<LAY::S::NT>(s, dot, br.id, dsum, s_red, s_ticket);
+    else if constexpr (MODE != OutMode::Add)
       release_ticket(s);
   }
 } // namespace mpdg

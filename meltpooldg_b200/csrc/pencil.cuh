@@ -30,15 +30,10 @@
 #ifndef MPDG_PENCIL_BZ
 #define MPDG_PENCIL_BZ 4
 #endif
-#ifndef MPDG_PENCIL_MINB2
-#define MPDG_PENCIL_MINB2 12
-#endif
 #ifndef MPDG_PENCIL_MINB3
 #define MPDG_PENCIL_MINB3 5
 #endif
-#ifndef MPDG_PENCIL_K2
-#define MPDG_PENCIL_K2 0
-#endif
+
 #ifndef MPDG_PENCIL_MINB4
 #define MPDG_PENCIL_MINB4 4
 #endif
@@ -51,7 +46,7 @@ namespace mpdg
     static constexpr int N = K + 1, M = N * N;
     static constexpr int BX = 32, BY = MPDG_PENCIL_BY, BZ = MPDG_PENCIL_BZ;
     // CTAs per SM the register allocation is held to (K = 4: 4 x 128 threads at <= 128 registers)
-    static constexpr int MINB = K == 2 ? MPDG_PENCIL_MINB2 : (K == 3 ? MPDG_PENCIL_MINB3 : MPDG_PENCIL_MINB4);
+    static constexpr int MINB = K == 3 ? MPDG_PENCIL_MINB3 : MPDG_PENCIL_MINB4;
     static constexpr int NT = K * BX;        // threads: x points 0 .. K*BX-1
     static constexpr int TP = K * BX + 1;    // x points of the transposition buffer (odd)
     static constexpr int MP = M | 1;         // face-buffer stride (odd)
@@ -73,11 +68,14 @@ namespace mpdg
 
   // Op supplies the fast-diagonalisation tables and the per-cell scaling:
   //   we(), wo(), lam()  1-D tables;  alpha(), cxg(), cyg(), czg()  geometry;  kcell(cell)  k_c.
-  template <int K, typename T, OutMode MODE, class Op>
+  // With DOT the x lines also add d_mode * (modal value)^2, i.e. the cells' forms src_c^T A_c src_c,
+  // to the fused dot product (release_ticket_dot).
+  template <int K, typename T, OutMode MODE, class Op, bool DOT = false>
   __device__ __forceinline__ void
   pencil_body(const GridDesc &g, const SyncDesc &s, const T *src, T *dst, const T *bvec, bool mask_src, const Op &op,
-              T *smem, unsigned *s_ticket)
+              T *smem, unsigned *s_ticket, const DotSink &dot = DotSink{}, double *s_red = nullptr)
   {
+    double dsum = 0.0;
     using LAY       = PencilLayout<K, T>;
     using SH        = typename LAY::S;
     using BR        = typename LAY::BR;
@@ -219,9 +217,17 @@ namespace mpdg
                   const T kc   = kcs[cx];
                   const T beta = fma(kc, mus[m], alpha);
                   const T kcx  = kc * cxg;
+                  T form = T(0);
 #pragma unroll
                   for (int i = 0; i < N; ++i)
-                    x[i] *= fma(kcx, lam[i], beta);
+                    {
+                      const T d = fma(kcx, lam[i], beta);
+                      if constexpr (DOT)
+                        form = fma(d * x[i], x[i], form);
+                      x[i] *= d;
+                    }
+                  if constexpr (DOT)
+                    dsum += (double)form;
                   bwd_line<T, N, 1>(x, 0, we, wo);
 #pragma unroll
                   for (int i = 1; i < K; ++i)
@@ -394,7 +400,9 @@ namespace mpdg
             __syncthreads();
           }
       }
-    if constexpr (MODE != OutMode::Add)
+    if constexpr (DOT)
+      release_ticket_dot<NT>(s, dot, br.id, dsum, s_red, s_ticket);
+    else if constexpr (MODE != OutMode::Add)
       release_ticket(s);
   }
 } // namespace mpdg

@@ -148,18 +148,53 @@ namespace mpdg
       });
     }
 
+    // 16-byte packs for the streaming CG kernels (4 floats / 2 doubles per access)
+    template <typename T>
+    struct Pack;
+    template <>
+    struct Pack<float>
+    {
+      using V                  = float4;
+      static constexpr int W   = 4;
+      __device__ static float &at(V &v, int k) { return (&v.x)[k]; }
+    };
+    template <>
+    struct Pack<double>
+    {
+      using V                  = double2;
+      static constexpr int W   = 2;
+      __device__ static double &at(V &v, int k) { return (&v.x)[k]; }
+    };
+
     template <typename T>
     __global__ void
     cg_update_p_kernel(const T *__restrict__ r, const T *__restrict__ invd, T *__restrict__ p, const CGState *st,
-                       long long n)
+                       long long n, int packed)
     {
       if (st->done)
         return;
-      const T beta = (T)st->beta;
-      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      const T         beta  = (T)st->beta;
+      const bool      first = st->it == 0;
+      const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+      using P               = Pack<T>;
+      const long long nv    = packed ? n / P::W : 0;
+      for (long long i = tid; i < nv; i += stride)
+        {
+          typename P::V rv = reinterpret_cast<const typename P::V *>(r)[i];
+          typename P::V dv = invd ? reinterpret_cast<const typename P::V *>(invd)[i] : rv;
+          typename P::V pv = first ? rv : reinterpret_cast<const typename P::V *>(p)[i];
+#pragma unroll
+          for (int k = 0; k < P::W; ++k)
+            {
+              const T z    = invd ? P::at(rv, k) * P::at(dv, k) : P::at(rv, k);
+              P::at(pv, k) = first ? z : z + beta * P::at(pv, k);
+            }
+          reinterpret_cast<typename P::V *>(p)[i] = pv;
+        }
+      for (long long i = nv * P::W + tid; i < n; i += stride)
         {
           const T z = invd ? r[i] * invd[i] : r[i];
-          p[i]      = (st->it == 0) ? z : z + beta * p[i];
+          p[i]      = first ? z : z + beta * p[i];
         }
     }
 
@@ -178,13 +213,37 @@ namespace mpdg
     template <typename T>
     __global__ void
     cg_update_xr_kernel(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p, const T *__restrict__ v,
-                        const T *__restrict__ invd, CGState *st, double *hist, Reducer red, long long n)
+                        const T *__restrict__ invd, CGState *st, double *hist, Reducer red, long long n, int packed)
     {
       if (st->done)
         return;
       const T alpha = (T)st->alpha;
       double  a[2]  = {0.0, 0.0};
-      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+      using P               = Pack<T>;
+      const long long nv    = packed ? n / P::W : 0;
+      for (long long i = tid; i < nv; i += stride)
+        {
+          using V = typename P::V;
+          V xv = reinterpret_cast<const V *>(x)[i], rv = reinterpret_cast<const V *>(r)[i];
+          V pv = reinterpret_cast<const V *>(p)[i], vv = reinterpret_cast<const V *>(v)[i];
+          V dv = rv;
+          if (invd)
+            dv = reinterpret_cast<const V *>(invd)[i];
+#pragma unroll
+          for (int k = 0; k < P::W; ++k)
+            {
+              P::at(xv, k) += alpha * P::at(pv, k);
+              const T ri   = P::at(rv, k) - alpha * P::at(vv, k);
+              P::at(rv, k) = ri;
+              const T zi   = invd ? ri * P::at(dv, k) : ri;
+              a[0] += (double)ri * (double)ri;
+              a[1] += (double)ri * (double)zi;
+            }
+          reinterpret_cast<V *>(x)[i] = xv;
+          reinterpret_cast<V *>(r)[i] = rv;
+        }
+      for (long long i = nv * P::W + tid; i < n; i += stride)
         {
           x[i] += alpha * p[i];
           const T ri = r[i] - alpha * v[i];
@@ -392,6 +451,12 @@ namespace mpdg
     }
 
     inline int
+    aligned16(const void *p)
+    {
+      return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; // null counts as aligned (unused operand)
+    }
+
+    int
     stream_blocks(long long n)
     {
       const long long b = (n + 255) / 256;
@@ -411,7 +476,8 @@ namespace mpdg
   cudaError_t
   cg_update_p(const T *r, const T *invd, T *p, const CGState *st, long long n, cudaStream_t s)
   {
-    cg_update_p_kernel<T><<<stream_blocks(n), 256, 0, s>>>(r, invd, p, st, n);
+    const int packed = aligned16(r) && aligned16(invd) && aligned16(p);
+    cg_update_p_kernel<T><<<stream_blocks(packed ? (n + 3) / 4 : n), 256, 0, s>>>(r, invd, p, st, n, packed);
     return cudaGetLastError();
   }
   template <typename T>
@@ -426,7 +492,8 @@ namespace mpdg
   cg_update_xr(T *x, T *r, const T *p, const T *v, const T *invd, CGState *st, double *hist, Reducer red,
                long long n, cudaStream_t s)
   {
-    cg_update_xr_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(x, r, p, v, invd, st, hist, red, n);
+    const int packed = aligned16(x) && aligned16(r) && aligned16(p) && aligned16(v) && aligned16(invd);
+    cg_update_xr_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(x, r, p, v, invd, st, hist, red, n, packed);
     return cudaGetLastError();
   }
 

@@ -253,6 +253,15 @@ MPDG_API int mpdg_heat_cell_stiffness_form(mpdg_op *op, const double *lam, const
 MPDG_API int mpdg_heat_vmult_noalloc(const mpdg_mesh_desc *mesh, const mpdg_op_params *params,
                                      const double *k_cells_dev, double *dst, const double *src, void *cuda_stream);
 
+/* Vector operations on the handle's stream over n_dofs entries (device arrays), as used by the
+   reference's Newton loop on distributed vectors (source/linear_algebra/newton_raphson_solver.cpp:
+   rhs = 0 and solution_update = 0 at :163-164, solution += solution_update at :75, l2_norm in
+   is_converged at :121-122).  mpdg_vec_axpby: y = a x + b y (x == NULL means 0).  mpdg_vec_norm:
+   Euclidean norm, deterministic (fixed summation order), written to *out (host). */
+MPDG_API int mpdg_vec_fill(mpdg_op *op, double *x, double value);
+MPDG_API int mpdg_vec_axpby(mpdg_op *op, double *y, double a, const double *x, double b);
+MPDG_API int mpdg_vec_norm(mpdg_op *op, const double *x, double *out);
+
 /* Number of error words raised by bounded device waits since the last call (and reset). */
 MPDG_API int mpdg_op_device_errors(mpdg_op *op);
 

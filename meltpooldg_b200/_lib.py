@@ -133,6 +133,9 @@ SIGNATURES = [
     ("mpdg_adjoint_heat", [P, P, P, D, P, C.POINTER(AdjointParams), P, C.POINTER(AdjointResult)], C.c_int),
     ("mpdg_heat_forward", [P, P, P, D, C.POINTER(AdjointParams), P], C.c_int),
     ("mpdg_heat_cell_stiffness_form", [P, P, P, P], C.c_int),
+    ("mpdg_vec_fill", [P, P, D], C.c_int),
+    ("mpdg_vec_axpby", [P, P, D, P, D], C.c_int),
+    ("mpdg_vec_norm", [P, P, C.POINTER(D)], C.c_int),
     ("mpdg_heat_vmult_noalloc", [P, P, P, P, P, P], C.c_int),
     ("mpdg_last_error", [], C.c_char_p),
 ]

@@ -1101,6 +1101,42 @@ mpdg_heat_cell_stiffness_form(mpdg_op *op, const double *lam, const double *T, d
 }
 
 int
+mpdg_vec_fill(mpdg_op *op, double *x, double value)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!x)
+    return fail(MPDG_ERR_ARG, "null vector passed to mpdg_vec_fill");
+  MPDG_CUDA(vec_fill<double>(x, value, op->ndofs, op->stream));
+  return MPDG_OK;
+}
+
+int
+mpdg_vec_axpby(mpdg_op *op, double *y, double a, const double *x, double b)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!y)
+    return fail(MPDG_ERR_ARG, "null vector passed to mpdg_vec_axpby");
+  MPDG_CUDA(vec_axpby<double>(y, a, x, b, y, op->ndofs, op->stream));
+  return MPDG_OK;
+}
+
+int
+mpdg_vec_norm(mpdg_op *op, const double *x, double *out)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!x || !out)
+    return fail(MPDG_ERR_ARG, "null argument to mpdg_vec_norm");
+  MPDG_CUDA(vec_multidot<double>(&x, &x, 1, op->ndofs, op->d_scal, op->reducer(), op->stream));
+  MPDG_CUDA(cudaMemcpyAsync(op->h_scal, op->d_scal, sizeof(double), cudaMemcpyDeviceToHost, op->stream));
+  MPDG_CUDA(cudaStreamSynchronize(op->stream));
+  *out = std::sqrt(op->h_scal[0]);
+  return MPDG_OK;
+}
+
+int
 mpdg_op_device_errors(mpdg_op *op)
 {
   if (!op)

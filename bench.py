@@ -80,6 +80,22 @@ def run_case(name):
         torch.cuda.synchronize()
         us = e0.elapsed_time(e1) / 10 * 1e3
         print(json.dumps({"case": name, "us_per_apply": us, "gdofs": mesh.ndofs / us / 1e3}), flush=True)
+    elif name.startswith("diag_"):
+        _, deg, cells = name.split("_")
+        mesh = Mesh(int(deg), (int(cells),) * 3, dirichlet_faces=63)
+        kc = np.exp(normal_cells(mesh, seed=2, sigma=0.5))
+        op = HeatDiffuseOperator(mesh, rho_cp=1.0, dt=1e-3, conductivity_cells=kc, stream=stream.cuda_stream)
+        d = torch.empty(mesh.ndofs, dtype=torch.float64, device="cuda")
+        for _ in range(3):
+            op.compute_inverse_diagonal_from_matrixfree(d)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(10):
+            op.compute_inverse_diagonal_from_matrixfree(d)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": name, "us_per_inverse_diagonal": e0.elapsed_time(e1) / 10 * 1e3}), flush=True)
     elif name == "advection":
         print(json.dumps({"case": name, **run_advection(torch, stream)}), flush=True)
     elif name in ("solve_fp64", "solve_mixed"):

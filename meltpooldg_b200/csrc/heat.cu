@@ -462,65 +462,76 @@ namespace mpdg
     int      invert;
   };
 
-  template <typename T>
+  // The cells that share lattice index P along one direction (1 or 2) and P's local index in each.
+  template <int K>
+  struct Neighbours1D
+  {
+    int  c[2], l[2];
+    bool v[2];
+    __device__ __forceinline__
+    Neighbours1D(int P, int m)
+    {
+      const int q = P / K, r = P - q * K;
+      if (r == 0)
+        {
+          c[0] = q - 1, l[0] = K, v[0] = q - 1 >= 0;
+          c[1] = q, l[1] = 0, v[1] = q < m;
+        }
+      else
+        {
+          c[0] = q, l[0] = r, v[0] = true;
+          c[1] = q, l[1] = r, v[1] = false;
+        }
+    }
+  };
+
+  // One CTA per lattice row (J, L) in a grid-stride loop, threads along x (coalesced stores); the
+  // diagonal entry is the sum over the (up to 8) cells sharing the point of the tensor-product form
+  // a Mx My Mz + k_c (cx Kx My Mz + cy Mx Ky Mz + cz Mx My Kz) at the point's local indices.
+  template <int K, typename T>
   __global__ void
   heat_diag_kernel(const __grid_constant__ DiagArgs<T> a)
   {
-    const long long ndofs = (long long)a.g.n[0] * a.g.n[1] * a.g.n[2];
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < ndofs;
-         idx += (long long)gridDim.x * blockDim.x)
+    const int       n0 = a.g.n[0], n1 = a.g.n[1];
+    const long long rows = (long long)n1 * a.g.n[2];
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x)
       {
-        const int I = (int)(idx % a.g.n[0]), J = (int)((idx / a.g.n[0]) % a.g.n[1]),
-                  L = (int)(idx / ((long long)a.g.n[0] * a.g.n[1]));
-        T d;
-        if (is_constrained(a.g, I, J, L, idx))
-          d = T(1);
-        else
+        const int        J = (int)(row % n1), L = (int)(row / n1);
+        const Neighbours1D<K> ny(J, a.g.m[1]), nz(L, a.g.m[2]);
+        const bool rowcon = ((a.g.faces & 4u) && J == 0) || ((a.g.faces & 8u) && J == n1 - 1) ||
+                            ((a.g.faces & 16u) && L == 0) || ((a.g.faces & 32u) && L == a.g.n[2] - 1);
+        for (int I = threadIdx.x; I < n0; I += blockDim.x)
           {
-            int       cs[3][2], ls[3][2], nc[3];
-            const int P[3] = {I, J, L};
-            for (int dd = 0; dd < 3; ++dd)
+            const long long idx = (long long)I + (long long)n0 * row;
+            bool con = rowcon || ((a.g.faces & 1u) && I == 0) || ((a.g.faces & 2u) && I == n0 - 1);
+            if (a.g.cmask != nullptr && a.g.cmask[idx] != 0)
+              con = true;
+            T d = T(0);
+            if (!con)
               {
-                nc[dd]      = 0;
-                const int q = P[dd] / a.K, r = P[dd] % a.K;
-                if (r == 0)
-                  {
-                    if (q - 1 >= 0)
-                      {
-                        cs[dd][nc[dd]] = q - 1;
-                        ls[dd][nc[dd]] = a.K;
-                        ++nc[dd];
-                      }
-                    if (q < a.g.m[dd])
-                      {
-                        cs[dd][nc[dd]] = q;
-                        ls[dd][nc[dd]] = 0;
-                        ++nc[dd];
-                      }
-                  }
-                else
-                  {
-                    cs[dd][0] = q;
-                    ls[dd][0] = r;
-                    nc[dd]    = 1;
-                  }
+                const Neighbours1D<K> nx(I, a.g.m[0]);
+#pragma unroll
+                for (int z = 0; z < 2; ++z)
+#pragma unroll
+                  for (int y = 0; y < 2; ++y)
+#pragma unroll
+                    for (int x = 0; x < 2; ++x)
+                      if (nx.v[x] && ny.v[y] && nz.v[z])
+                        {
+                          const long long cell = (long long)nx.c[x] +
+                                                 (long long)a.g.m[0] * ((long long)ny.c[y] + (long long)a.g.m[1] * nz.c[z]);
+                          const T kc = a.kcell ? a.kcell[cell] : a.kconst;
+                          const T mx = a.mdiag[nx.l[x]], my = a.mdiag[ny.l[y]], mz = a.mdiag[nz.l[z]];
+                          const T kx = a.kdiag[nx.l[x]], ky = a.kdiag[ny.l[y]], kz = a.kdiag[nz.l[z]];
+                          d += a.alpha * mx * my * mz + kc * (a.cx * kx * my * mz + a.cy * mx * ky * mz + a.cz * mx * my * kz);
+                        }
               }
-            d = T(0);
-            for (int z = 0; z < nc[2]; ++z)
-              for (int y = 0; y < nc[1]; ++y)
-                for (int x = 0; x < nc[0]; ++x)
-                  {
-                    const long long cell =
-                      (long long)cs[0][x] + (long long)a.g.m[0] * ((long long)cs[1][y] + (long long)a.g.m[1] * cs[2][z]);
-                    const T kc = a.kcell ? a.kcell[cell] : a.kconst;
-                    const T mx = a.mdiag[ls[0][x]], my = a.mdiag[ls[1][y]], mz = a.mdiag[ls[2][z]];
-                    const T kx = a.kdiag[ls[0][x]], ky = a.kdiag[ls[1][y]], kz = a.kdiag[ls[2][z]];
-                    d += a.alpha * mx * my * mz + kc * (a.cx * kx * my * mz + a.cy * mx * ky * mz + a.cz * mx * my * kz);
-                  }
+            else
+              d = T(1);
+            if (a.invert && !con)
+              d = (fabs(d) > a.threshold) ? T(1) / d : T(1);
+            a.diag[idx] = d;
           }
-        if (a.invert)
-          d = (fabs(d) > a.threshold) ? T(1) / d : T(1);
-        a.diag[idx] = d;
       }
   }
 
@@ -759,9 +770,17 @@ namespace mpdg
     a.threshold = (T)threshold;
     a.diag      = diag;
     a.invert    = invert ? 1 : 0;
-    const long long n = (long long)g.n[0] * g.n[1] * g.n[2];
-    const int       blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
-    heat_diag_kernel<T><<<blocks, 256, 0, s>>>(a);
+    const long long rows    = (long long)g.n[1] * g.n[2];
+    const int       blocks  = (int)std::min<long long>(rows, 148LL * 32);
+    const int       threads = std::min(1024, std::max(32, (g.n[0] + 31) / 32 * 32));
+    switch (K)
+      {
+        case 1: heat_diag_kernel<1, T><<<blocks, threads, 0, s>>>(a); break;
+        case 2: heat_diag_kernel<2, T><<<blocks, threads, 0, s>>>(a); break;
+        case 3: heat_diag_kernel<3, T><<<blocks, threads, 0, s>>>(a); break;
+        case 4: heat_diag_kernel<4, T><<<blocks, threads, 0, s>>>(a); break;
+        default: return cudaErrorInvalidValue;
+      }
     return cudaGetLastError();
   }
 

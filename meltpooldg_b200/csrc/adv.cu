@@ -235,110 +235,6 @@ namespace mpdg
     brick_end<BR, T, MODE>(br, a.g, a.s, s_dst, a.dst, a.b);
   }
 
-  // ---- local diagonal entries per cell: A_c[ii] by quadrature (MatrixFreeTools::compute_diagonal)
-  template <typename T, int N>
-  struct AdvDiagArgs
-  {
-    T        B[N * N], G[N * N], qp[N], qw[N];
-    T        inv_dt, th_adv, th_dif;
-    T        vel[12], origin[3], h[3];
-    int      m[3];
-    T       *cellbuf; // ncells * N^3
-  };
-
-  template <typename T, int N>
-  __global__ void
-  adv_cell_diag_kernel(const __grid_constant__ AdvDiagArgs<T, N> a)
-  {
-    const long long ncells = (long long)a.m[0] * a.m[1] * a.m[2];
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells; c += (long long)gridDim.x * blockDim.x)
-      {
-        const int cx = (int)(c % a.m[0]), cy = (int)((c / a.m[0]) % a.m[1]), cz = (int)(c / ((long long)a.m[0] * a.m[1]));
-        const T   x0 = a.origin[0] + a.h[0] * cx, y0 = a.origin[1] + a.h[1] * cy, z0 = a.origin[2] + a.h[2] * cz;
-        const T   det = a.h[0] * a.h[1] * a.h[2];
-        for (int l = 0; l < N; ++l)
-          for (int j = 0; j < N; ++j)
-            for (int i = 0; i < N; ++i)
-              {
-                T s = 0;
-                for (int qz = 0; qz < N; ++qz)
-                  for (int qy = 0; qy < N; ++qy)
-                    for (int qx = 0; qx < N; ++qx)
-                      {
-                        const T bx = a.B[qx * N + i], by = a.B[qy * N + j], bz = a.B[qz * N + l];
-                        const T phi = bx * by * bz;
-                        const T gx = a.G[qx * N + i] * by * bz / a.h[0];
-                        const T gy = bx * a.G[qy * N + j] * bz / a.h[1];
-                        const T gz = bx * by * a.G[qz * N + l] / a.h[2];
-                        const T x = x0 + a.h[0] * a.qp[qx], y = y0 + a.h[1] * a.qp[qy], z = z0 + a.h[2] * a.qp[qz];
-                        const T vx = a.vel[0] + a.vel[3] * x + a.vel[4] * y + a.vel[5] * z;
-                        const T vy = a.vel[1] + a.vel[6] * x + a.vel[7] * y + a.vel[8] * z;
-                        const T vz = a.vel[2] + a.vel[9] * x + a.vel[10] * y + a.vel[11] * z;
-                        const T JxW = a.qw[qx] * a.qw[qy] * a.qw[qz] * det;
-                        s += JxW * (a.inv_dt * phi * phi + a.th_adv * phi * (vx * gx + vy * gy + vz * gz) +
-                                    a.th_dif * (gx * gx + gy * gy + gz * gz));
-                      }
-                a.cellbuf[c * N * N * N + (l * N + j) * N + i] = s;
-              }
-      }
-  }
-
-  // diag[P] = sum over the (<= 8) cells containing P of their local entry; constrained -> 1
-  template <typename T>
-  __global__ void
-  gather_cellbuf_kernel(const GridDesc g, int K, const T *cellbuf, T *diag)
-  {
-    const int       N     = K + 1;
-    const long long ndofs = (long long)g.n[0] * g.n[1] * g.n[2];
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < ndofs;
-         idx += (long long)gridDim.x * blockDim.x)
-      {
-        const int I = (int)(idx % g.n[0]), J = (int)((idx / g.n[0]) % g.n[1]), L = (int)(idx / ((long long)g.n[0] * g.n[1]));
-        if (is_constrained(g, I, J, L, idx))
-          {
-            diag[idx] = T(1);
-            continue;
-          }
-        int       cs[3][2], ls[3][2], nc[3];
-        const int P[3] = {I, J, L};
-        for (int d = 0; d < 3; ++d)
-          {
-            nc[d]       = 0;
-            const int q = P[d] / K, r = P[d] % K;
-            if (r == 0)
-              {
-                if (q - 1 >= 0)
-                  {
-                    cs[d][nc[d]] = q - 1;
-                    ls[d][nc[d]] = K;
-                    ++nc[d];
-                  }
-                if (q < g.m[d])
-                  {
-                    cs[d][nc[d]] = q;
-                    ls[d][nc[d]] = 0;
-                    ++nc[d];
-                  }
-              }
-            else
-              {
-                cs[d][0] = q;
-                ls[d][0] = r;
-                nc[d]    = 1;
-              }
-          }
-        T s = T(0);
-        for (int z = 0; z < nc[2]; ++z)
-          for (int y = 0; y < nc[1]; ++y)
-            for (int x = 0; x < nc[0]; ++x)
-              {
-                const long long cell = (long long)cs[0][x] + (long long)g.m[0] * ((long long)cs[1][y] + (long long)g.m[1] * cs[2][z]);
-                s += cellbuf[cell * N * N * N + (ls[2][z] * N + ls[1][y]) * N + ls[0][x]];
-              }
-        diag[idx] = s;
-      }
-  }
-
   // ------------------------------------------------------------------------------------------
   static cudaError_t
   upload_adv_tables()
@@ -464,22 +360,114 @@ namespace mpdg
       }
   }
 
-  template <typename T, int N>
-  static cudaError_t
-  cell_diag(const GridDesc &g, const AdvParams &p, T *cellbuf, cudaStream_t s)
+
+  // ---- diagonal in closed form (MatrixFreeTools::compute_diagonal of the tangent).
+  // With phi_i = phi_a(x) phi_b(y) phi_c(z) and an affine velocity, every term of
+  //   A_ii = int phi_i^2 / dt + theta v . grad(phi_i) phi_i + theta eps |grad phi_i|^2
+  // over a box cell is a sum of products of 1-D quadrature moments of the local indices (a, b, c):
+  //   m   = h S[a],  mX = h (x0 S[a] + h S1[a])        (int phi^2,   int x phi^2)
+  //   t   = T[a],    tX = x0 T[a] + h T1[a]            (int phi' phi, int x phi' phi)
+  //   dd  = D[a] / h                                     (int phi'^2)
+  // with S = sum w B^2, S1 = sum w q B^2, T = sum w G B, T1 = sum w q G B, D = sum w G^2 on the
+  // reference Gauss rule.  One thread per DoF sums the (<= 8) cells sharing it; constrained -> 1.
+  template <typename T>
+  struct AdvDiagArgs
   {
-    AdvDiagArgs<T, N> a;
-    const Tables1D   &t = tables(N - 1);
-    for (int i = 0; i < N * N; ++i)
+    GridDesc g;
+    T        S[MAX_N], S1[MAX_N], T0[MAX_N], T1[MAX_N], D[MAX_N];
+    T        inv_dt, th_adv, th_dif;
+    T        vel[12], origin[3], h[3];
+    T       *diag;
+  };
+
+  template <int K, typename T>
+  __global__ void
+  adv_diag_kernel(const __grid_constant__ AdvDiagArgs<T> a)
+  {
+    const int       n0 = a.g.n[0], n1 = a.g.n[1];
+    const long long rows = (long long)n1 * a.g.n[2];
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x)
       {
-        a.B[i] = (T)t.B[i];
-        a.G[i] = (T)t.G[i];
+        const int             J = (int)(row % n1), L = (int)(row / n1);
+        const Neighbours1D<K> ny(J, a.g.m[1]), nz(L, a.g.m[2]);
+        for (int I = threadIdx.x; I < n0; I += blockDim.x)
+          {
+            const long long idx = (long long)I + (long long)n0 * row;
+            if (is_constrained(a.g, I, J, L, idx))
+              {
+                a.diag[idx] = T(1);
+                continue;
+              }
+            const Neighbours1D<K> nx(I, a.g.m[0]);
+            const Neighbours1D<K> *nb[3] = {&nx, &ny, &nz};
+            T                      d     = T(0);
+#pragma unroll
+            for (int z = 0; z < 2; ++z)
+#pragma unroll
+              for (int y = 0; y < 2; ++y)
+#pragma unroll
+                for (int x = 0; x < 2; ++x)
+                  {
+                    if (!(nx.v[x] && ny.v[y] && nz.v[z]))
+                      continue;
+                    const int sel[3] = {x, y, z};
+                    T         m[3], mX[3], t[3], tX[3], dd[3];
+#pragma unroll
+                    for (int e = 0; e < 3; ++e)
+                      {
+                        const int li = nb[e]->l[sel[e]];
+                        const T   h  = a.h[e], x0 = a.origin[e] + h * (T)nb[e]->c[sel[e]];
+                        m[e]         = h * a.S[li];
+                        mX[e]        = h * (x0 * a.S[li] + h * a.S1[li]);
+                        t[e]         = a.T0[li];
+                        tX[e]        = x0 * a.T0[li] + h * a.T1[li];
+                        dd[e]        = a.D[li] / h;
+                      }
+                    T v = a.inv_dt * m[0] * m[1] * m[2] +
+                          a.th_dif * (dd[0] * m[1] * m[2] + m[0] * dd[1] * m[2] + m[0] * m[1] * dd[2]);
+                    T adv = T(0);
+#pragma unroll
+                    for (int dir = 0; dir < 3; ++dir)
+                      {
+                        const int e1 = (dir + 1) % 3, e2 = (dir + 2) % 3;
+                        // int v_dir (d phi / d x_dir) phi, v_dir = vel[dir] + sum_e G[dir][e] x_e
+                        T term = a.vel[dir] * t[dir] * m[e1] * m[e2];
+                        term += a.vel[3 + 3 * dir + dir] * tX[dir] * m[e1] * m[e2];
+                        term += a.vel[3 + 3 * dir + e1] * t[dir] * mX[e1] * m[e2];
+                        term += a.vel[3 + 3 * dir + e2] * t[dir] * m[e1] * mX[e2];
+                        adv += term;
+                      }
+                    d += v + a.th_adv * adv;
+                  }
+            a.diag[idx] = d;
+          }
       }
-    for (int q = 0; q < N; ++q)
+  }
+
+  template <typename T>
+  cudaError_t
+  adv_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, cudaStream_t s)
+  {
+    if (K < 1 || K > 2)
+      return cudaErrorInvalidValue;
+    AdvDiagArgs<T>   a{};
+    const Tables1D &t = tables(K);
+    const int       n = t.n;
+    for (int i = 0; i < n; ++i)
       {
-        a.qp[q] = (T)t.qp[q];
-        a.qw[q] = (T)t.qw[q];
+        double S = 0, S1 = 0, T0 = 0, T1 = 0, D = 0;
+        for (int q = 0; q < n; ++q)
+          {
+            const double w = t.qw[q], b = t.B[q * n + i], gq = t.G[q * n + i];
+            S += w * b * b;
+            S1 += w * t.qp[q] * b * b;
+            T0 += w * gq * b;
+            T1 += w * t.qp[q] * gq * b;
+            D += w * gq * gq;
+          }
+        a.S[i] = (T)S, a.S1[i] = (T)S1, a.T0[i] = (T)T0, a.T1[i] = (T)T1, a.D[i] = (T)D;
       }
+    a.g      = g;
     a.inv_dt = (T)p.inv_dt;
     a.th_adv = (T)p.theta_adv;
     a.th_dif = (T)p.theta_dif;
@@ -489,38 +477,22 @@ namespace mpdg
       {
         a.origin[d] = (T)p.origin[d];
         a.h[d]      = (T)p.h[d];
-        a.m[d]      = g.m[d];
       }
-    a.cellbuf             = cellbuf;
-    const long long nc    = (long long)g.m[0] * g.m[1] * g.m[2];
-    const int       blocks = (int)std::min<long long>((nc + 127) / 128, 148LL * 16);
-    adv_cell_diag_kernel<T, N><<<blocks, 128, 0, s>>>(a);
-    return cudaGetLastError();
-  }
-
-  template <typename T>
-  cudaError_t
-  adv_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, T *cellbuf, cudaStream_t s)
-  {
-    cudaError_t e;
+    a.diag                  = diag;
+    const long long rows    = (long long)g.n[1] * g.n[2];
+    const int       blocks  = (int)std::min<long long>(rows, 148LL * 32);
+    const int       threads = std::min(1024, std::max(32, (g.n[0] + 31) / 32 * 32));
     if (K == 1)
-      e = cell_diag<T, 2>(g, p, cellbuf, s);
-    else if (K == 2)
-      e = cell_diag<T, 3>(g, p, cellbuf, s);
+      adv_diag_kernel<1, T><<<blocks, threads, 0, s>>>(a);
     else
-      return cudaErrorInvalidValue;
-    if (e != cudaSuccess)
-      return e;
-    const long long n      = (long long)g.n[0] * g.n[1] * g.n[2];
-    const int       blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
-    gather_cellbuf_kernel<T><<<blocks, 256, 0, s>>>(g, K, cellbuf, diag);
+      adv_diag_kernel<2, T><<<blocks, threads, 0, s>>>(a);
     return cudaGetLastError();
   }
 
   template cudaError_t adv_apply<double>(const AdvLaunch<double> &, cudaStream_t);
   template cudaError_t adv_apply<float>(const AdvLaunch<float> &, cudaStream_t);
-  template cudaError_t adv_diagonal<double>(const GridDesc &, int, const AdvParams &, double *, double *, cudaStream_t);
-  template cudaError_t adv_diagonal<float>(const GridDesc &, int, const AdvParams &, float *, float *, cudaStream_t);
+  template cudaError_t adv_diagonal<double>(const GridDesc &, int, const AdvParams &, double *, cudaStream_t);
+  template cudaError_t adv_diagonal<float>(const GridDesc &, int, const AdvParams &, float *, cudaStream_t);
   template void adv_brick_shape<double>(int, int[3]);
   template void adv_brick_shape<float>(int, int[3]);
 } // namespace mpdg

@@ -86,6 +86,29 @@ namespace mpdg
     return g.cmask != nullptr && g.cmask[idx] != 0;
   }
 
+  // The cells that share lattice index P along one direction (1 or 2) and P's local index in each.
+  template <int K>
+  struct Neighbours1D
+  {
+    int  c[2], l[2];
+    bool v[2];
+    __device__ __forceinline__
+    Neighbours1D(int P, int m)
+    {
+      const int q = P / K, r = P - q * K;
+      if (r == 0)
+        {
+          c[0] = q - 1, l[0] = K, v[0] = q - 1 >= 0;
+          c[1] = q, l[1] = 0, v[1] = q < m;
+        }
+      else
+        {
+          c[0] = q, l[0] = r, v[0] = true;
+          c[1] = q, l[1] = r, v[1] = false;
+        }
+    }
+  };
+
   __device__ __forceinline__ unsigned
   ld_acquire(const unsigned *p)
   {

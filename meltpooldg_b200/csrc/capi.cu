@@ -257,11 +257,7 @@ namespace
       }
     else
       {
-        const int n3  = (op->degree + 1) * (op->degree + 1) * (op->degree + 1);
-        T        *buf = op->vec<T>(sizeof(T) == 8 ? "celldiag64" : "celldiag32", (size_t)op->ncells * n3);
-        if (!buf)
-          return fail(MPDG_ERR_NOMEM, "cell diagonal buffer");
-        MPDG_CUDA(adv_diagonal<T>(g, op->degree, adv_params(op, 0, false), diag, buf, op->stream));
+        MPDG_CUDA(adv_diagonal<T>(g, op->degree, adv_params(op, 0, false), diag, op->stream));
         MPDG_CUDA(vec_absmax<T>(diag, op->ndofs, op->d_scal, op->reducer(), op->stream));
         MPDG_CUDA(vec_invert_rel<T>(diag, op->d_scal, op->ndofs, op->stream));
       }

@@ -462,29 +462,6 @@ namespace mpdg
     int      invert;
   };
 
-  // The cells that share lattice index P along one direction (1 or 2) and P's local index in each.
-  template <int K>
-  struct Neighbours1D
-  {
-    int  c[2], l[2];
-    bool v[2];
-    __device__ __forceinline__
-    Neighbours1D(int P, int m)
-    {
-      const int q = P / K, r = P - q * K;
-      if (r == 0)
-        {
-          c[0] = q - 1, l[0] = K, v[0] = q - 1 >= 0;
-          c[1] = q, l[1] = 0, v[1] = q < m;
-        }
-      else
-        {
-          c[0] = q, l[0] = r, v[0] = true;
-          c[1] = q, l[1] = r, v[1] = false;
-        }
-    }
-  };
-
   // One CTA per lattice row (J, L) in a grid-stride loop, threads along x (coalesced stores); the
   // diagonal entry is the sum over the (up to 8) cells sharing the point of the tensor-product form
   // a Mx My Mz + k_c (cx Kx My Mz + cy Mx Ky Mz + cz Mx My Kz) at the point's local indices.

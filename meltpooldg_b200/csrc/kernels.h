@@ -82,7 +82,7 @@ namespace mpdg
 
   // per-cell diagonal entries gathered per DoF, then optionally inverted with the advection rule
   template <typename T>
-  cudaError_t adv_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, T *cellbuf, cudaStream_t s);
+  cudaError_t adv_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, cudaStream_t s);
 
   template <typename T>
   void adv_brick_shape(int K, int shape[3]);

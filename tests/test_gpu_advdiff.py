@@ -41,6 +41,18 @@ def test_vmult_matches_oracle(degree, m, theta, eps):
     assert g.device_errors() == 0
 
 
+@pytest.mark.parametrize("degree,m", [(1, (7, 6, 9)), (2, (5, 7, 4))])
+@pytest.mark.parametrize("theta,eps", [(1.0, 1e-3), (0.5, 0.2)])
+def test_inverse_diagonal_closed_form(degree, m, theta, eps):
+    """The closed-form diagonal (1-D quadrature moments) against the oracle's unit-vector applies."""
+    import torch
+
+    o, g, om, cm = adv_pair(degree, m, faces=0b001001, theta=theta, eps=eps)
+    d = torch.empty(om.ndofs, dtype=torch.float64, device="cuda")
+    g.compute_inverse_diagonal_from_matrixfree(d)
+    assert rel_err(d.cpu().numpy(), o.inverse_diagonal()) <= 1e-12
+
+
 def test_per_dof_mask_and_diagonal():
     import torch
 

@@ -121,6 +121,62 @@ namespace mpdg
         }
   }
 
+  // One direction d of the advection and diffusion terms, line by line (a line along d at a time):
+  //   g = D_d uq along the line;  R += theta_adv v_d JxW g / h_d;  R += D_d^T (theta_dif JxW g / h_d^2)
+  // Only the k+1 values of one line are live besides uq and R (the whole-array form needs a third
+  // cell array); the arithmetic and its order per entry are those of the whole-array sweeps.
+  template <typename T, int N, int D>
+  __device__ __forceinline__ void
+  adv_direction(const T *uq, T *R, const T *tD, const T *tqp, const T *tw3, T c_g, T inv_h, T vd0, T gx, T gy,
+                T gz, T th_adv, T th_dif)
+  {
+    constexpr int S = D == 0 ? 1 : (D == 1 ? N : N * N);
+#pragma unroll
+    for (int a = 0; a < N; ++a)
+#pragma unroll
+      for (int c = 0; c < N; ++c)
+        {
+          const int base = D == 0 ? (a * N + c) * N : (D == 1 ? a * N * N + c : a * N + c);
+          T         g[N];
+#pragma unroll
+          for (int r = 0; r < N; ++r)
+            {
+              T s = tD[r * N] * uq[base];
+#pragma unroll
+              for (int k = 1; k < N; ++k)
+                s = fma(tD[r * N + k], uq[base + k * S], s);
+              g[r] = s;
+            }
+#pragma unroll
+          for (int r = 0; r < N; ++r)
+            {
+              const int q  = base + r * S;
+              const int qx = q % N, qy = (q / N) % N, qz = q / (N * N);
+              const T   vd = vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
+              const T   gw = g[r] * (c_g * tw3[q]);
+              R[q]         = fma(th_adv * vd, gw, R[q]);
+              g[r]         = th_dif * gw * inv_h;
+            }
+          if (th_dif != T(0))
+#pragma unroll
+            for (int r = 0; r < N; ++r)
+              {
+                T s = R[base + r * S];
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                  s = fma(tD[k * N + r], g[k], s);
+                R[base + r * S] = s;
+              }
+        }
+  }
+
+#ifndef MPDG_ADV_MINB_F64
+#define MPDG_ADV_MINB_F64 2
+#endif
+#ifndef MPDG_ADV_MINB_F32
+#define MPDG_ADV_MINB_F32 4
+#endif
+
   template <int K, typename T>
   struct AdvLayout
   {
@@ -129,10 +185,11 @@ namespace mpdg
     static constexpr int  NT = BX * BY * BZ;
     using BR                 = Brick<K, BX, BY, BZ, NT>;
     static constexpr size_t bytes = sizeof(T) * 2 * (size_t)BR::NPTS; // staged input + accumulator
+    static constexpr int    MINB  = sizeof(T) == 8 ? MPDG_ADV_MINB_F64 : MPDG_ADV_MINB_F32; // CTAs per SM
   };
 
   template <int K, typename T, OutMode MODE>
-  __global__ void __launch_bounds__(AdvLayout<K, T>::BR::NT)
+  __global__ void __launch_bounds__(AdvLayout<K, T>::BR::NT, AdvLayout<K, T>::MINB)
   adv_apply_kernel(const __grid_constant__ AdvArgs<T, K + 1> a)
   {
     using LAY             = AdvLayout<K, T>;
@@ -179,46 +236,21 @@ namespace mpdg
 #pragma unroll
         for (int q = 0; q < N * N * N; ++q)
           R[q] = (tw3[q] * c_mass) * uq[q];
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-          {
-            T g[N * N * N];
-#pragma unroll
-            for (int q = 0; q < N * N * N; ++q)
-              g[q] = uq[q];
-            if (d == 0)
-              sweep<T, N, 0, false>(g, tD);
-            else if (d == 1)
-              sweep<T, N, 1, false>(g, tD);
-            else
-              sweep<T, N, 2, false>(g, tD);
-            const T inv_h = T(1) / a.h[d];
-            const T c_g   = a.det * inv_h;
-            const T vd0   = a.vel[d] + a.vel[3 + 3 * d] * x0 + a.vel[4 + 3 * d] * y0 + a.vel[5 + 3 * d] * z0;
-            const T gx = a.vel[3 + 3 * d] * a.h[0], gy = a.vel[4 + 3 * d] * a.h[1], gz = a.vel[5 + 3 * d] * a.h[2];
-#pragma unroll
-            for (int qz = 0; qz < N; ++qz)
-#pragma unroll
-              for (int qy = 0; qy < N; ++qy)
-#pragma unroll
-                for (int qx = 0; qx < N; ++qx)
-                  {
-                    const int q  = (qz * N + qy) * N + qx;
-                    const T   vd = vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
-                    const T   gw = g[q] * (c_g * tw3[q]);
-                    R[q]         = fma(a.th_adv * vd, gw, R[q]);
-                    g[q]         = a.th_dif * gw * inv_h;
-                  }
-            if (a.th_dif != T(0))
-              {
-                if (d == 0)
-                  sweep_tr_acc<T, N, 0>(R, g, tD);
-                else if (d == 1)
-                  sweep_tr_acc<T, N, 1>(R, g, tD);
-                else
-                  sweep_tr_acc<T, N, 2>(R, g, tD);
-              }
-          }
+        {
+          const T th_adv = a.th_adv, th_dif = a.th_dif;
+#define MPDG_ADV_DIR(d)                                                                                         \
+  {                                                                                                             \
+    const T inv_h = T(1) / a.h[d];                                                                              \
+    const T c_g   = a.det * inv_h;                                                                              \
+    const T vd0   = a.vel[d] + a.vel[3 + 3 * d] * x0 + a.vel[4 + 3 * d] * y0 + a.vel[5 + 3 * d] * z0;          \
+    adv_direction<T, N, d>(uq, R, tD, tqp, tw3, c_g, inv_h, vd0, a.vel[3 + 3 * d] * a.h[0],                   \
+                           a.vel[4 + 3 * d] * a.h[1], a.vel[5 + 3 * d] * a.h[2], th_adv, th_dif);              \
+  }
+          MPDG_ADV_DIR(0)
+          MPDG_ADV_DIR(1)
+          MPDG_ADV_DIR(2)
+#undef MPDG_ADV_DIR
+        }
         sweep<T, N, 2, true>(R, tB);
         sweep<T, N, 1, true>(R, tB);
         sweep<T, N, 0, true>(R, tB);

@@ -105,6 +105,21 @@ def run_case(name):
         raise SystemExit(f"unknown case {name}")
 
 
+def max_over_ranks(values, world_size, device="cuda"):
+    """Per-rank times -> their maximum over all ranks (the job's time), via the process group."""
+    import torch
+
+    t = torch.tensor(values, device=device, dtype=torch.float64)
+    if world_size > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return t.tolist()
+
+
+def replica_throughput(n_dofs_per_replica, world_size, ms):
+    """Whole-job GDoF/s of N independent replicas (weak scaling): all DoFs over the slowest rank's time."""
+    return world_size * n_dofs_per_replica / (ms * 1e-3) / 1e9
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -463,10 +478,7 @@ def main():
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3) / ke
 
-    t = torch.tensor([ms, ms_e2e], device="cuda", dtype=torch.float64)
-    if ws > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms, ms_e2e = t.tolist()
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e], ws, device="cuda")
 
     solve = None
     if not args.no_solve and rank == 0:
@@ -498,7 +510,7 @@ def main():
         achieved = ALGO_BYTES / (ms * 1e-3) / 1e9
         traffic = committed_traffic()
         line = {
-            "metric": METRIC, "value": ws * mesh.ndofs / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": ws,
+            "metric": METRIC, "value": replica_throughput(mesh.ndofs, ws, ms), "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(WORKLOAD, parallelism=f"replicas{ws}",
@@ -506,7 +518,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": ALGO_BYTES},
-            "e2e": {"value": ws * mesh.ndofs / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
+            "e2e": {"value": replica_throughput(mesh.ndofs, ws, ms_e2e), "unit": UNIT,
                     "h2d_bytes_per_step": 8 * mesh.ndofs, "d2h_bytes_per_step": 8 * mesh.ndofs,
                     "ms_per_step": ms_e2e},
             "gpu_launches": args.steps,

@@ -42,6 +42,8 @@ namespace mpdg
     int            n[3];   // lattice points per direction (K m + 1)
     unsigned       faces;  // Dirichlet faces: bit 2d low face of dim d, bit 2d+1 high face
     const uint8_t *cmask;  // optional per-DoF Dirichlet flags (device), may be null
+    unsigned       acc_lo_z = 0; // the lattice is a z-slab of a larger one: its low z plane already
+                                 // holds the previous slab's contributions and is only added into
   };
 
   struct SyncDesc
@@ -310,7 +312,7 @@ namespace mpdg
   // up to three times with the same value.
   template <class BR, typename T, OutMode MODE>
   __device__ __forceinline__ void
-  brick_init_publish(const BR &br, const SyncDesc &s, T *dst, const T *bvec)
+  brick_init_publish(const BR &br, const SyncDesc &s, T *dst, const T *bvec, unsigned acc_lo_z = 0)
   {
     static_assert(MODE != OutMode::Add, "Add mode needs no initialisation");
     constexpr int F0 = BR::PY * BR::PZ, F1 = BR::PX * BR::PZ, F2 = BR::PX * BR::PY;
@@ -343,6 +345,8 @@ namespace mpdg
           }
         if (!use || !br.inside(px, py, pz) || br.low_shared(px, py, pz))
           continue;
+        if (acc_lo_z && pz == 0 && br.g0[2] == 0)
+          continue; // accumulated onto the previous slab's values, never reset
         const int idx = br.index(px, py, pz);
         dst[idx]      = (MODE == OutMode::BPlus) ? bvec[idx] : T(0);
       }
@@ -498,7 +502,7 @@ namespace mpdg
             return false;
           }
         br.set(g, t);
-        brick_init_publish<BR, T, MODE>(br, s, dst, bvec);
+        brick_init_publish<BR, T, MODE>(br, s, dst, bvec, g.acc_lo_z);
       }
     else
       br.set(g, blockIdx.x);

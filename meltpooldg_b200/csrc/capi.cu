@@ -96,6 +96,9 @@ struct mpdg_op
   double   *h_scal = nullptr; // pinned scalars
   cudaStream_t stream = nullptr;
   std::map<std::string, std::pair<void *, size_t>> ws;
+  // copy streams and events of the slab-pipelined host-buffer apply (created on first use)
+  cudaStream_t             s_h2d = nullptr, s_d2h = nullptr;
+  std::vector<cudaEvent_t> ev;
 
   GridDesc
   grid() const
@@ -624,6 +627,12 @@ mpdg_op_destroy(mpdg_op *op)
   cudaFree(op->d_err);
   cudaFree(op->d_red);
   cudaFree(op->d_part);
+  for (cudaEvent_t e : op->ev)
+    cudaEventDestroy(e);
+  if (op->s_h2d)
+    cudaStreamDestroy(op->s_h2d);
+  if (op->s_d2h)
+    cudaStreamDestroy(op->s_d2h);
   cudaFree(op->d_scal);
   cudaFree(op->d_cg);
   cudaFree(op->d_mask);
@@ -736,6 +745,79 @@ mpdg_op_residual(mpdg_op *op, double *r, const double *b, const double *x)
   return apply<double>(op, (int)OutMode::BPlus, -1.0, r, x, b, 1);
 }
 
+namespace
+{
+  // Host-buffer apply of a heat operator, pipelined over z-slabs of cells: slab s (cells
+  // [c_s, c_s+1)) is applied as a mesh of its own as soon as its input planes [K c_s, K c_s+1] are on
+  // the device; its low boundary plane accumulates onto the previous slab's values (acc_lo_z), and
+  // the output planes [K c_s, K c_s+1) are final once slab s is done, so their device-to-host copy
+  // overlaps the host-to-device copies of the later slabs (both PCIe directions at once).
+  int
+  vmult_host_slabs(mpdg_op *op, double *dst_host, const double *src_host, double *ds, double *dd)
+  {
+    constexpr int S = 8;
+    if (!op->s_h2d)
+      {
+        MPDG_CUDA(cudaStreamCreateWithFlags(&op->s_h2d, cudaStreamNonBlocking));
+        MPDG_CUDA(cudaStreamCreateWithFlags(&op->s_d2h, cudaStreamNonBlocking));
+      }
+    while ((int)op->ev.size() < 2 * S + 1)
+      {
+        cudaEvent_t e;
+        MPDG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        op->ev.push_back(e);
+      }
+    const int    K = op->degree, m2 = op->m[2];
+    const size_t plane = (size_t)(K * op->m[0] + 1) * (size_t)(K * op->m[1] + 1);
+    int          c[S + 1];
+    for (int s = 0; s <= S; ++s)
+      c[s] = (int)((long long)m2 * s / S);
+    // the copies start after the work already on the operator's stream
+    MPDG_CUDA(cudaEventRecord(op->ev[2 * S], op->stream));
+    MPDG_CUDA(cudaStreamWaitEvent(op->s_h2d, op->ev[2 * S], 0));
+    for (int s = 0; s < S; ++s)
+      {
+        const size_t p0 = (size_t)K * c[s], p1 = (size_t)K * c[s + 1]; // input planes [p0, p1]
+        const size_t q0 = s == 0 ? 0 : (size_t)K * c[s] + 1;            // not copied before
+        MPDG_CUDA(cudaMemcpyAsync(ds + q0 * plane, src_host + q0 * plane, sizeof(double) * (p1 + 1 - q0) * plane,
+                                  cudaMemcpyHostToDevice, op->s_h2d));
+        MPDG_CUDA(cudaEventRecord(op->ev[s], op->s_h2d));
+        MPDG_CUDA(cudaStreamWaitEvent(op->stream, op->ev[s], 0));
+        // slab s as a lattice of its own
+        HeatLaunch<double> h;
+        h.degree   = K;
+        h.mode     = (int)OutMode::Set;
+        h.scale    = 1.0;
+        h.geo      = heat_geom(op, op->rho_cp / op->dt);
+        h.grid     = op->grid();
+        h.grid.m[2] = c[s + 1] - c[s];
+        h.grid.n[2] = K * h.grid.m[2] + 1;
+        h.grid.nbr[2] = (h.grid.m[2] + op->brick[2] - 1) / op->brick[2];
+        if (s > 0)
+          h.grid.faces &= ~16u; // the slab's low plane is not the domain's
+        if (s + 1 < S)
+          h.grid.faces &= ~32u;
+        h.grid.acc_lo_z = s > 0 ? 1u : 0u;
+        h.sync     = op->sync();
+        h.kconst   = op->k;
+        h.kcell    = op->d_k64 ? op->d_k64 + (size_t)c[s] * op->m[0] * op->m[1] : nullptr;
+        h.src      = ds + p0 * plane;
+        h.dst      = dd + p0 * plane;
+        h.mask_src = 1;
+        h.march    = true;
+        MPDG_CUDA(heat_apply<double>(h, op->stream));
+        MPDG_CUDA(cudaEventRecord(op->ev[S + s], op->stream));
+        MPDG_CUDA(cudaStreamWaitEvent(op->s_d2h, op->ev[S + s], 0));
+        const size_t o1 = s + 1 < S ? p1 : p1 + 1; // output planes [p0, o1)
+        MPDG_CUDA(cudaMemcpyAsync(dst_host + p0 * plane, dd + p0 * plane, sizeof(double) * (o1 - p0) * plane,
+                                  cudaMemcpyDeviceToHost, op->s_d2h));
+      }
+    MPDG_CUDA(cudaStreamSynchronize(op->s_d2h));
+    MPDG_CUDA(cudaStreamSynchronize(op->stream));
+    return MPDG_OK;
+  }
+} // namespace
+
 int
 mpdg_op_vmult_host(mpdg_op *op, double *dst_host, const double *src_host)
 {
@@ -747,6 +829,8 @@ mpdg_op_vmult_host(mpdg_op *op, double *dst_host, const double *src_host)
   if (!ds || !dd)
     return fail(MPDG_ERR_NOMEM, "staging vectors");
   const size_t bytes = sizeof(double) * op->ndofs;
+  if (op->kind == MPDG_HEAT && op->d_mask == nullptr && op->m[2] >= 16 && op->ndofs >= (1 << 22))
+    return vmult_host_slabs(op, dst_host, src_host, ds, dd);
   MPDG_CUDA(cudaMemcpyAsync(ds, src_host, bytes, cudaMemcpyHostToDevice, op->stream));
   if (int e = apply<double>(op, (int)OutMode::Set, 1.0, dd, ds, nullptr, 1))
     return e;

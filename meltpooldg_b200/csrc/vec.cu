@@ -362,43 +362,98 @@ namespace mpdg
     }
 
     // h_k = w . v_k (k < m), plus ||w||^2 as entry m
-    template <typename T>
+    // h_k = w . v_k (k < m <= MB), out[m] = |w|^2; 16-byte packs when every vector is aligned
+    template <typename T, int MB>
     __global__ void
-    dots_against_kernel(const T *w, const __grid_constant__ VecList<T> L, int m, long long n, double *out, Reducer red)
+    dots_against_kernel(const T *w, const __grid_constant__ VecList<T> L, int m, long long n, double *out, Reducer red,
+                        int packed)
     {
-      double a[MAXV + 1] = {};
-      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      double          a[MB + 1] = {};
+      const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+      using P               = Pack<T>;
+      using V               = typename P::V;
+      const long long nv    = packed ? n / P::W : 0;
+      for (long long i = tid; i < nv; i += stride)
+        {
+          V      wv = reinterpret_cast<const V *>(w)[i];
+          double wd[P::W];
+#pragma unroll
+          for (int e = 0; e < P::W; ++e)
+            {
+              wd[e] = (double)P::at(wv, e);
+              a[MB] += wd[e] * wd[e];
+            }
+#pragma unroll
+          for (int k = 0; k < MB; ++k)
+            if (k < m)
+              {
+                V vv = reinterpret_cast<const V *>(L.v[k])[i];
+#pragma unroll
+                for (int e = 0; e < P::W; ++e)
+                  a[k] += wd[e] * (double)P::at(vv, e);
+              }
+        }
+      for (long long i = nv * P::W + tid; i < n; i += stride)
         {
           const double wi = (double)w[i];
 #pragma unroll
-          for (int k = 0; k < MAXV; ++k)
+          for (int k = 0; k < MB; ++k)
             if (k < m)
               a[k] += wi * (double)L.v[k][i];
-          a[MAXV] += wi * wi;
+          a[MB] += wi * wi;
         }
       // move the norm entry next to the m dots
-      double b[MAXV + 1];
+      double b[MB + 1];
 #pragma unroll
-      for (int k = 0; k <= MAXV; ++k)
-        b[k] = (k < m) ? a[k] : (k == m ? a[MAXV] : 0.0);
-      reduce_finish<MAXV + 1>(b, m + 1, red, [&](double *tot) {
+      for (int k = 0; k <= MB; ++k)
+        b[k] = (k < m) ? a[k] : (k == m ? a[MB] : 0.0);
+      reduce_finish<MB + 1>(b, m + 1, red, [&](double *tot) {
         for (int k = 0; k <= m; ++k)
           out[k] = tot[k];
       });
     }
 
-    // w -= sum_k h_k v_k; out[0] = ||w||^2
-    template <typename T>
+    // w -= sum_k h_k v_k (k < m <= MB); out[0] = ||w||^2
+    template <typename T, int MB>
     __global__ void
     orth_update_kernel(T *w, const __grid_constant__ VecList<T> L, const double *h, int m, long long n, double *out,
-                       Reducer red)
+                       Reducer red, int packed)
     {
-      __shared__ double hs[MAXV];
-      if (threadIdx.x < MAXV)
+      __shared__ double hs[MB];
+      if (threadIdx.x < MB)
         hs[threadIdx.x] = threadIdx.x < m ? h[threadIdx.x] : 0.0;
       __syncthreads();
-      double a[1] = {0.0};
-      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      double          a[1] = {0.0};
+      const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+      using P               = Pack<T>;
+      using V               = typename P::V;
+      const long long nv    = packed ? n / P::W : 0;
+      for (long long i = tid; i < nv; i += stride)
+        {
+          V      wv = reinterpret_cast<const V *>(w)[i];
+          double sd[P::W];
+#pragma unroll
+          for (int e = 0; e < P::W; ++e)
+            sd[e] = (double)P::at(wv, e);
+#pragma unroll
+          for (int k = 0; k < MB; ++k)
+            if (k < m)
+              {
+                V vv = reinterpret_cast<const V *>(L.v[k])[i];
+#pragma unroll
+                for (int e = 0; e < P::W; ++e)
+                  sd[e] -= hs[k] * (double)P::at(vv, e);
+              }
+#pragma unroll
+          for (int e = 0; e < P::W; ++e)
+            {
+              const T t     = (T)sd[e];
+              P::at(wv, e) = t;
+              a[0] += (double)t * (double)t;
+            }
+          reinterpret_cast<V *>(w)[i] = wv;
+        }
+      for (long long i = nv * P::W + tid; i < n; i += stride)
         {
           double s = (double)w[i];
           for (int k = 0; k < m; ++k)
@@ -565,9 +620,20 @@ namespace mpdg
     if (m < 1 || m > MAXV)
       return cudaErrorInvalidValue;
     VecList<T> L{};
+    int        packed = aligned16(w);
     for (int k = 0; k < m; ++k)
-      L.v[k] = v[k];
-    dots_against_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, m, n, out, red);
+      {
+        L.v[k] = v[k];
+        packed = packed && aligned16(v[k]);
+      }
+    if (m <= 4)
+      dots_against_kernel<T, 4><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, m, n, out, red, packed);
+    else if (m <= 8)
+      dots_against_kernel<T, 8><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, m, n, out, red, packed);
+    else if (m <= 16)
+      dots_against_kernel<T, 16><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, m, n, out, red, packed);
+    else
+      dots_against_kernel<T, MAXV><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, m, n, out, red, packed);
     return cudaGetLastError();
   }
   template <typename T>
@@ -578,9 +644,20 @@ namespace mpdg
     if (m < 1 || m > MAXV)
       return cudaErrorInvalidValue;
     VecList<T> L{};
+    int        packed = aligned16(w);
     for (int k = 0; k < m; ++k)
-      L.v[k] = v[k];
-    orth_update_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, h, m, n, out, red);
+      {
+        L.v[k] = v[k];
+        packed = packed && aligned16(v[k]);
+      }
+    if (m <= 4)
+      orth_update_kernel<T, 4><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, h, m, n, out, red, packed);
+    else if (m <= 8)
+      orth_update_kernel<T, 8><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, h, m, n, out, red, packed);
+    else if (m <= 16)
+      orth_update_kernel<T, 16><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, h, m, n, out, red, packed);
+    else
+      orth_update_kernel<T, MAXV><<<RED_BLOCKS, RED_THREADS, 0, s>>>(w, L, h, m, n, out, red, packed);
     return cudaGetLastError();
   }
   template <typename T>

@@ -336,15 +336,10 @@ namespace mpdg
     a.b        = h.b;
     a.mask_src = h.mask_src;
     a.skip     = h.skip;
-    auto kern  = adv_apply_kernel<K, T, MODE>;
-    static thread_local bool attr_done = false;
-    if (!attr_done)
-      {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LAY::bytes);
-        if (e != cudaSuccess)
-          return e;
-        attr_done = true;
-      }
+    auto                                   kern = adv_apply_kernel<K, T, MODE>;
+    static std::atomic<unsigned long long> devices{0};
+    if (cudaError_t e = ensure_smem(kern, LAY::bytes, devices); e != cudaSuccess)
+      return e;
     const unsigned nbricks = (unsigned)h.grid.nbr[0] * h.grid.nbr[1] * h.grid.nbr[2];
     kern<<<nbricks, LAY::BR::NT, LAY::bytes, stream>>>(a);
     return cudaGetLastError();

@@ -24,7 +24,10 @@
 //    shared or constrained), so a lattice point costs a few integer operations.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
+
+#include <cuda_runtime.h>
 
 namespace mpdg
 {
@@ -64,6 +67,24 @@ namespace mpdg
     double       *alpha = nullptr;
     const double *rho   = nullptr;
   };
+
+  // Dynamic shared memory above 48 KB is opted into once per kernel and device.
+  template <class F>
+  inline cudaError_t
+  ensure_smem(F kern, size_t bytes, std::atomic<unsigned long long> &devices)
+  {
+    int         dev = 0;
+    cudaError_t e   = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+      return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (devices.load() & bit)
+      return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess)
+      devices.fetch_or(bit);
+    return e;
+  }
 
   constexpr unsigned SPIN_LIMIT    = 1u << 22; // x 32 ns sleeps: ~0.1-0.2 s
   constexpr int      ERR_FLAG_WAIT = 1;

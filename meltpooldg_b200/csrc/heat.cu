@@ -551,24 +551,6 @@ namespace mpdg
     return cudaSuccess;
   }
 
-  // Dynamic shared memory above 48 KB is opted into once per kernel and device.
-  template <class F>
-  static cudaError_t
-  ensure_smem(F kern, size_t bytes, std::atomic<unsigned long long> &devices)
-  {
-    int         dev = 0;
-    cudaError_t e   = cudaGetDevice(&dev);
-    if (e != cudaSuccess)
-      return e;
-    const unsigned long long bit = 1ull << (dev & 63);
-    if (devices.load() & bit)
-      return cudaSuccess;
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e == cudaSuccess)
-      devices.fetch_or(bit);
-    return e;
-  }
-
   template <int K, typename T, OutMode MODE>
   static cudaError_t
   launch_apply(const HeatLaunch<T> &h, cudaStream_t stream)
@@ -641,15 +623,11 @@ namespace mpdg
     if (h.dot.part != nullptr)
       return cudaErrorInvalidValue; // the brick kernel has no fused dot (heat_apply_fuses_dot is false)
     {
-        auto kern = heat_apply_kernel<K, T, MODE>;
-        static thread_local bool attr_done = false;
-        if (!attr_done)
-          {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
-            if (e != cudaSuccess)
-              return e;
-            attr_done = true;
-          }
+        auto                                   kern = heat_apply_kernel<K, T, MODE>;
+        static std::atomic<unsigned long long> dev_brick{0};
+        cudaError_t                            e = ensure_smem(kern, L::bytes, dev_brick);
+        if (e != cudaSuccess)
+          return e;
         kern<<<nbricks, L::BR::NT, L::bytes, stream>>>(a);
       }
     return cudaGetLastError();

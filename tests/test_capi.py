@@ -58,3 +58,20 @@ def test_invalid_arguments_rejected_without_gpu():
     assert L.mpdg_op_create(ctypes.byref(mesh), ctypes.byref(p), ctypes.byref(h)) == _lib.MPDG_ERR_ZERO_DT
     assert b"ExcZeroTimeIncrement" in L.mpdg_last_error()
     assert L.mpdg_op_vmult(None, None, None) == _lib.MPDG_ERR_ARG
+
+
+def test_header_compiles_as_c_and_cpp(tmp_path):
+    """include/mpdg_gpu.h is plain C (C99) and C++; include/mpdg/mpdg.hpp is C++17."""
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src_c = tmp_path / "h.c"
+    src_c.write_text('#include "mpdg_gpu.h"\nint main(void) { return MPDG_OK; }\n')
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-I",
+                        os.path.join(root, "include"), str(src_c)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    src_cc = tmp_path / "h.cc"
+    src_cc.write_text('#include "mpdg/mpdg.hpp"\nint main() { mpdg::LinearSolverData d; return d.restart == 30 ? 0 : 1; }\n')
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-I",
+                        os.path.join(root, "include"), str(src_cc)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

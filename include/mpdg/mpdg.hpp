@@ -144,6 +144,13 @@ namespace mpdg
     {
       check(mpdg_op_create_rhs(op_, dst, a, b, c));
     }
+    // utilities_matrixfree.hpp:33-100 (x_D = dirichlet_values on constrained DoFs)
+    void
+    create_rhs_and_apply_dirichlet(double *rhs, const double *a, const double *dirichlet_values,
+                                   const double *b = nullptr, const double *c = nullptr, bool zero_out = true) const
+    {
+      check(mpdg_op_create_rhs_and_apply_dirichlet(op_, rhs, a, b, c, dirichlet_values, zero_out ? 1 : 0));
+    }
     // operator_base.hpp:268-272
     void
     compute_inverse_diagonal_from_matrixfree(double *diag) const

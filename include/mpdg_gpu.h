@@ -253,6 +253,14 @@ MPDG_API int mpdg_heat_cell_stiffness_form(mpdg_op *op, const double *lam, const
 MPDG_API int mpdg_heat_vmult_noalloc(const mpdg_mesh_desc *mesh, const mpdg_op_params *params,
                                      const double *k_cells_dev, double *dst, const double *src, void *cuda_stream);
 
+/* create_rhs_and_apply_dirichlet_matrixfree (include/meltpooldg/linear_algebra/utilities_matrixfree.hpp:33-100):
+   with the Dirichlet constraints switched off (the no-BC DoF set), temp = -A x_D + create_rhs(a, b, c)
+   where x_D holds dirichlet_values on the constrained DoFs and 0 elsewhere (constraints.distribute on
+   a zero vector); then rhs = temp (zero_out != 0) or rhs += temp, and the constrained rows of rhs are
+   set to 0.  All arrays are device arrays of n_dofs entries; b, c may be NULL as in create_rhs. */
+MPDG_API int mpdg_op_create_rhs_and_apply_dirichlet(mpdg_op *op, double *rhs, const double *a, const double *b,
+                                                    const double *c, const double *dirichlet_values, int zero_out);
+
 /* Vector operations on the handle's stream over n_dofs entries (device arrays), as used by the
    reference's Newton loop on distributed vectors (source/linear_algebra/newton_raphson_solver.cpp:
    rhs = 0 and solution_update = 0 at :163-164, solution += solution_update at :75, l2_norm in

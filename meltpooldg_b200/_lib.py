@@ -133,6 +133,7 @@ SIGNATURES = [
     ("mpdg_adjoint_heat", [P, P, P, D, P, C.POINTER(AdjointParams), P, C.POINTER(AdjointResult)], C.c_int),
     ("mpdg_heat_forward", [P, P, P, D, C.POINTER(AdjointParams), P], C.c_int),
     ("mpdg_heat_cell_stiffness_form", [P, P, P, P], C.c_int),
+    ("mpdg_op_create_rhs_and_apply_dirichlet", [P, P, P, P, P, P, C.c_int], C.c_int),
     ("mpdg_vec_fill", [P, P, D], C.c_int),
     ("mpdg_vec_axpby", [P, P, D, P, D], C.c_int),
     ("mpdg_vec_norm", [P, P, C.POINTER(D)], C.c_int),

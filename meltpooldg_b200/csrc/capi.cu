@@ -1181,6 +1181,32 @@ mpdg_heat_cell_stiffness_form(mpdg_op *op, const double *lam, const double *T, d
 }
 
 int
+mpdg_op_create_rhs_and_apply_dirichlet(mpdg_op *op, double *rhs, const double *a, const double *b, const double *c,
+                                       const double *dirichlet_values, int zero_out)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!rhs || !a || !dirichlet_values)
+    return fail(MPDG_ERR_ARG, "null argument to mpdg_op_create_rhs_and_apply_dirichlet");
+  double *bc = op->vec<double>("lift_bc"), *tmp = op->vec<double>("lift_tmp");
+  if (!bc || !tmp)
+    return fail(MPDG_ERR_NOMEM, "lifting work vectors");
+  const GridDesc with_bc = op->grid(); // the constraint set of the operator (dof_idx)
+  MPDG_CUDA(vec_copy_constrained<double>(bc, dirichlet_values, with_bc, op->stream));
+  const bool saved = op->with_bc;
+  op->with_bc      = false; // reset_dof_index(dof_no_bc_idx)
+  int rc           = apply<double>(op, (int)OutMode::Set, -1.0, tmp, bc, nullptr, 1);
+  if (rc == MPDG_OK)
+    rc = mpdg_op_create_rhs(op, tmp, a, b, c);
+  op->with_bc = saved; // reset_dof_index(dof_idx)
+  if (rc != MPDG_OK)
+    return rc;
+  MPDG_CUDA(vec_axpby<double>(rhs, 1.0, tmp, zero_out ? 0.0 : 1.0, zero_out ? nullptr : rhs, op->ndofs, op->stream));
+  MPDG_CUDA(vec_set_constrained<double>(rhs, 0.0, with_bc, op->stream));
+  return MPDG_OK;
+}
+
+int
 mpdg_vec_fill(mpdg_op *op, double *x, double value)
 {
   if (int e = check_op(op))

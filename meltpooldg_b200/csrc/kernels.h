@@ -173,4 +173,7 @@ namespace mpdg
   // set constrained entries (face mask / per-DoF mask) of x to v
   template <typename T>
   cudaError_t vec_set_constrained(T *x, T v, const GridDesc &g, cudaStream_t s);
+  // dst = src on constrained DoFs, 0 elsewhere
+  template <typename T>
+  cudaError_t vec_copy_constrained(T *dst, const T *src, const GridDesc &g, cudaStream_t s);
 } // namespace mpdg

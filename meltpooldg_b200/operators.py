@@ -149,6 +149,13 @@ class OperatorMatrixFree:
     def create_rhs(self, dst, a, b=None, c=None) -> None:
         check(lib().mpdg_op_create_rhs(self._h, _ptr(dst), _ptr(a), _ptr(b), _ptr(c)))
 
+    def create_rhs_and_apply_dirichlet(self, rhs, a, dirichlet_values, b=None, c=None, zero_out: bool = True) -> None:
+        """create_rhs_and_apply_dirichlet_matrixfree (utilities_matrixfree.hpp:33-100): rhs (=|+=)
+        -A x_D + create_rhs(a, b, c) without the Dirichlet constraints, then constrained rows 0;
+        x_D = dirichlet_values on constrained DoFs, 0 elsewhere."""
+        check(lib().mpdg_op_create_rhs_and_apply_dirichlet(self._h, _ptr(rhs), _ptr(a), _ptr(b), _ptr(c),
+                                                          _ptr(dirichlet_values), 1 if zero_out else 0))
+
     def device_errors(self) -> int:
         return lib().mpdg_op_device_errors(self._h)
 

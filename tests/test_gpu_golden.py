@@ -52,19 +52,14 @@ def test_vortex_log_gpu(dim, key):
     ref = np.array([float(v) for v in GOLD[key]["values"]])
     phi = to_gpu(phi0)
     mask_t = torch.tensor(mask, device="cuda").bool()
+    dirichlet_minus_one = torch.full_like(phi, -1.0)
     data = LinearSolverData("GMRES", "Diagonal", rel_tolerance=1e-12)
     out = []
     for _ in range(5):
         old = phi.clone()
-        # create_rhs_and_apply_dirichlet_matrixfree (utilities_matrixfree.hpp:39-100)
-        bc = torch.where(mask_t, -1.0, 0.0).double()
-        rhs = torch.zeros_like(phi)
-        g.reset_dof_index(False)
-        g.vmult(rhs, bc)
-        rhs *= -1.0
-        g.create_rhs(rhs, old)
-        g.reset_dof_index(True)
-        rhs[mask_t] = 0.0
+        # create_rhs_and_apply_dirichlet_matrixfree (utilities_matrixfree.hpp:39-100), Dirichlet -1
+        rhs = torch.empty_like(phi)
+        g.create_rhs_and_apply_dirichlet(rhs, old, dirichlet_minus_one)
         x = old.clone()
         LinearSolver.solve(g, x, rhs, data)
         x[mask_t] = -1.0

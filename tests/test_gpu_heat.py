@@ -168,3 +168,20 @@ def test_vmult_host_buffers():
     y = np.zeros_like(x)
     g.vmult_host(y, x)
     assert rel_err(y, o.vmult(x)) <= 1e-12
+
+
+@pytest.mark.parametrize("zero_out", [True, False])
+def test_create_rhs_and_apply_dirichlet(zero_out):
+    """rhs = -A_noBC x_D + create_rhs(T, T_old, q) on free rows, 0 on constrained rows."""
+    o, g, om, cm = heat_pair(2, (9, 8, 5), faces=0b100111)
+    T, To, q, xd = (uniform_dofs(om, seed=s) for s in (41, 42, 43, 44))
+    x_D = np.where(cm == 1, xd, 0.0)
+    ref = -o.with_(cmask=None).vmult(x_D)
+    o.with_(cmask=None).create_rhs(ref, T, To, q)
+    start = uniform_dofs(om, seed=45)
+    if not zero_out:
+        ref = ref + start
+    ref[cm == 1] = 0.0
+    rhs = to_gpu(start)
+    g.create_rhs_and_apply_dirichlet(rhs, to_gpu(T), to_gpu(xd), b=to_gpu(To), c=to_gpu(q), zero_out=zero_out)
+    assert rel_err(rhs.cpu().numpy(), ref) <= 1e-12

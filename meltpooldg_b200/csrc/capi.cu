@@ -84,6 +84,7 @@ struct mpdg_op
   float    *d_k32 = nullptr;
   double    theta = 1.0, eps = 0.0, vel[12]{};
   int       brick[3]{}, nbr[3]{};
+  int       nbr32[3]{};  // bricks per direction of the FP32 apply (its column segments may be longer)
   long long ndofs = 0, ncells = 0;
   unsigned *d_sync = nullptr; // [0] ticket, [1] done, [2] reducer counter, [3..] flags
   int      *d_err  = nullptr;
@@ -100,6 +101,7 @@ struct mpdg_op
   cudaStream_t             s_h2d = nullptr, s_d2h = nullptr;
   std::vector<cudaEvent_t> ev;
 
+  template <typename T = double>
   GridDesc
   grid() const
   {
@@ -107,7 +109,7 @@ struct mpdg_op
     for (int d = 0; d < 3; ++d)
       {
         g.m[d]   = m[d];
-        g.nbr[d] = nbr[d];
+        g.nbr[d] = sizeof(T) == 4 ? nbr32[d] : nbr[d];
         g.n[d]   = degree * m[d] + 1;
       }
     g.faces = with_bc ? faces : 0u;
@@ -215,7 +217,7 @@ namespace
         h.mode   = mode;
         h.scale  = scale;
         h.geo    = heat_geom(op, which == 2 ? 0.0 : (which == 1 ? 1.0 : op->rho_cp / op->dt));
-        h.grid   = op->grid();
+        h.grid   = op->grid<T>();
         h.sync   = op->sync();
         h.kconst = which == 1 ? 0.0 : op->k;
         h.kcell  = which == 1 ? nullptr : op->kcell<T>();
@@ -236,7 +238,7 @@ namespace
         h.mode     = mode;
         h.scale    = scale;
         h.p        = adv_params(op, op->theta - 1.0, which == 3);
-        h.grid     = op->grid();
+        h.grid     = op->grid<T>();
         h.sync     = op->sync();
         h.src      = src;
         h.dst      = dst;
@@ -275,16 +277,36 @@ namespace
     return MPDG_OK;
   }
 
+  // Iterations to enqueue before the next convergence check of the CG loop.  The residual reduction
+  // rate of the previous batch, extrapolated to the tolerance, bounds it from above, so that few of
+  // the enqueued iterations run after convergence (each costs its launches, which return at once);
+  // otherwise the batch doubles up to 64.
+  inline int
+  next_cg_batch(int prev, int it, double res, double tol, int it_prev, double res_prev)
+  {
+    const int cap = std::min(2 * prev, 64);
+    if (it > it_prev && res > 0.0 && res_prev > res && tol > 0.0 && tol < res)
+      {
+        const double need = std::log(tol / res) / (std::log(res / res_prev) / (it - it_prev));
+        if (need < cap)
+          return std::max(2, (int)std::ceil(need));
+      }
+    return cap;
+  }
+
   // ---------------------------------------------------------------------------------------------
-  // Preconditioned CG (dealii::SolverCG semantics), all scalars on the device.
+  // Preconditioned CG (dealii::SolverCG semantics), all scalars on the device.  x_zero: the caller
+  // guarantees x == 0, so the initial residual is b itself and its apply is skipped; b_scratch (with
+  // x_zero only): b is the caller's scratch and becomes the residual vector in place.
   template <typename T>
   int
   cg_solve(mpdg_op *op, T *x, const T *b, const T *invd, int max_it, double abs_tol, double rel_tol,
-           mpdg_solve_info *info, const char *tag)
+           mpdg_solve_info *info, const char *tag, bool x_zero = false, T *b_scratch = nullptr)
   {
     const long long n = op->ndofs;
     const std::string t(tag);
-    T *r = op->vec<T>(t + "r"), *p = op->vec<T>(t + "p"), *v = op->vec<T>(t + "v");
+    T *r = x_zero && b_scratch == b ? b_scratch : op->vec<T>(t + "r");
+    T *p = op->vec<T>(t + "p"), *v = op->vec<T>(t + "v");
     if (!r || !p || !v)
       return fail(MPDG_ERR_NOMEM, "CG work vectors");
     double *hist = op->vec<double>(t + "hist", (size_t)max_it + 2);
@@ -297,7 +319,12 @@ namespace
     *op->h_cg  = st;
     MPDG_CUDA(cudaMemcpyAsync(op->d_cg, op->h_cg, sizeof(CGState), cudaMemcpyHostToDevice, op->stream));
     // r = b - A x
-    if (int e = apply<T>(op, (int)OutMode::BPlus, -1.0, r, x, b, 1))
+    if (x_zero)
+      {
+        if (r != b)
+          MPDG_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * n, cudaMemcpyDeviceToDevice, op->stream));
+      }
+    else if (int e = apply<T>(op, (int)OutMode::BPlus, -1.0, r, x, b, 1))
       return e;
     MPDG_CUDA(cg_init<T>(r, invd, p, op->d_cg, hist, op->reducer(), n, op->stream));
     // heat operators without a per-DoF mask fuse p^T A p into the apply and set alpha on the device
@@ -307,7 +334,8 @@ namespace
     sink.part  = op->d_part;
     sink.alpha = &op->d_cg->alpha;
     sink.rho   = &op->d_cg->rho;
-    int batch = 4;
+    int    batch = 4, it_prev = 0;
+    double res_prev = -1.0;
     for (;;)
       {
         for (int k = 0; k < batch; ++k)
@@ -322,9 +350,12 @@ namespace
           }
         MPDG_CUDA(cudaMemcpyAsync(op->h_cg, op->d_cg, sizeof(CGState), cudaMemcpyDeviceToHost, op->stream));
         MPDG_CUDA(cudaStreamSynchronize(op->stream));
-        if (op->h_cg->done)
+        const CGState &cur = *op->h_cg;
+        if (cur.done)
           break;
-        batch = std::min(batch * 2, 64);
+        batch    = next_cg_batch(batch, cur.it, cur.res, cur.tol, it_prev, it_prev == 0 ? cur.res0 : res_prev);
+        it_prev  = cur.it;
+        res_prev = cur.res;
       }
     const CGState &f = *op->h_cg;
     if (info)
@@ -561,15 +592,27 @@ mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op
   op->eps    = params->diffusivity;
   for (int i = 0; i < 12; ++i)
     op->vel[i] = params->velocity[i];
+  int brick32[3];
   if (op->kind == MPDG_HEAT)
-    heat_brick_shape<double>(op->degree, op->brick, mesh->dirichlet_mask == nullptr);
+    {
+      heat_brick_shape<double>(op->degree, op->brick, mesh->dirichlet_mask == nullptr);
+      heat_brick_shape<float>(op->degree, brick32, mesh->dirichlet_mask == nullptr);
+    }
   else
-    adv_brick_shape<double>(op->degree, op->brick);
+    {
+      adv_brick_shape<double>(op->degree, op->brick);
+      adv_brick_shape<float>(op->degree, brick32);
+    }
   for (int d = 0; d < 3; ++d)
-    op->nbr[d] = (op->m[d] + op->brick[d] - 1) / op->brick[d];
+    {
+      op->nbr[d]   = (op->m[d] + op->brick[d] - 1) / op->brick[d];
+      op->nbr32[d] = (op->m[d] + brick32[d] - 1) / brick32[d];
+    }
   op->ndofs             = n0 * n1 * n2;
   op->ncells            = (long long)op->m[0] * op->m[1] * op->m[2];
-  const long long nbrk  = (long long)op->nbr[0] * op->nbr[1] * op->nbr[2];
+  // brick flags and fused-dot partials serve the FP64 and the FP32 apply
+  const long long nbrk  = std::max((long long)op->nbr[0] * op->nbr[1] * op->nbr[2],
+                                   (long long)op->nbr32[0] * op->nbr32[1] * op->nbr32[2]);
   auto            clean = [&](int code, const std::string &msg) {
     mpdg_op_destroy(op);
     return fail(code, msg);
@@ -920,21 +963,31 @@ mpdg_solve_mixed(mpdg_op *op, double *x, const double *b, const mpdg_mixed_param
   MPDG_CUDA(vec_convert<float, double>(invd32, invd64, n, op->stream));
   const double *bb = b;
   MPDG_CUDA(vec_multidot<double>(&bb, &bb, 1, n, op->d_scal, op->reducer(), op->stream));
-  MPDG_CUDA(cudaMemcpy(op->h_scal, op->d_scal, sizeof(double), cudaMemcpyDeviceToHost));
-  const double bnorm = std::sqrt(op->h_scal[0]);
+  // a zero initial guess (max |x| == 0) makes the first outer residual b itself
+  MPDG_CUDA(vec_absmax<double>(x, n, op->d_scal + 1, op->reducer(), op->stream));
+  MPDG_CUDA(cudaMemcpy(op->h_scal, op->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  const double bnorm  = std::sqrt(op->h_scal[0]);
+  const bool   x_zero = op->h_scal[1] == 0.0;
   const double tol   = prm->outer_rel_tol * bnorm;
   int          inner_total = 0, outer = 0, status = MPDG_ERR_NOT_CONVERGED;
   double       res = 0.0, res0 = -1.0;
   std::vector<double> hist;
   for (outer = 0; outer <= prm->max_outer; ++outer)
     {
-      if (int e = apply<double>(op, (int)OutMode::BPlus, -1.0, r64, x, b, 1))
-        return e;
-      const double *rr = r64;
-      MPDG_CUDA(vec_multidot<double>(&rr, &rr, 1, n, op->d_scal, op->reducer(), op->stream));
-      MPDG_CUDA(cudaMemcpyAsync(op->h_scal, op->d_scal, sizeof(double), cudaMemcpyDeviceToHost, op->stream));
-      MPDG_CUDA(cudaStreamSynchronize(op->stream));
-      res = std::sqrt(op->h_scal[0]);
+      const bool    from_b = outer == 0 && x_zero;
+      const double *r_cur  = from_b ? b : r64;
+      if (from_b)
+        res = bnorm;
+      else
+        {
+          if (int e = apply<double>(op, (int)OutMode::BPlus, -1.0, r64, x, b, 1))
+            return e;
+          const double *rr = r64;
+          MPDG_CUDA(vec_multidot<double>(&rr, &rr, 1, n, op->d_scal, op->reducer(), op->stream));
+          MPDG_CUDA(cudaMemcpyAsync(op->h_scal, op->d_scal, sizeof(double), cudaMemcpyDeviceToHost, op->stream));
+          MPDG_CUDA(cudaStreamSynchronize(op->stream));
+          res = std::sqrt(op->h_scal[0]);
+        }
       if (res0 < 0)
         res0 = res;
       hist.push_back(res);
@@ -945,7 +998,7 @@ mpdg_solve_mixed(mpdg_op *op, double *x, const double *b, const mpdg_mixed_param
         }
       if (outer == prm->max_outer)
         break;
-      MPDG_CUDA(vec_convert<float, double>(r32, r64, n, op->stream));
+      MPDG_CUDA(vec_convert<float, double>(r32, r_cur, n, op->stream));
       MPDG_CUDA(vec_fill<float>(e32, 0.0f, n, op->stream));
       mpdg_solve_info in{};
       int             rc;
@@ -953,7 +1006,7 @@ mpdg_solve_mixed(mpdg_op *op, double *x, const double *b, const mpdg_mixed_param
         rc = gmres_solve<float>(op, e32, r32, invd32, prm->max_inner, 0.0, prm->inner_rel_tol,
                                 prm->restart > 0 ? prm->restart : 30, &in, "mi32_");
       else
-        rc = cg_solve<float>(op, e32, r32, invd32, prm->max_inner, 0.0, prm->inner_rel_tol, &in, "mi32_");
+        rc = cg_solve<float>(op, e32, r32, invd32, prm->max_inner, 0.0, prm->inner_rel_tol, &in, "mi32_", true, r32);
       if (rc != MPDG_OK && rc != MPDG_ERR_NOT_CONVERGED)
         return rc;
       inner_total += in.iterations;

@@ -359,7 +359,7 @@ namespace mpdg
 #define MPDG_MARCH_MINB_F64 5
 #endif
 #ifndef MPDG_MARCH_MINB_F32
-#define MPDG_MARCH_MINB_F32 7
+#define MPDG_MARCH_MINB_F32 8
 #endif
   // CTAs per SM the register allocation of the column-marching kernel is held to
   template <typename T>
@@ -369,12 +369,12 @@ namespace mpdg
   };
 
   template <int K, typename T, OutMode MODE, bool DOT>
-  __global__ void __launch_bounds__(MarchShape<K>::NT, MarchMinBlocks<T>::value)
+  __global__ void __launch_bounds__(MarchShape<K, T>::NT, MarchMinBlocks<T>::value)
   heat_march_kernel(const __grid_constant__ HeatArgs<T, K + 1> a)
   {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned s_ticket;
-    __shared__ double   s_red[MarchShape<K>::NT / 32];
+    __shared__ double   s_red[MarchShape<K, T>::NT / 32];
     if (a.skip != nullptr && *a.skip != 0)
       return;
     HeatCellOp<K, T> op{a};
@@ -639,8 +639,8 @@ namespace mpdg
   {
     switch (K)
       {
-        case 1: bx = MarchShape<1>::BX; by = MarchShape<1>::BY; bz = MarchShape<1>::BZ; break;
-        case 2: bx = MarchShape<2>::BX; by = MarchShape<2>::BY; bz = MarchShape<2>::BZ; break;
+        case 1: bx = MarchShape<1, T>::BX; by = MarchShape<1, T>::BY; bz = MarchShape<1, T>::BZ; break;
+        case 2: bx = MarchShape<2, T>::BX; by = MarchShape<2, T>::BY; bz = MarchShape<2, T>::BZ; break;
         case 3: bx = HeatBrickShape<3, T>::BX; by = HeatBrickShape<3, T>::BY; bz = HeatBrickShape<3, T>::BZ; break;
         default: bx = HeatBrickShape<4, T>::BX; by = HeatBrickShape<4, T>::BY; bz = HeatBrickShape<4, T>::BZ; break;
       }

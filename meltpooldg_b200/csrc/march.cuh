@@ -18,16 +18,22 @@
 
 namespace mpdg
 {
-  template <int K>
+#ifndef MPDG_MARCH_BZ2_F32
+#define MPDG_MARCH_BZ2_F32 16
+#endif
+  // Cell layers per column segment: longer segments amortise the brick handshake and the staging
+  // prologue; for k = 2 in FP64 the 8-layer segment gives more CTAs per wave and wins.
+  template <int K, typename T>
   struct MarchShape
   {
-    static constexpr int BX = 32, BY = 4, BZ = (K == 1 ? 16 : 8), NT = 128;
+    static constexpr int BX = 32, BY = 4, NT = 128;
+    static constexpr int BZ = K == 1 ? 16 : (sizeof(T) == 4 ? MPDG_MARCH_BZ2_F32 : 8);
   };
 
   template <int K, typename T>
   struct MarchLayout
   {
-    using S                 = MarchShape<K>;
+    using S                 = MarchShape<K, T>;
     static constexpr int N  = K + 1;
     static constexpr int PX = K * S::BX + 1, PY = K * S::BY + 1, NPL = K + 1;
     static constexpr int LAYER = NPL * PY * PX;           // staged points per layer

@@ -210,6 +210,12 @@ namespace mpdg
       reduce_finish<1>(a, 1, red, [&](double *tot) { st->alpha = st->rho / tot[0]; });
     }
 
+    // The x / r update walks the vectors from the high end down: the apply before it finishes at the
+    // high end, so the first packs it reads of p and v are still in L2, and cg_update_p after it starts
+    // at the low end, where this kernel has just left r, invd and p.
+#ifndef MPDG_CG_XR_REVERSE
+#define MPDG_CG_XR_REVERSE 1
+#endif
     template <typename T>
     __global__ void
     cg_update_xr_kernel(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p, const T *__restrict__ v,
@@ -222,8 +228,9 @@ namespace mpdg
       const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
       using P               = Pack<T>;
       const long long nv    = packed ? n / P::W : 0;
-      for (long long i = tid; i < nv; i += stride)
+      for (long long i0 = tid; i0 < nv; i0 += stride)
         {
+          const long long i = MPDG_CG_XR_REVERSE ? nv - 1 - i0 : i0;
           using V = typename P::V;
           V xv = reinterpret_cast<const V *>(x)[i], rv = reinterpret_cast<const V *>(r)[i];
           V pv = reinterpret_cast<const V *>(p)[i], vv = reinterpret_cast<const V *>(v)[i];

@@ -170,6 +170,37 @@ MPDG_API int mpdg_op_reset_dof_index(mpdg_op *op, int with_dirichlet);
 /* replace the per-cell conductivity (heat); k_cells has n_cells entries (device pointer) */
 MPDG_API int mpdg_op_set_conductivity(mpdg_op *op, const double *k_cells);
 
+/* Boundary-face terms of the heat operator on whole box faces (bit 2d = low face of dimension d,
+   bit 2d+1 = high face), HeatData's convection / radiation sections and the Neumann map of the
+   reference (source/heat/heat_diffuse_operator.cpp: rhs_boundary_loop :719-781, tangent
+   :1088-1129, both in vmult :239-264 and in the diagonal :297-357):
+     vmult          += int_f (h + 4 eps sigma T^3) u phi            over convection / radiation faces
+     create_rhs     -= int_f [eps sigma (T^4 - T_inf^4) + h (T - T_inf) + g.n] phi
+     inverse diag   built from diag_i + int_f (h + 4 eps sigma T^3) phi_i^2
+   sigma = 5.670374419e-8 (include/meltpooldg/utilities/physical_constants.hpp:6).  g.n is one
+   constant normal flux per face (the reference evaluates a Function there).  A face may not carry
+   both a Neumann flux and convection / radiation (the reference's AssertThrow, :744-748), nor be a
+   Dirichlet face: MPDG_ERR_ARG.  The tangent and the diagonal read T with Dirichlet DoFs as 0, the
+   rhs reads T plainly (FEFaceEvaluation gather_evaluate vs read_dof_values_plain). */
+typedef struct mpdg_heat_bc
+{
+  uint32_t convection_faces;
+  uint32_t radiation_faces;
+  uint32_t neumann_faces;
+  uint32_t reserved;
+  double   convection_coefficient;          /* HeatData::convection.convection_coefficient */
+  double   convection_temperature_infinity; /* HeatData::convection.temperature_infinity   */
+  double   emissivity;                      /* HeatData::radiation.emissivity              */
+  double   radiation_temperature_infinity;  /* HeatData::radiation.temperature_infinity    */
+  double   neumann_flux[6];                 /* g . n on each Neumann face                  */
+} mpdg_heat_bc;
+MPDG_API int mpdg_op_set_heat_bc(mpdg_op *op, const mpdg_heat_bc *bc);
+/* The linearisation temperature of the radiation tangent and diagonal (the operator's const
+   reference to the temperature vector, heat_diffuse_operator.hpp:121-135): a DEVICE array of
+   n_dofs entries that the caller keeps alive and current; NULL detaches it.  vmult and the
+   inverse diagonal of an operator with radiation faces and no temperature return MPDG_ERR_ARG. */
+MPDG_API int mpdg_op_set_temperature(mpdg_op *op, const double *temperature);
+
 /* OperatorMatrixFree::vmult (operator_base.hpp:239-243): dst = A src (FP64 / FP32) */
 MPDG_API int mpdg_op_vmult(mpdg_op *op, double *dst, const double *src);
 MPDG_API int mpdg_op_vmult_f32(mpdg_op *op, float *dst, const float *src);

@@ -53,6 +53,22 @@ class OpParams(C.Structure):
     ]
 
 
+class HeatBC(C.Structure):
+    """mpdg_heat_bc: convection / radiation / Neumann terms on whole box faces (6-bit masks)."""
+
+    _fields_ = [
+        ("convection_faces", C.c_uint32),
+        ("radiation_faces", C.c_uint32),
+        ("neumann_faces", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("convection_coefficient", C.c_double),
+        ("convection_temperature_infinity", C.c_double),
+        ("emissivity", C.c_double),
+        ("radiation_temperature_infinity", C.c_double),
+        ("neumann_flux", C.c_double * 6),
+    ]
+
+
 class SolverParams(C.Structure):
     _fields_ = [
         ("solver", C.c_int32),
@@ -118,6 +134,8 @@ SIGNATURES = [
     ("mpdg_op_reset_time_increment", [P, D], C.c_int),
     ("mpdg_op_reset_dof_index", [P, C.c_int], C.c_int),
     ("mpdg_op_set_conductivity", [P, P], C.c_int),
+    ("mpdg_op_set_heat_bc", [P, C.POINTER(HeatBC)], C.c_int),
+    ("mpdg_op_set_temperature", [P, P], C.c_int),
     ("mpdg_op_vmult", [P, P, P], C.c_int),
     ("mpdg_op_vmult_f32", [P, P, P], C.c_int),
     ("mpdg_op_vmult_host", [P, P, P], C.c_int),

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "mpdg_gpu.h"
@@ -83,6 +84,8 @@ struct mpdg_op
   double   *d_k64 = nullptr;
   float    *d_k32 = nullptr;
   double    theta = 1.0, eps = 0.0, vel[12]{};
+  HeatFaceBC    fbc{};            // boundary-face terms (heat)
+  const double *d_temp = nullptr; // linearisation temperature of the radiation tangent (not owned)
   int       brick[3]{}, nbr[3]{};
   int       nbr32[3]{};  // bricks per direction of the FP32 apply (its column segments may be longer)
   long long ndofs = 0, ncells = 0;
@@ -128,6 +131,11 @@ struct mpdg_op
     s.epoch  = epoch;
     s.error  = d_err;
     return s;
+  }
+  bool
+  tangent_faces() const
+  {
+    return kind == MPDG_HEAT && heat_faces_active(fbc, 0);
   }
   Reducer
   reducer() const
@@ -229,7 +237,25 @@ namespace
         h.march    = op->d_mask == nullptr;
         if (dot)
           h.dot = *dot;
+        if (which == 0 && op->tangent_faces() && op->fbc.radiation_faces && !op->d_temp)
+          return fail(MPDG_ERR_ARG, "radiation faces need the linearisation temperature (mpdg_op_set_temperature)");
         MPDG_CUDA(heat_apply<T>(h, op->stream));
+        if (which == 0 && op->tangent_faces())
+          {
+            HeatFaceLaunch<T> f;
+            f.degree = op->degree;
+            f.mode   = 0;
+            f.scale  = scale;
+            for (int d = 0; d < 3; ++d)
+              f.hlen[d] = op->h[d];
+            f.grid = h.grid;
+            f.bc   = op->fbc;
+            f.temp = op->d_temp;
+            f.src  = src;
+            f.dst  = dst;
+            f.skip = skip;
+            MPDG_CUDA(heat_faces<T>(f, op->stream));
+          }
       }
     else
       {
@@ -255,7 +281,31 @@ namespace
   inverse_diagonal(mpdg_op *op, T *diag)
   {
     const GridDesc g = op->grid();
-    if (op->kind == MPDG_HEAT)
+    if (op->kind == MPDG_HEAT && op->tangent_faces())
+      {
+        // cell and face parts summed in FP64, then inverted (|d| > 1e-10 ? 1/d : 1)
+        if (op->fbc.radiation_faces && !op->d_temp)
+          return fail(MPDG_ERR_ARG, "radiation faces need the linearisation temperature (mpdg_op_set_temperature)");
+        double *d64 = std::is_same<T, double>::value ? reinterpret_cast<double *>(diag) : op->vec<double>("face_diag");
+        if (!d64)
+          return fail(MPDG_ERR_NOMEM, "diagonal work vector");
+        MPDG_CUDA(heat_diagonal<double>(g, op->degree, heat_geom(op, op->rho_cp / op->dt), op->k, op->kcell<double>(),
+                                        d64, false, 0.0, op->stream));
+        HeatFaceLaunch<double> f;
+        f.degree = op->degree;
+        f.mode   = 2;
+        for (int d = 0; d < 3; ++d)
+          f.hlen[d] = op->h[d];
+        f.grid = g;
+        f.bc   = op->fbc;
+        f.temp = op->d_temp;
+        f.diag = d64;
+        MPDG_CUDA(heat_faces<double>(f, op->stream));
+        MPDG_CUDA(vec_invert<double>(d64, 1.0e-10, op->ndofs, op->stream));
+        if (!std::is_same<T, double>::value)
+          MPDG_CUDA(vec_convert<T, double>(diag, d64, op->ndofs, op->stream));
+      }
+    else if (op->kind == MPDG_HEAT)
       {
         MPDG_CUDA(heat_diagonal<T>(g, op->degree, heat_geom(op, op->rho_cp / op->dt), op->k, op->kcell<T>(), diag,
                                    true, 1.0e-10, op->stream));
@@ -328,7 +378,7 @@ namespace
       return e;
     MPDG_CUDA(cg_init<T>(r, invd, p, op->d_cg, hist, op->reducer(), n, op->stream));
     // heat operators without a per-DoF mask fuse p^T A p into the apply and set alpha on the device
-    const bool fused = op->kind == MPDG_HEAT && op->d_part != nullptr &&
+    const bool fused = op->kind == MPDG_HEAT && op->d_part != nullptr && !op->tangent_faces() &&
                        heat_apply_fuses_dot(op->degree, op->d_mask != nullptr, true);
     DotSink    sink;
     sink.part  = op->d_part;
@@ -749,6 +799,45 @@ mpdg_op_set_conductivity(mpdg_op *op, const double *k_cells)
 }
 
 int
+mpdg_op_set_heat_bc(mpdg_op *op, const mpdg_heat_bc *bc)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_HEAT || !bc)
+    return fail(MPDG_ERR_ARG, "boundary-face terms apply to the heat operator");
+  const uint32_t conv = bc->convection_faces, rad = bc->radiation_faces, neu = bc->neumann_faces;
+  if ((conv | rad | neu) & ~63u)
+    return fail(MPDG_ERR_ARG, "face masks have 6 bits");
+  if (neu & (conv | rad))
+    return fail(MPDG_ERR_ARG, "a face cannot carry both a Neumann flux and radiation / convection");
+  if ((conv | rad | neu) & op->faces)
+    return fail(MPDG_ERR_ARG, "a Dirichlet face cannot carry boundary-face terms");
+  HeatFaceBC f;
+  f.convection_faces                = conv;
+  f.radiation_faces                 = rad;
+  f.neumann_faces                   = neu;
+  f.convection_coefficient          = bc->convection_coefficient;
+  f.convection_temperature_infinity = bc->convection_temperature_infinity;
+  f.emissivity_sigma                = bc->emissivity * 5.670374419e-8; // Stefan-Boltzmann, W/(m^2 K^4)
+  f.radiation_temperature_infinity  = bc->radiation_temperature_infinity;
+  for (int i = 0; i < 6; ++i)
+    f.neumann_flux[i] = bc->neumann_flux[i];
+  op->fbc = f;
+  return MPDG_OK;
+}
+
+int
+mpdg_op_set_temperature(mpdg_op *op, const double *temperature)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_HEAT)
+    return fail(MPDG_ERR_ARG, "the linearisation temperature belongs to the heat operator");
+  op->d_temp = temperature;
+  return MPDG_OK;
+}
+
+int
 mpdg_op_vmult(mpdg_op *op, double *dst, const double *src)
 {
   if (int e = check_op(op))
@@ -872,7 +961,8 @@ mpdg_op_vmult_host(mpdg_op *op, double *dst_host, const double *src_host)
   if (!ds || !dd)
     return fail(MPDG_ERR_NOMEM, "staging vectors");
   const size_t bytes = sizeof(double) * op->ndofs;
-  if (op->kind == MPDG_HEAT && op->d_mask == nullptr && op->m[2] >= 16 && op->ndofs >= (1 << 22))
+  if (op->kind == MPDG_HEAT && op->d_mask == nullptr && !op->tangent_faces() && op->m[2] >= 16 &&
+      op->ndofs >= (1 << 22))
     return vmult_host_slabs(op, dst_host, src_host, ds, dd);
   MPDG_CUDA(cudaMemcpyAsync(ds, src_host, bytes, cudaMemcpyHostToDevice, op->stream));
   if (int e = apply<double>(op, (int)OutMode::Set, 1.0, dd, ds, nullptr, 1))
@@ -923,7 +1013,22 @@ mpdg_op_create_rhs(mpdg_op *op, double *dst, const double *a, const double *b, c
         MPDG_CUDA(vec_axpby<double>(v, 1.0, v, 1.0, c, op->ndofs, op->stream));
       if (int e = apply<double>(op, (int)OutMode::Add, 1.0, dst, v, nullptr, 0, 1))
         return e;
-      return apply<double>(op, (int)OutMode::Add, -1.0, dst, a, nullptr, 0, 2);
+      if (int e = apply<double>(op, (int)OutMode::Add, -1.0, dst, a, nullptr, 0, 2))
+        return e;
+      if (heat_faces_active(op->fbc, 1))
+        {
+          HeatFaceLaunch<double> f;
+          f.degree = op->degree;
+          f.mode   = 1;
+          for (int d = 0; d < 3; ++d)
+            f.hlen[d] = op->h[d];
+          f.grid = op->grid();
+          f.bc   = op->fbc;
+          f.temp = a;
+          f.dst  = dst;
+          MPDG_CUDA(heat_faces<double>(f, op->stream));
+        }
+      return MPDG_OK;
     }
   return apply<double>(op, (int)OutMode::Add, 1.0, dst, a, nullptr, 0, 3);
 }
@@ -1132,6 +1237,8 @@ mpdg_adjoint_heat(mpdg_op *op, const double *log_k, const double *qhat, double a
     return e;
   if (!log_k || !qhat || !T_target || !prm || prm->n_steps < 1)
     return fail(MPDG_ERR_ARG, "invalid argument to mpdg_adjoint_heat");
+  if (heat_faces_active(op->fbc, 1))
+    return fail(MPDG_ERR_UNSUPPORTED, "the adjoint covers operators without boundary-face terms");
   double *invd = nullptr;
   if (int e = adjoint_setup(op, log_k, &invd))
     return e;

@@ -50,6 +50,37 @@ namespace mpdg
   template <typename T>
   void heat_brick_shape(int K, int shape[3], bool march);
 
+  // ---- boundary-face terms of the heat operator (faces.cu); face f: bit 2d low / 2d+1 high of dim d
+  struct HeatFaceBC
+  {
+    unsigned convection_faces = 0, radiation_faces = 0, neumann_faces = 0;
+    double   convection_coefficient = 0.0, convection_temperature_infinity = 0.0;
+    double   emissivity_sigma = 0.0, radiation_temperature_infinity = 0.0; // eps * Stefan-Boltzmann
+    double   neumann_flux[6]{};                                              // g . n per face
+  };
+
+  template <typename T>
+  struct HeatFaceLaunch
+  {
+    int           degree = 2;
+    int           mode   = 0; // 0 tangent (dst += scale F src), 1 rhs (dst += face rhs of temp), 2 diagonal
+    double        scale  = 1.0;
+    double        hlen[3]{};
+    GridDesc      grid{};
+    HeatFaceBC    bc{};
+    const double *temp = nullptr; // linearisation point / temperature of the rhs
+    const T      *src  = nullptr;
+    T            *dst  = nullptr;
+    double       *diag = nullptr;
+    const int    *skip = nullptr;
+  };
+
+  // whether mode (0 tangent / 2 diagonal, 1 rhs) has any face to integrate
+  bool heat_faces_active(const HeatFaceBC &bc, int mode);
+
+  template <typename T>
+  cudaError_t heat_faces(const HeatFaceLaunch<T> &h, cudaStream_t s);
+
   // ---- advection-diffusion (source/level_set/advection_diffusion_operator.cpp)
   struct AdvParams
   {

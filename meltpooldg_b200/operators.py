@@ -178,6 +178,28 @@ class HeatDiffuseOperator(OperatorMatrixFree):
     def set_conductivity(self, k_cells_device) -> None:
         check(lib().mpdg_op_set_conductivity(self._h, _ptr(k_cells_device)))
 
+    def set_boundary_conditions(self, convection_faces: int = 0, convection_coefficient: float = 0.0,
+                                convection_temperature_infinity: float = 0.0, radiation_faces: int = 0,
+                                emissivity: float = 0.0, radiation_temperature_infinity: float = 0.0,
+                                neumann_faces: int = 0, neumann_flux=(0.0,) * 6) -> None:
+        """HeatData's convection / radiation sections and a constant normal flux g.n per Neumann face
+        (face masks: bit 2d = low face of dimension d, bit 2d+1 = high face)."""
+        bc = L.HeatBC()
+        bc.convection_faces, bc.radiation_faces, bc.neumann_faces = convection_faces, radiation_faces, neumann_faces
+        bc.convection_coefficient = float(convection_coefficient)
+        bc.convection_temperature_infinity = float(convection_temperature_infinity)
+        bc.emissivity = float(emissivity)
+        bc.radiation_temperature_infinity = float(radiation_temperature_infinity)
+        for i in range(6):
+            bc.neumann_flux[i] = float(neumann_flux[i])
+        check(lib().mpdg_op_set_heat_bc(self._h, C.byref(bc)))
+
+    def set_temperature(self, temperature_device) -> None:
+        """Linearisation temperature of the radiation tangent (kept by reference, as the reference's
+        operator keeps a const reference to its temperature vector)."""
+        self._temperature = temperature_device
+        check(lib().mpdg_op_set_temperature(self._h, _ptr(temperature_device)))
+
 
 class AdvectionDiffusionOperator(OperatorMatrixFree):
     """M/dt + theta (v.grad + eps K) with an affine velocity v(x) = v0 + G x."""

@@ -209,6 +209,18 @@ namespace mpdg
     {
       check(mpdg_op_set_conductivity(handle(), k_cells));
     }
+    // HeatData's convection / radiation sections and constant Neumann fluxes on box faces
+    void
+    set_boundary_conditions(const mpdg_heat_bc &bc)
+    {
+      check(mpdg_op_set_heat_bc(handle(), &bc));
+    }
+    // the temperature the radiation tangent is linearised at (device array, kept by reference)
+    void
+    set_temperature(const double *temperature)
+    {
+      check(mpdg_op_set_temperature(handle(), temperature));
+    }
   };
 
   class AdvectionDiffusionOperator : public OperatorMatrixFree
@@ -353,7 +365,9 @@ namespace mpdg
   // heat_diffuse_operation.cpp:86-102 (Newton rules) and :213-289 (time step), single phase, no
   // predictor (PredictorType::none keeps the current solution as the initial guess).  T, T_old and
   // the work vectors are device arrays of n_dofs() entries; q (heat source, may be null) is read
-  // plainly like heat_source in create_rhs.
+  // plainly like heat_source in create_rhs.  The operator is linearised at T (its temperature
+  // reference, heat_diffuse_operator.hpp:121-135), so radiation faces get the tangent of the
+  // current Newton iterate.
   class HeatDiffuseOperation
   {
   public:
@@ -369,6 +383,7 @@ namespace mpdg
       , newton_(nonlinear, op, rhs, solution_update)
     {
       op_.fill(zero_, 0.0);
+      op_.set_temperature(T_);
       newton_.residual = [this](const double * /*evaluation_point*/, double *rhs) {
         op_.create_rhs(rhs, T_, T_old_, q_ ? q_ : zero_);
       };

@@ -13,10 +13,10 @@ LIBDIR = os.path.join(ROOT, "meltpooldg_b200")
 CUDA = "/usr/local/cuda"
 
 
-def build_program(tmp_path):
-    exe = str(tmp_path / "heat_newton")
+def build_program(tmp_path, name="heat_newton"):
+    exe = str(tmp_path / name)
     cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
-           "-I", os.path.join(CUDA, "include"), os.path.join(ROOT, "tests", "cpp", "heat_newton.cpp"),
+           "-I", os.path.join(CUDA, "include"), os.path.join(ROOT, "tests", "cpp", name + ".cpp"),
            "-o", exe, "-L", LIBDIR, "-lmpdg_b200", "-Wl,-rpath," + LIBDIR, "-L", os.path.join(CUDA, "lib64"),
            "-lcudart", "-Wl,-rpath," + os.path.join(CUDA, "lib64")]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -28,6 +28,7 @@ def test_cpp_host_layer_compiles_and_links(tmp_path):
     if not os.path.exists(os.path.join(LIBDIR, "libmpdg_b200.so")):
         pytest.skip("library not built")
     build_program(tmp_path)
+    build_program(tmp_path, "heat_radiation")
 
 
 @pytest.mark.gpu
@@ -45,3 +46,54 @@ def test_cpp_newton_time_steps_reproduce_reference_log(tmp_path):
     got = ["%.5e" % norm.l2_norm(T[s]) for s in range(5)]
     gold = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_logs.json")))
     assert got == gold["heat_unidirectional_2d_q1"]["values"]
+
+
+def oracle_radiation_steps():
+    """The time steps of tests/cpp/heat_radiation.cpp on the oracle: Newton on the cell oracle plus
+    oracle/faces.py, each linear step solved by Jacobi-CG (scipy) to 1e-14, to a correction below
+    1e-12 of the temperature."""
+    from scipy.sparse.linalg import LinearOperator, cg
+
+    from oracle.faces import HeatBC, face_diagonal, face_rhs, face_tangent
+    from oracle.oracle import Mesh as OMesh
+    from oracle.oracle import Operator as OOp
+
+    om = OMesh(2, (8, 8, 8))
+    o = OOp(om, "heat", rho_cp=1.0, dt=1e-2, k=1.0)
+    bc = HeatBC(convection_faces=0b000011, convection_coefficient=10.0, convection_temperature_infinity=300.0,
+                radiation_faces=0b111100, emissivity=0.6, radiation_temperature_infinity=300.0)
+    n = om.ndofs
+    X, _, _ = om.coords()
+    T = 1000.0 - 300.0 * X
+    steps = []
+    cell_diag = o.diagonal()
+    for _ in range(3):
+        T_old = T.copy()
+        for _ in range(30):
+            r = np.zeros(n)
+            o.create_rhs(r, T, T_old, None)
+            r += face_rhs(om, None, bc, T)
+            Tl = T.copy()
+            J = LinearOperator((n, n), matvec=lambda v, Tl=Tl: o.vmult(v) + face_tangent(om, None, bc, Tl, v))
+            P = 1.0 / (cell_diag + face_diagonal(om, None, bc, Tl))
+            d, info = cg(J, r, rtol=1e-14, atol=0.0, maxiter=10000, M=LinearOperator((n, n), matvec=lambda v: P * v))
+            assert info == 0
+            T = T + d
+            if np.linalg.norm(d) <= 1e-12 * np.linalg.norm(T):
+                break
+        steps.append(T.copy())
+    return np.array(steps)
+
+
+@pytest.mark.gpu
+def test_cpp_newton_with_radiation_faces_matches_oracle(tmp_path):
+    exe = build_program(tmp_path, "heat_radiation")
+    out = str(tmp_path / "T.bin")
+    r = subprocess.run([exe, out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    ref = oracle_radiation_steps()
+    got = np.fromfile(out, dtype=np.float64).reshape(ref.shape)
+    for s in range(ref.shape[0]):
+        assert np.max(np.abs(got[s] - ref[s])) <= 1e-9 * np.max(np.abs(ref[s]))
+    # the radiation and convection faces cool the block
+    assert ref[-1].mean() < (1000.0 - 150.0)

@@ -19,11 +19,13 @@
 // mpdg::NewtonDidNotConverge, everything else mpdg::Error with mpdg_last_error() as the message.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <functional>
 #include <stdexcept>
 #include <string>
 #include <utility>
+#include <vector>
 
 #include "mpdg_gpu.h"
 
@@ -174,6 +176,19 @@ namespace mpdg
       double n = 0.0;
       check(mpdg_vec_norm(op_, x, &n));
       return n;
+    }
+    double
+    dot(const double *x, const double *y) const
+    {
+      double d = 0.0;
+      check(mpdg_vec_dot(op_, x, y, &d));
+      return d;
+    }
+    // constraints.distribute(dst) with the Dirichlet values held in values
+    void
+    distribute_constraints(double *dst, const double *values) const
+    {
+      check(mpdg_op_distribute_constraints(op_, dst, values));
     }
     mpdg_op *
     handle() const
@@ -362,8 +377,109 @@ namespace mpdg
     double                   *rhs_, *du_;
   };
 
-  // heat_diffuse_operation.cpp:86-102 (Newton rules) and :213-289 (time step), single phase, no
-  // predictor (PredictorType::none keeps the current solution as the initial guess).  T, T_old and
+  // A device vector of n_dofs() doubles owned by the host layer (zero-filled).
+  class DeviceVector
+  {
+  public:
+    DeviceVector() = default;
+    explicit DeviceVector(const OperatorMatrixFree &op)
+    {
+      check(mpdg_vec_alloc(op.handle(), &p_));
+    }
+    DeviceVector(DeviceVector &&o) noexcept
+      : p_(std::exchange(o.p_, nullptr))
+    {}
+    DeviceVector &
+    operator=(DeviceVector &&o) noexcept
+    {
+      std::swap(p_, o.p_);
+      return *this;
+    }
+    DeviceVector(const DeviceVector &) = delete;
+    DeviceVector &operator=(const DeviceVector &) = delete;
+    ~DeviceVector()
+    {
+      if (p_)
+        mpdg_vec_free(p_);
+    }
+    double *
+    get() const
+    {
+      return p_;
+    }
+
+  private:
+    double *p_ = nullptr;
+  };
+
+  // ---- predictors (include/meltpooldg/linear_algebra/predictor.hpp, predictor_data.hpp) ------------
+  enum class PredictorType
+  {
+    none,
+    zero,
+    linear_extrapolation,
+    least_squares_projection
+  };
+
+  struct PredictorData
+  {
+    PredictorType type                   = PredictorType::none;
+    int           n_old_solution_vectors = 2; // least_squares_projection only
+  };
+
+  // LeastSquaresProjection::vmult (predictor.hpp:37-84): the combination sum_s c_s x_s of the old
+  // solutions x_0 .. x_{n-1} that minimises |A sum_s c_s x_s - rhs|.  The images A x_s are
+  // orthogonalised one after the other (Gram-Schmidt against the already orthogonalised ones, with
+  // the coefficients P(j, s) / P(j, j)); an image whose remaining squared norm falls below 1e-16 of
+  // the first one ends the basis.  The coefficients follow from the upper-triangular system P c = V^T rhs
+  // by back substitution.  work holds at least n vectors.
+  inline void
+  least_squares_projection(const OperatorMatrixFree &A, double *solution, const double *rhs,
+                           const std::vector<const double *> &old, const std::vector<double *> &work)
+  {
+    const int           n = (int)old.size();
+    std::vector<double> P((size_t)n * n, 0.0);
+    auto                at = [&](int i, int j) -> double & { return P[(size_t)i * n + j]; };
+    int                 step = 0;
+    for (; step < n; ++step)
+      {
+        double *v = work[step];
+        A.vmult(v, old[step]);
+        at(0, step) = A.dot(v, work[0]);
+        for (int j = 0; j < step; ++j)
+          {
+            A.axpby(v, -at(j, step) / at(j, j), work[j], 1.0);
+            at(j + 1, step) = A.dot(v, work[j + 1]);
+          }
+        if (at(step, step) < 1e-16 * at(0, 0))
+          break;
+      }
+    std::vector<double> c(step);
+    for (int s = 0; s < step; ++s)
+      c[s] = A.dot(work[s], rhs);
+    for (int s = step - 1; s >= 0; --s)
+      {
+        double sum = c[s];
+        for (int j = s + 1; j < step; ++j)
+          sum -= c[j] * at(s, j);
+        c[s] = sum / at(s, s);
+      }
+    A.axpby(solution, step > 0 ? c[0] : 0.0, old[0], 0.0);
+    for (int s = 1; s < step; ++s)
+      A.axpby(solution, c[s], old[s], 1.0);
+  }
+
+  // heat_diffuse_operation.cpp:86-102 (Newton rules) and :213-289 (time step), single phase.  The
+  // solution history holds max(n_old_solution_vectors, 2) vectors (:47-48): T (current), T_old and,
+  // for a longer least-squares history, vectors of its own.  init_time_advance runs the predictor
+  // (Predictor::vmult, predictor.hpp:118-160): none keeps the current solution, zero starts from 0,
+  // linear_extrapolation extrapolates with the ratio of the current to the old time increment
+  // (predictor_linear.hpp), least_squares_projection projects once n_old_solution_vectors calls have
+  // filled the history (until then it keeps the current solution, as none does: the reference swaps
+  // the current solution into the predictor buffer there before committing the history, which would
+  // leave the recent old solution zero, and that is not followed).  Then the history is committed
+  // (solution_history.hpp:70-77), the prediction becomes the current solution and the Dirichlet
+  // values of the previous solution are distributed into it (:249).  T, T_old and
   // the work vectors are device arrays of n_dofs() entries; q (heat source, may be null) is read
   // plainly like heat_source in create_rhs.  The operator is linearised at T (its temperature
   // reference, heat_diffuse_operator.hpp:121-135), so radiation faces get the tangent of the
@@ -373,17 +489,28 @@ namespace mpdg
   public:
     HeatDiffuseOperation(HeatDiffuseOperator &op, double *T, double *T_old, const double *q, double *rhs,
                          double *solution_update, double *zero, const LinearSolverData &linear,
-                         const NonlinearSolverData &nonlinear)
+                         const NonlinearSolverData &nonlinear, const PredictorData &predictor = PredictorData())
       : op_(op)
       , T_(T)
       , T_old_(T_old)
       , q_(q)
       , zero_(zero)
       , linear_(linear)
+      , predictor_(predictor)
       , newton_(nonlinear, op, rhs, solution_update)
     {
       op_.fill(zero_, 0.0);
       op_.set_temperature(T_);
+      // solution history: every old slot starts as the initial solution (SolutionHistory::apply_old)
+      const int n_hist = std::max(predictor_.n_old_solution_vectors, 2);
+      history_         = {T_, T_old_};
+      for (int i = 2; i < n_hist; ++i)
+        {
+          owned_.emplace_back(op_);
+          history_.push_back(owned_.back().get());
+        }
+      for (size_t i = 1; i < history_.size(); ++i)
+        op_.axpby(history_[i], 1.0, T_, 0.0);
       newton_.residual = [this](const double * /*evaluation_point*/, double *rhs) {
         op_.create_rhs(rhs, T_, T_old_, q_ ? q_ : zero_);
       };
@@ -392,12 +519,59 @@ namespace mpdg
       };
     }
 
-    // init_time_advance: reset the time increment and commit the old solution
+    // init_time_advance (:213-250): reset the time increment, predict, commit the history
     void
     init_time_advance(double dt)
     {
       op_.reset_time_increment(dt);
-      op_.axpby(T_old_, 1.0, T_, 0.0);
+      dt_old_ = n_calls_ == 0 ? dt : dt_cur_;
+      dt_cur_ = dt;
+      if (!buffer_.get())
+        buffer_ = DeviceVector(op_);
+      double *pred = buffer_.get();
+      switch (predictor_.type)
+        {
+          case PredictorType::none:
+            op_.axpby(pred, 1.0, T_, 0.0);
+            break;
+          case PredictorType::zero:
+            op_.fill(pred, 0.0);
+            break;
+          case PredictorType::linear_extrapolation:
+            {
+              const double r = dt_cur_ / dt_old_;
+              op_.axpby(pred, 1.0 + r, T_, 0.0);
+              op_.axpby(pred, -r, history_[1], 1.0);
+              break;
+            }
+          case PredictorType::least_squares_projection:
+            {
+              const int n_old = predictor_.n_old_solution_vectors;
+              if (n_calls_ >= n_old)
+                {
+                  // rhs of the projection: create_rhs at T_old = T (:236-243)
+                  if (!lsp_rhs_.get())
+                    lsp_rhs_ = DeviceVector(op_);
+                  while ((int)lsp_work_.size() < n_old)
+                    lsp_work_.emplace_back(op_);
+                  op_.fill(lsp_rhs_.get(), 0.0);
+                  op_.create_rhs(lsp_rhs_.get(), T_, T_, q_ ? q_ : zero_);
+                  std::vector<const double *> old(history_.begin(), history_.begin() + n_old);
+                  std::vector<double *>       work;
+                  for (auto &w : lsp_work_)
+                    work.push_back(w.get());
+                  least_squares_projection(op_, pred, lsp_rhs_.get(), old, work);
+                }
+              else
+                op_.axpby(pred, 1.0, T_, 0.0);
+              break;
+            }
+        }
+      for (size_t i = history_.size() - 1; i >= 1; --i)
+        op_.axpby(history_[i], 1.0, history_[i - 1], 0.0);
+      op_.axpby(T_, 1.0, pred, 0.0);
+      op_.distribute_constraints(T_, history_[1]);
+      ++n_calls_;
     }
 
     // solve: Newton on the current time step (ExcNewtonDidNotConverge -> HeatTransferNoConvergence)
@@ -414,11 +588,17 @@ namespace mpdg
     }
 
   private:
-    HeatDiffuseOperator &op_;
-    double              *T_, *T_old_;
-    const double        *q_;
-    double              *zero_;
-    LinearSolverData     linear_;
-    NewtonRaphsonSolver  newton_;
+    HeatDiffuseOperator      &op_;
+    double                   *T_, *T_old_;
+    const double             *q_;
+    double                   *zero_;
+    LinearSolverData          linear_;
+    PredictorData             predictor_;
+    NewtonRaphsonSolver       newton_;
+    std::vector<double *>     history_;
+    std::vector<DeviceVector> owned_, lsp_work_;
+    DeviceVector              buffer_, lsp_rhs_;
+    double                    dt_cur_ = 0.0, dt_old_ = 0.0;
+    int                       n_calls_ = 0;
   };
 } // namespace mpdg

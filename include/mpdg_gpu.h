@@ -300,6 +300,17 @@ MPDG_API int mpdg_op_create_rhs_and_apply_dirichlet(mpdg_op *op, double *rhs, co
 MPDG_API int mpdg_vec_fill(mpdg_op *op, double *x, double value);
 MPDG_API int mpdg_vec_axpby(mpdg_op *op, double *y, double a, const double *x, double b);
 MPDG_API int mpdg_vec_norm(mpdg_op *op, const double *x, double *out);
+/* x . y, deterministic, written to *out (host); the Gram-Schmidt dots of the least-squares
+   projection predictor (include/meltpooldg/linear_algebra/predictor.hpp:37-66) */
+MPDG_API int mpdg_vec_dot(mpdg_op *op, const double *x, const double *y, double *out);
+/* AffineConstraints::distribute for Dirichlet values held in a vector: dst = values on the DoFs
+   constrained by the operator's current constraint set, other entries untouched
+   (source/heat/heat_diffuse_operation.cpp:249 after the predictor) */
+MPDG_API int mpdg_op_distribute_constraints(mpdg_op *op, double *dst, const double *values);
+/* A device vector of n_dofs doubles, zero-filled on the handle's stream, for host layers that do
+   not link the CUDA runtime themselves (solution history, predictor work vectors). */
+MPDG_API int mpdg_vec_alloc(mpdg_op *op, double **x);
+MPDG_API int mpdg_vec_free(double *x);
 
 /* Number of error words raised by bounded device waits since the last call (and reset). */
 MPDG_API int mpdg_op_device_errors(mpdg_op *op);

@@ -1403,6 +1403,53 @@ mpdg_vec_norm(mpdg_op *op, const double *x, double *out)
 }
 
 int
+mpdg_vec_dot(mpdg_op *op, const double *x, const double *y, double *out)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!x || !y || !out)
+    return fail(MPDG_ERR_ARG, "null argument to mpdg_vec_dot");
+  MPDG_CUDA(vec_multidot<double>(&x, &y, 1, op->ndofs, op->d_scal, op->reducer(), op->stream));
+  MPDG_CUDA(cudaMemcpyAsync(op->h_scal, op->d_scal, sizeof(double), cudaMemcpyDeviceToHost, op->stream));
+  MPDG_CUDA(cudaStreamSynchronize(op->stream));
+  *out = op->h_scal[0];
+  return MPDG_OK;
+}
+
+int
+mpdg_op_distribute_constraints(mpdg_op *op, double *dst, const double *values)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!dst || !values)
+    return fail(MPDG_ERR_ARG, "null argument to mpdg_op_distribute_constraints");
+  MPDG_CUDA(vec_distribute_constrained<double>(dst, values, op->grid(), op->stream));
+  return MPDG_OK;
+}
+
+int
+mpdg_vec_alloc(mpdg_op *op, double **x)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!x)
+    return fail(MPDG_ERR_ARG, "null argument to mpdg_vec_alloc");
+  *x = nullptr;
+  if (cudaMalloc(x, sizeof(double) * op->ndofs) != cudaSuccess)
+    return fail(MPDG_ERR_NOMEM, "mpdg_vec_alloc");
+  MPDG_CUDA(cudaMemsetAsync(*x, 0, sizeof(double) * op->ndofs, op->stream));
+  return MPDG_OK;
+}
+
+int
+mpdg_vec_free(double *x)
+{
+  if (x && cudaFree(x) != cudaSuccess)
+    return fail(MPDG_ERR_CUDA, "cudaFree in mpdg_vec_free");
+  return MPDG_OK;
+}
+
+int
 mpdg_op_device_errors(mpdg_op *op)
 {
   if (!op)

@@ -207,4 +207,7 @@ namespace mpdg
   // dst = src on constrained DoFs, 0 elsewhere
   template <typename T>
   cudaError_t vec_copy_constrained(T *dst, const T *src, const GridDesc &g, cudaStream_t s);
+  // dst = src on constrained DoFs, other entries untouched
+  template <typename T>
+  cudaError_t vec_distribute_constrained(T *dst, const T *src, const GridDesc &g, cudaStream_t s);
 } // namespace mpdg

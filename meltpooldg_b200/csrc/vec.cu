@@ -525,6 +525,21 @@ namespace mpdg
         }
     }
 
+    // dst = src on constrained DoFs, other entries untouched (AffineConstraints::distribute with
+    // the Dirichlet values held in src)
+    template <typename T>
+    __global__ void
+    distribute_constrained_kernel(T *dst, const T *src, const GridDesc g)
+    {
+      const long long n = (long long)g.n[0] * g.n[1] * g.n[2];
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+          const int I = (int)(i % g.n[0]), J = (int)((i / g.n[0]) % g.n[1]), L = (int)(i / ((long long)g.n[0] * g.n[1]));
+          if (is_constrained(g, I, J, L, i))
+            dst[i] = src[i];
+        }
+    }
+
     inline int
     aligned16(const void *p)
     {
@@ -712,6 +727,15 @@ namespace mpdg
 
   template <typename T>
   cudaError_t
+  vec_distribute_constrained(T *dst, const T *src, const GridDesc &g, cudaStream_t s)
+  {
+    const long long n = (long long)g.n[0] * g.n[1] * g.n[2];
+    distribute_constrained_kernel<T><<<stream_blocks(n), 256, 0, s>>>(dst, src, g);
+    return cudaGetLastError();
+  }
+
+  template <typename T>
+  cudaError_t
   vec_set_constrained(T *x, T v, const GridDesc &g, cudaStream_t s)
   {
     const long long n = (long long)g.n[0] * g.n[1] * g.n[2];
@@ -740,7 +764,8 @@ namespace mpdg
   template cudaError_t vec_absmax<T>(const T *, long long, double *, Reducer, cudaStream_t);                    \
   template cudaError_t vec_invert_rel<T>(T *, const double *, long long, cudaStream_t);                         \
   template cudaError_t vec_set_constrained<T>(T *, T, const GridDesc &, cudaStream_t);                            \
-  template cudaError_t vec_copy_constrained<T>(T *, const T *, const GridDesc &, cudaStream_t);
+  template cudaError_t vec_copy_constrained<T>(T *, const T *, const GridDesc &, cudaStream_t);             \
+  template cudaError_t vec_distribute_constrained<T>(T *, const T *, const GridDesc &, cudaStream_t);
   MPDG_INST(double)
   MPDG_INST(float)
 #undef MPDG_INST

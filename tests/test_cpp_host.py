@@ -29,6 +29,7 @@ def test_cpp_host_layer_compiles_and_links(tmp_path):
         pytest.skip("library not built")
     build_program(tmp_path)
     build_program(tmp_path, "heat_radiation")
+    build_program(tmp_path, "heat_predictor")
 
 
 @pytest.mark.gpu
@@ -97,3 +98,56 @@ def test_cpp_newton_with_radiation_faces_matches_oracle(tmp_path):
         assert np.max(np.abs(got[s] - ref[s])) <= 1e-9 * np.max(np.abs(ref[s]))
     # the radiation and convection faces cool the block
     assert ref[-1].mean() < (1000.0 - 150.0)
+
+
+@pytest.mark.gpu
+def test_cpp_predictors_match_oracle(tmp_path):
+    """Each predicted temperature of tests/cpp/heat_predictor.cpp equals the oracle's predictor applied
+    to the same solution history (the program's own converged solutions), and all predictors reach
+    the same solutions."""
+    from oracle.faces import HeatBC, face_rhs, face_tangent
+    from oracle.oracle import Mesh as OMesh
+    from oracle.oracle import Operator as OOp
+    from oracle.predictor import least_squares_projection, linear_extrapolation
+
+    exe = build_program(tmp_path, "heat_predictor")
+    prefix = str(tmp_path / "pred")
+    r = subprocess.run([exe, prefix], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    om = OMesh(2, (8, 8, 8))
+    cm = om.face_mask(0b000001)
+    bc = HeatBC(convection_faces=0b000010, convection_coefficient=10.0, convection_temperature_infinity=300.0,
+                radiation_faces=0b111100, emissivity=0.6, radiation_temperature_infinity=300.0)
+    n = om.ndofs
+    X, _, _ = om.coords()
+    T0 = 1000.0 - 300.0 * X
+    dts = [1e-2, 1e-2, 2e-2, 1e-2, 1.5e-2]
+    finals = {}
+    for kind in ("none", "zero", "linear_extrapolation", "least_squares_projection"):
+        data = np.fromfile(prefix + "_" + kind + ".bin", dtype=np.float64).reshape(len(dts), 2, n)
+        hist = [T0, T0, T0]  # max(n_old_solution_vectors = 3, 2) vectors, all the initial solution
+        for k, dt in enumerate(dts):
+            pred, sol = data[k]
+            s0, s1 = hist[0], hist[1]
+            tol = 1e-13
+            if kind == "none":
+                ref = s0.copy()
+            elif kind == "zero":
+                ref = np.zeros(n)
+            elif kind == "linear_extrapolation":
+                ref = linear_extrapolation(s0, s1, dt, dts[k - 1] if k else dt)
+            elif k >= 3:
+                o = OOp(om, "heat", cmask=cm, rho_cp=1.0, dt=dt, k=1.0)
+                rhs = np.zeros(n)
+                o.create_rhs(rhs, s0, s0, None)
+                rhs += face_rhs(om, cm, bc, s0)
+                ref = least_squares_projection(lambda v: o.vmult(v) + face_tangent(om, cm, bc, s0, v), rhs, hist)
+                tol = 1e-8
+            else:
+                ref = s0.copy()
+            ref = np.where(cm != 0, s0, ref)  # Dirichlet values of the previous solution
+            assert np.max(np.abs(pred - ref)) <= tol * np.max(np.abs(ref)), (kind, k)
+            hist = [sol] + hist[:-1]
+        finals[kind] = data[-1, 1]
+    for kind, T in finals.items():
+        assert np.max(np.abs(T - finals["none"])) <= 1e-9 * np.max(np.abs(T)), kind

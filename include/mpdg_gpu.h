@@ -195,6 +195,12 @@ typedef struct mpdg_heat_bc
   double   neumann_flux[6];                 /* g . n on each Neumann face                  */
 } mpdg_heat_bc;
 MPDG_API int mpdg_op_set_heat_bc(mpdg_op *op, const mpdg_heat_bc *bc);
+/* SUPG streamline stabilisation of the advection-diffusion operator (AdvectionDiffusionData::
+   conv_stab, source/level_set/advection_diffusion_operator.cpp:455-533): vmult, create_rhs and the
+   inverse diagonal add int tau_c (v.grad phi)(u/dt + theta v.grad u - theta eps lap u) (theta - 1 in
+   create_rhs), tau_c = (coefficient < 0 ? 1 / max_q |v| (0 if below 1e-6) : coefficient) times the
+   cell diameter / sqrt(3).  enabled = 0 switches it off (ConvectionStabilizationType::none). */
+MPDG_API int mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient);
 /* The linearisation temperature of the radiation tangent and diagonal (the operator's const
    reference to the temperature vector, heat_diffuse_operator.hpp:121-135): a DEVICE array of
    n_dofs entries that the caller keeps alive and current; NULL detaches it.  vmult and the

@@ -136,6 +136,7 @@ SIGNATURES = [
     ("mpdg_op_set_conductivity", [P, P], C.c_int),
     ("mpdg_op_set_heat_bc", [P, C.POINTER(HeatBC)], C.c_int),
     ("mpdg_vec_dot", [P, P, P, P], C.c_int),
+    ("mpdg_op_set_supg", [P, C.c_int, D], C.c_int),
     ("mpdg_op_distribute_constraints", [P, P, P], C.c_int),
     ("mpdg_vec_alloc", [P, C.POINTER(C.c_void_p)], C.c_int),
     ("mpdg_vec_free", [P], C.c_int),

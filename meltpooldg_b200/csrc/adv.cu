@@ -11,8 +11,17 @@
 //   u_q = (B(x)B(x)B) u;  for d: g = D_d u_q (collocation derivative on the Gauss points),
 //   R += JxW theta v_d g / h_d,  R += D_d^T (JxW theta eps g / h_d^2);  out = (B(x)B(x)B)^T R,
 // starting from R = JxW u_q / dt.  Peak register use is three cell arrays (u_q, R, g).
+//
+// SUPG (ConvectionStabilizationType::SUPG, :455-457, :486-490, stabilisation parameter :497-533):
+// the strong residual s = u/dt + theta v.grad u - theta eps lap u at the Gauss points (the second
+// derivative is the collocation derivative applied twice: exact for the degree-k interpolant), tested
+// with tau_c v.grad phi; tau_c = (coefficient < 0 ? 1 / max_q |v| (0 below 1e-6) : coefficient) times
+// the cell size diameter / sqrt(3) (source/core/scratch_data.cpp:262-277).  The rhs uses the same
+// form with theta replaced by theta - 1 (:322-345).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <set>
 
@@ -43,6 +52,7 @@ namespace mpdg
   struct AdvArgs
   {
     T            det;
+    T            supg_coef, cell_size;
     GridDesc     g;
     SyncDesc     s;
     T            inv_dt, th_adv, th_dif; // already multiplied by scale
@@ -170,6 +180,108 @@ namespace mpdg
         }
   }
 
+  // SUPG, direction D of the strong residual: s += theta_adv v_d (D_d u_q) / h_d - theta_dif (D_d D_d u_q) / h_d^2
+  template <typename T, int N, int D>
+  __device__ __forceinline__ void
+  supg_residual(const T *uq, T *sres, const T *tD, const T *tqp, T inv_h, T vd0, T gx, T gy, T gz, T th_adv,
+                T th_dif)
+  {
+    constexpr int S = D == 0 ? 1 : (D == 1 ? N : N * N);
+#pragma unroll
+    for (int a = 0; a < N; ++a)
+#pragma unroll
+      for (int c = 0; c < N; ++c)
+        {
+          const int base = D == 0 ? (a * N + c) * N : (D == 1 ? a * N * N + c : a * N + c);
+          T         g[N];
+#pragma unroll
+          for (int r = 0; r < N; ++r)
+            {
+              T s = tD[r * N] * uq[base];
+#pragma unroll
+              for (int k = 1; k < N; ++k)
+                s = fma(tD[r * N + k], uq[base + k * S], s);
+              g[r] = s;
+            }
+#pragma unroll
+          for (int r = 0; r < N; ++r)
+            {
+              T gg = tD[r * N] * g[0];
+#pragma unroll
+              for (int k = 1; k < N; ++k)
+                gg = fma(tD[r * N + k], g[k], gg);
+              const int q  = base + r * S;
+              const int qx = q % N, qy = (q / N) % N, qz = q / (N * N);
+              const T   vd = vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
+              sres[q] += th_adv * vd * g[r] * inv_h - th_dif * gg * inv_h * inv_h;
+            }
+        }
+  }
+
+  // SUPG, direction D of the test with tau v.grad phi: R += D_d^T (c_t w3 v_d s), c_t = tau det / h_d
+  template <typename T, int N, int D>
+  __device__ __forceinline__ void
+  supg_test(const T *sres, T *R, const T *tD, const T *tqp, const T *tw3, T c_t, T vd0, T gx, T gy, T gz)
+  {
+    constexpr int S = D == 0 ? 1 : (D == 1 ? N : N * N);
+#pragma unroll
+    for (int a = 0; a < N; ++a)
+#pragma unroll
+      for (int c = 0; c < N; ++c)
+        {
+          const int base = D == 0 ? (a * N + c) * N : (D == 1 ? a * N * N + c : a * N + c);
+          T         t[N];
+#pragma unroll
+          for (int r = 0; r < N; ++r)
+            {
+              const int q  = base + r * S;
+              const int qx = q % N, qy = (q / N) % N, qz = q / (N * N);
+              const T   vd = vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
+              t[r]         = c_t * tw3[q] * vd * sres[q];
+            }
+#pragma unroll
+          for (int r = 0; r < N; ++r)
+            {
+              T s = R[base + r * S];
+#pragma unroll
+              for (int k = 0; k < N; ++k)
+                s = fma(tD[k * N + r], t[k], s);
+              R[base + r * S] = s;
+            }
+        }
+  }
+
+  // tau_c of the cell with lower corner (x0, y0, z0)
+  template <typename T, int N>
+  __device__ __forceinline__ T
+  supg_tau(const T *vel, const T *h, const T *tqp, T x0, T y0, T z0, T coef, T cell_size)
+  {
+    T tau = coef;
+    if (coef < T(0))
+      {
+        T vmax = T(0);
+#pragma unroll
+        for (int qz = 0; qz < N; ++qz)
+#pragma unroll
+          for (int qy = 0; qy < N; ++qy)
+#pragma unroll
+            for (int qx = 0; qx < N; ++qx)
+              {
+                const T x = x0 + h[0] * tqp[qx], y = y0 + h[1] * tqp[qy], z = z0 + h[2] * tqp[qz];
+                T       n2 = T(0);
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                  {
+                    const T v = vel[d] + vel[3 + 3 * d] * x + vel[4 + 3 * d] * y + vel[5 + 3 * d] * z;
+                    n2        = fma(v, v, n2);
+                  }
+                vmax = fmax(vmax, sqrt(n2));
+              }
+        tau = vmax >= T(1e-6) ? T(1) / vmax : T(0);
+      }
+    return tau * cell_size;
+  }
+
 #ifndef MPDG_ADV_MINB_F64
 #define MPDG_ADV_MINB_F64 2
 #endif
@@ -188,8 +300,9 @@ namespace mpdg
     static constexpr int    MINB  = sizeof(T) == 8 ? MPDG_ADV_MINB_F64 : MPDG_ADV_MINB_F32; // CTAs per SM
   };
 
-  template <int K, typename T, OutMode MODE>
-  __global__ void __launch_bounds__(AdvLayout<K, T>::BR::NT, AdvLayout<K, T>::MINB)
+  // the SUPG form keeps a third cell array (the strong residual) and gets the registers of one CTA per SM
+  template <int K, typename T, OutMode MODE, bool SUPG>
+  __global__ void __launch_bounds__(AdvLayout<K, T>::BR::NT, SUPG ? 1 : AdvLayout<K, T>::MINB)
   adv_apply_kernel(const __grid_constant__ AdvArgs<T, K + 1> a)
   {
     using LAY             = AdvLayout<K, T>;
@@ -250,6 +363,31 @@ namespace mpdg
           MPDG_ADV_DIR(1)
           MPDG_ADV_DIR(2)
 #undef MPDG_ADV_DIR
+          if constexpr (SUPG)
+            {
+              const T tau = supg_tau<T, N>(a.vel, a.h, tqp, x0, y0, z0, a.supg_coef, a.cell_size);
+              T       sres[N * N * N];
+#pragma unroll
+              for (int q = 0; q < N * N * N; ++q)
+                sres[q] = a.inv_dt * uq[q];
+              T vd0[3], gv[3][3], ih[3];
+#pragma unroll
+              for (int d = 0; d < 3; ++d)
+                {
+                  ih[d]  = T(1) / a.h[d];
+                  vd0[d] = a.vel[d] + a.vel[3 + 3 * d] * x0 + a.vel[4 + 3 * d] * y0 + a.vel[5 + 3 * d] * z0;
+#pragma unroll
+                  for (int e = 0; e < 3; ++e)
+                    gv[d][e] = a.vel[3 + 3 * d + e] * a.h[e];
+                }
+              supg_residual<T, N, 0>(uq, sres, tD, tqp, ih[0], vd0[0], gv[0][0], gv[0][1], gv[0][2], th_adv, th_dif);
+              supg_residual<T, N, 1>(uq, sres, tD, tqp, ih[1], vd0[1], gv[1][0], gv[1][1], gv[1][2], th_adv, th_dif);
+              supg_residual<T, N, 2>(uq, sres, tD, tqp, ih[2], vd0[2], gv[2][0], gv[2][1], gv[2][2], th_adv, th_dif);
+              const T td = tau * a.det;
+              supg_test<T, N, 0>(sres, R, tD, tqp, tw3, td * ih[0], vd0[0], gv[0][0], gv[0][1], gv[0][2]);
+              supg_test<T, N, 1>(sres, R, tD, tqp, tw3, td * ih[1], vd0[1], gv[1][0], gv[1][1], gv[1][2]);
+              supg_test<T, N, 2>(sres, R, tD, tqp, tw3, td * ih[2], vd0[2], gv[2][0], gv[2][1], gv[2][2]);
+            }
         }
         sweep<T, N, 2, true>(R, tB);
         sweep<T, N, 1, true>(R, tB);
@@ -336,9 +474,11 @@ namespace mpdg
     a.b        = h.b;
     a.mask_src = h.mask_src;
     a.skip     = h.skip;
-    auto                                   kern = adv_apply_kernel<K, T, MODE>;
-    static std::atomic<unsigned long long> devices{0};
-    if (cudaError_t e = ensure_smem(kern, LAY::bytes, devices); e != cudaSuccess)
+    a.supg_coef = (T)h.p.supg_coef;
+    a.cell_size = (T)(std::sqrt(h.p.h[0] * h.p.h[0] + h.p.h[1] * h.p.h[1] + h.p.h[2] * h.p.h[2]) / std::sqrt(3.0));
+    auto                                   kern = h.p.supg ? adv_apply_kernel<K, T, MODE, true> : adv_apply_kernel<K, T, MODE, false>;
+    static std::atomic<unsigned long long> devices{0}, devices_supg{0};
+    if (cudaError_t e = ensure_smem(kern, LAY::bytes, h.p.supg ? devices_supg : devices); e != cudaSuccess)
       return e;
     const unsigned nbricks = (unsigned)h.grid.nbr[0] * h.grid.nbr[1] * h.grid.nbr[2];
     kern<<<nbricks, LAY::BR::NT, LAY::bytes, stream>>>(a);
@@ -516,6 +656,118 @@ namespace mpdg
     return cudaGetLastError();
   }
 
+  // ---- SUPG part of the diagonal: one thread per cell; for each free local DoF i
+  //   tau_c sum_q JxW (v.grad phi_i)(phi_i / dt + theta v.grad phi_i - theta eps lap phi_i)
+  // with the 1-D values B, derivatives G and second derivatives H of the basis at the Gauss points.
+  template <typename T>
+  struct AdvSupgDiagArgs
+  {
+    GridDesc g;
+    T        B[MAX_N * MAX_N], G[MAX_N * MAX_N], H[MAX_N * MAX_N], qp[MAX_N], qw[MAX_N];
+    T        inv_dt, th_adv, th_dif, coef, cell_size, det;
+    T        vel[12], origin[3], h[3];
+    T       *diag;
+  };
+
+  template <int K, typename T>
+  __global__ void
+  adv_supg_diag_kernel(const __grid_constant__ AdvSupgDiagArgs<T> a)
+  {
+    constexpr int   N     = K + 1;
+    const int       m0    = a.g.m[0], m1 = a.g.m[1];
+    const long long ncell = (long long)m0 * m1 * a.g.m[2];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
+      {
+        const int cx = (int)(c % m0), cy = (int)((c / m0) % m1), cz = (int)(c / ((long long)m0 * m1));
+        const T   x0 = a.origin[0] + a.h[0] * cx, y0 = a.origin[1] + a.h[1] * cy, z0 = a.origin[2] + a.h[2] * cz;
+        const T   tau = supg_tau<T, N>(a.vel, a.h, a.qp, x0, y0, z0, a.coef, a.cell_size);
+        if (tau == T(0))
+          continue;
+        const T ih[3] = {T(1) / a.h[0], T(1) / a.h[1], T(1) / a.h[2]};
+        for (int l = 0; l < N; ++l)
+          for (int j = 0; j < N; ++j)
+            for (int i = 0; i < N; ++i)
+              {
+                const int       I = K * cx + i, J = K * cy + j, L = K * cz + l;
+                const long long idx = (long long)I + (long long)a.g.n[0] * ((long long)J + (long long)a.g.n[1] * L);
+                if (is_constrained(a.g, I, J, L, idx))
+                  continue;
+                T sum = T(0);
+                for (int qz = 0; qz < N; ++qz)
+                  for (int qy = 0; qy < N; ++qy)
+#pragma unroll
+                    for (int qx = 0; qx < N; ++qx)
+                      {
+                        const T bx = a.B[qx * N + i], by = a.B[qy * N + j], bz = a.B[qz * N + l];
+                        const T gx = a.G[qx * N + i] * ih[0], gy = a.G[qy * N + j] * ih[1], gz = a.G[qz * N + l] * ih[2];
+                        const T hx = a.H[qx * N + i] * ih[0] * ih[0], hy = a.H[qy * N + j] * ih[1] * ih[1],
+                                hz = a.H[qz * N + l] * ih[2] * ih[2];
+                        const T phi = bx * by * bz;
+                        const T dp[3] = {gx * by * bz, bx * gy * bz, bx * by * gz};
+                        const T lap   = hx * by * bz + bx * hy * bz + bx * by * hz;
+                        const T x = x0 + a.h[0] * a.qp[qx], y = y0 + a.h[1] * a.qp[qy], z = z0 + a.h[2] * a.qp[qz];
+                        T       vg = T(0);
+#pragma unroll
+                        for (int d = 0; d < 3; ++d)
+                          vg += (a.vel[d] + a.vel[3 + 3 * d] * x + a.vel[4 + 3 * d] * y + a.vel[5 + 3 * d] * z) * dp[d];
+                        sum += a.qw[qx] * a.qw[qy] * a.qw[qz] * vg * (a.inv_dt * phi + a.th_adv * vg - a.th_dif * lap);
+                      }
+                atomicAdd(a.diag + idx, tau * a.det * sum);
+              }
+      }
+  }
+
+  template <typename T>
+  cudaError_t
+  adv_supg_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, cudaStream_t s)
+  {
+    if (K < 1 || K > 2)
+      return cudaErrorInvalidValue;
+    if (!p.supg)
+      return cudaSuccess;
+    AdvSupgDiagArgs<T> a{};
+    const Tables1D    &t = tables(K);
+    const int          n = t.n;
+    for (int q = 0; q < n; ++q)
+      {
+        a.qp[q] = (T)t.qp[q];
+        a.qw[q] = (T)t.qw[q];
+        for (int i = 0; i < n; ++i)
+          {
+            double hsum = 0.0; // second derivative: collocation derivative of G on the Gauss points
+            for (int r = 0; r < n; ++r)
+              hsum += t.Dq[q * n + r] * t.G[r * n + i];
+            a.B[q * n + i] = (T)t.B[q * n + i];
+            a.G[q * n + i] = (T)t.G[q * n + i];
+            a.H[q * n + i] = (T)hsum;
+          }
+      }
+    a.g         = g;
+    a.inv_dt    = (T)p.inv_dt;
+    a.th_adv    = (T)p.theta_adv;
+    a.th_dif    = (T)p.theta_dif;
+    a.coef      = (T)p.supg_coef;
+    a.cell_size = (T)(std::sqrt(p.h[0] * p.h[0] + p.h[1] * p.h[1] + p.h[2] * p.h[2]) / std::sqrt(3.0));
+    a.det       = (T)(p.h[0] * p.h[1] * p.h[2]);
+    for (int i = 0; i < 12; ++i)
+      a.vel[i] = (T)p.vel[i];
+    for (int d = 0; d < 3; ++d)
+      {
+        a.origin[d] = (T)p.origin[d];
+        a.h[d]      = (T)p.h[d];
+      }
+    a.diag                 = diag;
+    const long long ncell  = (long long)g.m[0] * g.m[1] * g.m[2];
+    const int       blocks = (int)std::max<long long>(1, std::min<long long>((ncell + 127) / 128, 148LL * 16));
+    if (K == 1)
+      adv_supg_diag_kernel<1, T><<<blocks, 128, 0, s>>>(a);
+    else
+      adv_supg_diag_kernel<2, T><<<blocks, 128, 0, s>>>(a);
+    return cudaGetLastError();
+  }
+
+  template cudaError_t adv_supg_diagonal<double>(const GridDesc &, int, const AdvParams &, double *, cudaStream_t);
+  template cudaError_t adv_supg_diagonal<float>(const GridDesc &, int, const AdvParams &, float *, cudaStream_t);
   template cudaError_t adv_apply<double>(const AdvLaunch<double> &, cudaStream_t);
   template cudaError_t adv_apply<float>(const AdvLaunch<float> &, cudaStream_t);
   template cudaError_t adv_diagonal<double>(const GridDesc &, int, const AdvParams &, double *, cudaStream_t);

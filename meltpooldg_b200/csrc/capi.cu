@@ -85,6 +85,8 @@ struct mpdg_op
   float    *d_k32 = nullptr;
   double    theta = 1.0, eps = 0.0, vel[12]{};
   HeatFaceBC    fbc{};            // boundary-face terms (heat)
+  int           supg = 0;         // SUPG stabilisation (advection-diffusion)
+  double        supg_coef = 0.0;
   const double *d_temp = nullptr; // linearisation temperature of the radiation tangent (not owned)
   int       brick[3]{}, nbr[3]{};
   int       nbr32[3]{};  // bricks per direction of the FP32 apply (its column segments may be longer)
@@ -207,6 +209,8 @@ namespace
         p.origin[d] = op->origin[d];
         p.h[d]      = op->h[d];
       }
+    p.supg      = op->supg;
+    p.supg_coef = op->supg_coef;
     return p;
   }
 
@@ -312,9 +316,26 @@ namespace
       }
     else
       {
-        MPDG_CUDA(adv_diagonal<T>(g, op->degree, adv_params(op, 0, false), diag, op->stream));
-        MPDG_CUDA(vec_absmax<T>(diag, op->ndofs, op->d_scal, op->reducer(), op->stream));
-        MPDG_CUDA(vec_invert_rel<T>(diag, op->d_scal, op->ndofs, op->stream));
+        // the SUPG part sums terms of both signs: an FP32 diagonal is computed in FP64 and rounded once
+        double *d64 = std::is_same<T, double>::value ? reinterpret_cast<double *>(diag)
+                                                     : (op->supg ? op->vec<double>("supg_diag") : nullptr);
+        if (d64)
+          {
+            MPDG_CUDA(adv_diagonal<double>(g, op->degree, adv_params(op, 0, false), d64, op->stream));
+            MPDG_CUDA(adv_supg_diagonal<double>(g, op->degree, adv_params(op, 0, false), d64, op->stream));
+            MPDG_CUDA(vec_absmax<double>(d64, op->ndofs, op->d_scal, op->reducer(), op->stream));
+            MPDG_CUDA(vec_invert_rel<double>(d64, op->d_scal, op->ndofs, op->stream));
+            if (!std::is_same<T, double>::value)
+              MPDG_CUDA(vec_convert<T, double>(diag, d64, op->ndofs, op->stream));
+          }
+        else if (op->supg)
+          return fail(MPDG_ERR_NOMEM, "diagonal work vector");
+        else
+          {
+            MPDG_CUDA(adv_diagonal<T>(g, op->degree, adv_params(op, 0, false), diag, op->stream));
+            MPDG_CUDA(vec_absmax<T>(diag, op->ndofs, op->d_scal, op->reducer(), op->stream));
+            MPDG_CUDA(vec_invert_rel<T>(diag, op->d_scal, op->ndofs, op->stream));
+          }
       }
     return MPDG_OK;
   }
@@ -827,6 +848,18 @@ mpdg_op_set_heat_bc(mpdg_op *op, const mpdg_heat_bc *bc)
 }
 
 int
+mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_ADVDIFF)
+    return fail(MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator");
+  op->supg      = enabled ? 1 : 0;
+  op->supg_coef = coefficient;
+  return MPDG_OK;
+}
+
+int
 mpdg_op_set_temperature(mpdg_op *op, const double *temperature)
 {
   if (int e = check_op(op))
@@ -877,6 +910,10 @@ mpdg_op_residual(mpdg_op *op, double *r, const double *b, const double *x)
   return apply<double>(op, (int)OutMode::BPlus, -1.0, r, x, b, 1);
 }
 
+#ifndef MPDG_HOST_SLABS
+#define MPDG_HOST_SLABS 8
+#endif
+
 namespace
 {
   // Host-buffer apply of a heat operator, pipelined over z-slabs of cells: slab s (cells
@@ -887,7 +924,7 @@ namespace
   int
   vmult_host_slabs(mpdg_op *op, double *dst_host, const double *src_host, double *ds, double *dd)
   {
-    constexpr int S = 8;
+    constexpr int S = MPDG_HOST_SLABS;
     if (!op->s_h2d)
       {
         MPDG_CUDA(cudaStreamCreateWithFlags(&op->s_h2d, cudaStreamNonBlocking));

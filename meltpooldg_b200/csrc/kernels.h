@@ -90,6 +90,8 @@ namespace mpdg
     double vel[12];   // v(x) = vel[0..2] + G x, G = vel[3..11] row-major
     double origin[3];
     double h[3];
+    int    supg      = 0;   // SUPG streamline stabilisation (ConvectionStabilizationType::SUPG)
+    double supg_coef = 0.0; // < 0: tau_c = h_c / max_q |v|, else tau_c = supg_coef h_c
   };
 
   template <typename T>
@@ -114,6 +116,9 @@ namespace mpdg
   // per-cell diagonal entries gathered per DoF, then optionally inverted with the advection rule
   template <typename T>
   cudaError_t adv_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, cudaStream_t s);
+  // adds the SUPG part of the diagonal (p.supg) on the free rows
+  template <typename T>
+  cudaError_t adv_supg_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, cudaStream_t s);
 
   template <typename T>
   void adv_brick_shape(int K, int shape[3]);

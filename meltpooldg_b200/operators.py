@@ -213,6 +213,13 @@ class AdvectionDiffusionOperator(OperatorMatrixFree):
             p.velocity[i] = float(velocity[i])
         super().__init__(mesh, p, stream)
 
+    def set_convection_stabilization(self, type: str = "SUPG", coefficient: float = -1.0) -> None:
+        """AdvectionDiffusionData::conv_stab: type "none" or "SUPG"; coefficient < 0 selects
+        tau_c = h_c / max |v| over the cell's quadrature points, otherwise tau_c = coefficient h_c."""
+        if type not in ("none", "SUPG"):
+            raise ValueError("convection stabilization type must be 'none' or 'SUPG'")
+        check(lib().mpdg_op_set_supg(self._h, 1 if type == "SUPG" else 0, float(coefficient)))
+
 
 @dataclass
 class LinearSolverData:

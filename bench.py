@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--case", default=None,
-                    help="run one named case for profiling and exit: apply_<degree>_<cells>_<f64|f32> "
+                    help="run one named case for profiling and exit: apply_<degree>_<cells>_<f64|f32>, "
+                         "faces_<degree>_<cells>_<f64|f32>, supg_<degree>_<cells>_<f64|f32>, "
                          "(e.g. apply_2_128_f32) or solve_fp64 / solve_mixed (128^3 FE_Q(2) CG to 1e-8)")
     return ap.parse_args()
 
@@ -96,6 +97,47 @@ def run_case(name):
         e1.record(stream)
         torch.cuda.synchronize()
         print(json.dumps({"case": name, "us_per_inverse_diagonal": e0.elapsed_time(e1) / 10 * 1e3}), flush=True)
+    elif name.startswith("faces_") or name.startswith("supg_"):
+        # one apply with and without the extra terms: heat with convection (x faces) and radiation
+        # (y, z faces); advection-diffusion with SUPG (tau_c = h_c / max |v|)
+        _, deg, cells, prec = name.split("_")
+        dt = torch.float64 if prec == "f64" else torch.float32
+        if name.startswith("faces_"):
+            mesh = Mesh(int(deg), (int(cells),) * 3)
+            kc = np.exp(normal_cells(mesh, seed=2, sigma=0.5))
+            op = HeatDiffuseOperator(mesh, rho_cp=1.0, dt=1e-3, conductivity_cells=kc, stream=stream.cuda_stream)
+            T = torch.tensor(300.0 + 300.0 * (uniform_dofs(mesh, seed=5) + 1.0), device="cuda")
+            op.set_temperature(T)
+            extra = lambda: op.set_boundary_conditions(convection_faces=0b000011, convection_coefficient=10.0,  # noqa: E731
+                                                       convection_temperature_infinity=300.0,
+                                                       radiation_faces=0b111100, emissivity=0.6,
+                                                       radiation_temperature_infinity=300.0)
+        else:
+            from meltpooldg_b200.operators import AdvectionDiffusionOperator
+
+            mesh = Mesh(int(deg), (int(cells),) * 3, dirichlet_faces=0b000011)
+            op = AdvectionDiffusionOperator(mesh, dt=5e-3, theta=1.0, diffusivity=1e-3,
+                                            velocity=[0.5, -0.5, 0, 0, -1, 0, 1, 0, 0, 0, 0, 0],
+                                            stream=stream.cuda_stream)
+            extra = lambda: op.set_convection_stabilization("SUPG", -1.0)  # noqa: E731
+        x = torch.tensor(uniform_dofs(mesh, seed=1), dtype=dt, device="cuda")
+        y = torch.empty_like(x)
+        out = {"case": name, "dofs": mesh.ndofs}
+        for tag in ("plain", "with_terms"):
+            if tag == "with_terms":
+                extra()
+            for _ in range(3):
+                op.vmult(y, x)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(10):
+                op.vmult(y, x)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            us = e0.elapsed_time(e1) / 10 * 1e3
+            out[tag] = {"us_per_apply": us, "gdofs": mesh.ndofs / us / 1e3}
+        print(json.dumps(out), flush=True)
     elif name == "advection":
         print(json.dumps({"case": name, **run_advection(torch, stream)}), flush=True)
     elif name in ("solve_fp64", "solve_mixed"):

@@ -300,9 +300,17 @@ namespace mpdg
     static constexpr int    MINB  = sizeof(T) == 8 ? MPDG_ADV_MINB_F64 : MPDG_ADV_MINB_F32; // CTAs per SM
   };
 
-  // the SUPG form keeps a third cell array (the strong residual) and gets the registers of one CTA per SM
+  // The SUPG form keeps a third cell array (the strong residual) and is held to half the CTAs per SM
+  // of the plain form (at least one).
+  template <int K, typename T, bool SUPG>
+  struct AdvMinBlocks
+  {
+    static constexpr int value =
+      SUPG ? (AdvLayout<K, T>::MINB > 1 ? AdvLayout<K, T>::MINB / 2 : 1) : AdvLayout<K, T>::MINB;
+  };
+
   template <int K, typename T, OutMode MODE, bool SUPG>
-  __global__ void __launch_bounds__(AdvLayout<K, T>::BR::NT, SUPG ? 1 : AdvLayout<K, T>::MINB)
+  __global__ void __launch_bounds__(AdvLayout<K, T>::BR::NT, AdvMinBlocks<K, T, SUPG>::value)
   adv_apply_kernel(const __grid_constant__ AdvArgs<T, K + 1> a)
   {
     using LAY             = AdvLayout<K, T>;

@@ -225,7 +225,9 @@ namespace mpdg
                     MPDG_PUT(i, j, K)
 #undef MPDG_PUT
           }
-        __syncthreads();
+        // no barrier here: the next layer's cp.async staging overwrites the buffer every thread
+        // finished reading before this layer's y-exchange barrier, and the next y-exchange writes
+        // come after the next layer's first barrier
       }
     if constexpr (DOT)
       release_ticket_dot<LAY::S::NT>(s, dot, br.id, dsum, s_red, s_ticket);

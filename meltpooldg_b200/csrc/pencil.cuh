@@ -397,7 +397,9 @@ namespace mpdg
                       add(0, K);
                   }
               }
-            __syncthreads();
+            // no barrier here: the next row's first barrier (after its pencil transforms) already
+            // orders every shared buffer it reuses -- tb columns are rewritten only by their own
+            // thread before it, kcs and the face buffers only after it
           }
       }
     if constexpr (DOT)

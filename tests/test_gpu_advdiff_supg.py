@@ -92,3 +92,20 @@ def test_supg_gmres_reaches_the_oracle_residual():
     y = torch.empty_like(x)
     g.vmult(y, x)
     assert rel_err(y.cpu().numpy(), o.vmult(xs)) <= 1e-12
+
+
+def test_supg_mixed_precision_solve():
+    """FP32 GMRES inside FP64 defect correction on the stabilised operator reaches the oracle residual."""
+    import torch
+
+    from meltpooldg_b200.operators import LinearSolver
+
+    dt, theta, eps, coef = 5e-3, 1.0, 1e-3, 0.1
+    o, g, om, cm = supg_pair(2, (12, 10, 9), 0b010011, theta, eps, coef, dt)
+    b = uniform_dofs(om, seed=16)
+    b[cm != 0] = 0.0
+    x = torch.zeros(om.ndofs, dtype=torch.float64, device="cuda")
+    LinearSolver.solve_mixed(g, x, to_gpu(b), outer_rel_tol=1e-9, inner_rel_tol=1e-3, solver="GMRES")
+    xs = x.cpu().numpy()
+    r = b - o.vmult(xs) - supg_apply(om, cm, VEL, coef, 1.0 / dt, theta, theta * eps, xs)
+    assert np.linalg.norm(r) <= 2e-9 * np.linalg.norm(b)

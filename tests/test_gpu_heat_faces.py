@@ -154,3 +154,20 @@ def test_face_argument_checks():
     bc = L.HeatBC()
     bc.convection_faces = 1
     assert L.lib().mpdg_op_set_heat_bc(a._h, C.byref(bc)) == MPDG_ERR_ARG
+
+
+def test_host_buffer_vmult_with_faces():
+    """mpdg_op_vmult_host on an operator with face terms (large enough for the slab pipeline, which
+    the face terms switch off) equals the device vmult."""
+    import torch
+
+    o, g, om, cm, bc, T, Td = setup(2, (80, 80, 82), 0b000001, False,
+                                    dict(convection_faces=0b000010, radiation_faces=0b111100, **CONV, **RAD))
+    x = uniform_dofs(om, seed=4)
+    xd = to_gpu(x)
+    yd = torch.empty_like(xd)
+    g.vmult(yd, xd)
+    yh = np.empty_like(x)
+    g.vmult_host(yh, np.ascontiguousarray(x))
+    # the same kernels; atomics on shared points may add in another order
+    assert rel_err(yh, yd.cpu().numpy()) <= 1e-14

@@ -300,13 +300,14 @@ namespace mpdg
     static constexpr int    MINB  = sizeof(T) == 8 ? MPDG_ADV_MINB_F64 : MPDG_ADV_MINB_F32; // CTAs per SM
   };
 
-  // The SUPG form keeps a third cell array (the strong residual) and is held to half the CTAs per SM
-  // of the plain form (at least one).
+  // The SUPG form keeps a third cell array (the strong residual).  At k = 2 it is held to half the
+  // CTAs per SM of the plain form (at least one); at k = 1 the arrays are small and the plain
+  // occupancy wins despite some spilling (Q1 FP64: 658 against 988 us per 7.2 M DoFs).
   template <int K, typename T, bool SUPG>
   struct AdvMinBlocks
   {
     static constexpr int value =
-      SUPG ? (AdvLayout<K, T>::MINB > 1 ? AdvLayout<K, T>::MINB / 2 : 1) : AdvLayout<K, T>::MINB;
+      (SUPG && K == 2) ? (AdvLayout<K, T>::MINB > 1 ? AdvLayout<K, T>::MINB / 2 : 1) : AdvLayout<K, T>::MINB;
   };
 
   template <int K, typename T, OutMode MODE, bool SUPG>

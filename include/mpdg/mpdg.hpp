@@ -230,11 +230,23 @@ namespace mpdg
     {
       check(mpdg_op_set_heat_bc(handle(), &bc));
     }
-    // the temperature the radiation tangent is linearised at (device array, kept by reference)
+    // the temperature the radiation and solidification tangents are linearised at (device array,
+    // kept by reference)
     void
     set_temperature(const double *temperature)
     {
       check(mpdg_op_set_temperature(handle(), temperature));
+    }
+    // temperature-dependent material (nullptr switches it off) and the old temperature it needs
+    void
+    set_solidification(const mpdg_solid_liquid *material)
+    {
+      check(mpdg_op_set_solidification(handle(), material));
+    }
+    void
+    set_old_temperature(const double *temperature_old)
+    {
+      check(mpdg_op_set_old_temperature(handle(), temperature_old));
     }
   };
 
@@ -501,6 +513,7 @@ namespace mpdg
     {
       op_.fill(zero_, 0.0);
       op_.set_temperature(T_);
+      op_.set_old_temperature(T_old_);
       // solution history: every old slot starts as the initial solution (SolutionHistory::apply_old)
       const int n_hist = std::max(predictor_.n_old_solution_vectors, 2);
       history_         = {T_, T_old_};

@@ -207,6 +207,28 @@ MPDG_API int mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient);
    inverse diagonal of an operator with radiation faces and no temperature return MPDG_ERR_ARG. */
 MPDG_API int mpdg_op_set_temperature(mpdg_op *op, const double *temperature);
 
+/* Temperature-dependent material of the heat operator, MaterialTypes::liquid_solid without latent
+   heat (include/meltpooldg/core/material.templates.hpp:296-360, :540-620, :748-765), FE_Q(1, 2):
+   solid fraction f_s = clamp((T_liquidus - T) / (T_liquidus - T_solidus), 0, 1) (mushy zone) or
+   T < T_solidus (sharp); rho, c_p and k blend cubically, v_l + (v_s - v_l)(3 f_s^2 - 2 f_s^3).
+   With it vmult applies the solidification tangent (source/heat/heat_diffuse_operator.cpp:1029-1050)
+     (rho c_p(T) / dt + d(rho c_p)/dT (T - T_old) / dt) u,  k(T) grad u + dk/dT grad T u
+   at the temperature of mpdg_op_set_temperature and the old temperature of
+   mpdg_op_set_old_temperature (both read plainly); create_rhs(dst, T, T_old, q) adds
+   M q - int rho c_p(T) (T - T_old) / dt phi - int k(T) grad T . grad phi (:485-527); the inverse
+   diagonal is the tangent's.  rho_cp and the conductivity of mpdg_op_params are then unused.
+   NULL switches it off. */
+typedef struct mpdg_solid_liquid
+{
+  double  liquid_density, liquid_specific_heat, liquid_conductivity;
+  double  solid_density, solid_specific_heat, solid_conductivity;
+  double  liquidus_temperature, solidus_temperature;
+  int32_t sharp; /* SolidLiquidPropertiesTransitionType: 0 mushy_zone, 1 sharp */
+  int32_t reserved;
+} mpdg_solid_liquid;
+MPDG_API int mpdg_op_set_solidification(mpdg_op *op, const mpdg_solid_liquid *material);
+MPDG_API int mpdg_op_set_old_temperature(mpdg_op *op, const double *temperature_old);
+
 /* OperatorMatrixFree::vmult (operator_base.hpp:239-243): dst = A src (FP64 / FP32) */
 MPDG_API int mpdg_op_vmult(mpdg_op *op, double *dst, const double *src);
 MPDG_API int mpdg_op_vmult_f32(mpdg_op *op, float *dst, const float *src);

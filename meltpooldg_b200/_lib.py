@@ -69,6 +69,24 @@ class HeatBC(C.Structure):
     ]
 
 
+class SolidLiquid(C.Structure):
+    """mpdg_solid_liquid: liquid / solid density, specific heat and conductivity, liquidus and
+    solidus temperature, transition type (0 mushy zone, 1 sharp)."""
+
+    _fields_ = [
+        ("liquid_density", C.c_double),
+        ("liquid_specific_heat", C.c_double),
+        ("liquid_conductivity", C.c_double),
+        ("solid_density", C.c_double),
+        ("solid_specific_heat", C.c_double),
+        ("solid_conductivity", C.c_double),
+        ("liquidus_temperature", C.c_double),
+        ("solidus_temperature", C.c_double),
+        ("sharp", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
 class SolverParams(C.Structure):
     _fields_ = [
         ("solver", C.c_int32),
@@ -141,6 +159,8 @@ SIGNATURES = [
     ("mpdg_vec_alloc", [P, C.POINTER(C.c_void_p)], C.c_int),
     ("mpdg_vec_free", [P], C.c_int),
     ("mpdg_op_set_temperature", [P, P], C.c_int),
+    ("mpdg_op_set_solidification", [P, C.POINTER(SolidLiquid)], C.c_int),
+    ("mpdg_op_set_old_temperature", [P, P], C.c_int),
     ("mpdg_op_vmult", [P, P, P], C.c_int),
     ("mpdg_op_vmult_f32", [P, P, P], C.c_int),
     ("mpdg_op_vmult_host", [P, P, P], C.c_int),

@@ -85,6 +85,10 @@ struct mpdg_op
   float    *d_k32 = nullptr;
   double    theta = 1.0, eps = 0.0, vel[12]{};
   HeatFaceBC    fbc{};            // boundary-face terms (heat)
+  bool          solid = false;    // temperature-dependent material (heat, FE_Q(1, 2))
+  SolidMaterial smat{};
+  const double *d_temp_old = nullptr; // T_old of the solidification tangent (not owned)
+  long long     sync_cap = 0;         // brick flags allocated in d_sync (after the 3 counters)
   int           supg = 0;         // SUPG stabilisation (advection-diffusion)
   double        supg_coef = 0.0;
   const double *d_temp = nullptr; // linearisation temperature of the radiation tangent (not owned)
@@ -214,6 +218,57 @@ namespace
     return p;
   }
 
+  // Temperature-dependent material: the tangent (rhs = false) or the residual part of create_rhs
+  // (rhs = true, dst +=, src unused) with the operator's temperature and old temperature.  FP32
+  // applies read FP32 copies of both.
+  template <typename T>
+  int
+  solid_apply(mpdg_op *op, int mode, double scale, T *dst, const T *src, const T *b, int mask_src, const int *skip,
+              bool rhs, const double *temp = nullptr, const double *temp_old = nullptr)
+  {
+    const double *t64 = temp ? temp : op->d_temp, *to64 = temp_old ? temp_old : op->d_temp_old;
+    if (!t64 || !to64)
+      return fail(MPDG_ERR_ARG, "the solidification tangent needs the temperature and the old temperature "
+                                "(mpdg_op_set_temperature, mpdg_op_set_old_temperature)");
+    HeatSolidLaunch<T> h;
+    h.degree = op->degree;
+    h.mode   = mode;
+    h.rhs    = rhs ? 1 : 0;
+    h.scale  = scale;
+    h.dt     = op->dt;
+    for (int d = 0; d < 3; ++d)
+      h.hlen[d] = op->h[d];
+    h.mat  = op->smat;
+    h.grid = op->grid<T>();
+    int shape[3];
+    heat_solid_brick_shape<T>(op->degree, shape);
+    for (int d = 0; d < 3; ++d)
+      h.grid.nbr[d] = (op->m[d] + shape[d] - 1) / shape[d];
+    h.sync = op->sync();
+    if constexpr (std::is_same<T, double>::value)
+      {
+        h.temp     = t64;
+        h.temp_old = to64;
+      }
+    else
+      {
+        T *t32 = op->vec<T>("solid_t32"), *to32 = op->vec<T>("solid_to32");
+        if (!t32 || !to32)
+          return fail(MPDG_ERR_NOMEM, "FP32 temperature copies");
+        MPDG_CUDA(vec_convert<T, double>(t32, t64, op->ndofs, op->stream));
+        MPDG_CUDA(vec_convert<T, double>(to32, to64, op->ndofs, op->stream));
+        h.temp     = t32;
+        h.temp_old = to32;
+      }
+    h.src      = src;
+    h.dst      = dst;
+    h.b        = b;
+    h.mask_src = mask_src;
+    h.skip     = skip;
+    MPDG_CUDA(heat_solid_apply<T>(h, op->stream));
+    return MPDG_OK;
+  }
+
   // Generic apply.  mode: OutMode; 'which' selects the physics variant:
   //   0 tangent, 1 mass only (heat, coefficient mass_scale), 2 stiffness only (heat, scale on k),
   //   3 advection with theta replaced by theta - 1 (create_rhs)
@@ -243,7 +298,13 @@ namespace
           h.dot = *dot;
         if (which == 0 && op->tangent_faces() && op->fbc.radiation_faces && !op->d_temp)
           return fail(MPDG_ERR_ARG, "radiation faces need the linearisation temperature (mpdg_op_set_temperature)");
-        MPDG_CUDA(heat_apply<T>(h, op->stream));
+        if (which == 0 && op->solid)
+          {
+            if (int e = solid_apply<T>(op, mode, scale, dst, src, b, mask_src, skip, false))
+              return e;
+          }
+        else
+          MPDG_CUDA(heat_apply<T>(h, op->stream));
         if (which == 0 && op->tangent_faces())
           {
             HeatFaceLaunch<T> f;
@@ -285,16 +346,26 @@ namespace
   inverse_diagonal(mpdg_op *op, T *diag)
   {
     const GridDesc g = op->grid();
-    if (op->kind == MPDG_HEAT && op->tangent_faces())
+    if (op->kind == MPDG_HEAT && (op->tangent_faces() || op->solid))
       {
         // cell and face parts summed in FP64, then inverted (|d| > 1e-10 ? 1/d : 1)
         if (op->fbc.radiation_faces && !op->d_temp)
           return fail(MPDG_ERR_ARG, "radiation faces need the linearisation temperature (mpdg_op_set_temperature)");
+        if (op->solid && (!op->d_temp || !op->d_temp_old))
+          return fail(MPDG_ERR_ARG, "the solidification tangent needs the temperature and the old temperature");
         double *d64 = std::is_same<T, double>::value ? reinterpret_cast<double *>(diag) : op->vec<double>("face_diag");
         if (!d64)
           return fail(MPDG_ERR_NOMEM, "diagonal work vector");
-        MPDG_CUDA(heat_diagonal<double>(g, op->degree, heat_geom(op, op->rho_cp / op->dt), op->k, op->kcell<double>(),
-                                        d64, false, 0.0, op->stream));
+        if (op->solid)
+          {
+            MPDG_CUDA(vec_fill<double>(d64, 0.0, op->ndofs, op->stream));
+            MPDG_CUDA(heat_solid_diagonal(g, op->degree, op->smat, op->dt, op->h, op->d_temp, op->d_temp_old, d64,
+                                          op->stream));
+            MPDG_CUDA(vec_set_constrained<double>(d64, 1.0, g, op->stream));
+          }
+        else
+          MPDG_CUDA(heat_diagonal<double>(g, op->degree, heat_geom(op, op->rho_cp / op->dt), op->k,
+                                          op->kcell<double>(), d64, false, 0.0, op->stream));
         HeatFaceLaunch<double> f;
         f.degree = op->degree;
         f.mode   = 2;
@@ -399,7 +470,7 @@ namespace
       return e;
     MPDG_CUDA(cg_init<T>(r, invd, p, op->d_cg, hist, op->reducer(), n, op->stream));
     // heat operators without a per-DoF mask fuse p^T A p into the apply and set alpha on the device
-    const bool fused = op->kind == MPDG_HEAT && op->d_part != nullptr && !op->tangent_faces() &&
+    const bool fused = op->kind == MPDG_HEAT && op->d_part != nullptr && !op->tangent_faces() && !op->solid &&
                        heat_apply_fuses_dot(op->degree, op->d_mask != nullptr, true);
     DotSink    sink;
     sink.part  = op->d_part;
@@ -698,6 +769,7 @@ mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op
     return clean(MPDG_ERR_NOMEM, "device allocation in mpdg_op_create");
   if (op->kind == MPDG_HEAT && cudaMalloc(&op->d_part, sizeof(double) * nbrk) != cudaSuccess)
     return clean(MPDG_ERR_NOMEM, "fused dot partials");
+  op->sync_cap = nbrk;
   if (cudaMemset(op->d_sync, 0, sizeof(unsigned) * (3 + nbrk)) != cudaSuccess ||
       cudaMemset(op->d_err, 0, sizeof(int)) != cudaSuccess)
     return clean(MPDG_ERR_CUDA, "cudaMemset in mpdg_op_create");
@@ -844,6 +916,68 @@ mpdg_op_set_heat_bc(mpdg_op *op, const mpdg_heat_bc *bc)
   for (int i = 0; i < 6; ++i)
     f.neumann_flux[i] = bc->neumann_flux[i];
   op->fbc = f;
+  return MPDG_OK;
+}
+
+int
+mpdg_op_set_solidification(mpdg_op *op, const mpdg_solid_liquid *mat)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_HEAT)
+    return fail(MPDG_ERR_ARG, "temperature-dependent material applies to the heat operator");
+  if (!mat)
+    {
+      op->solid = false;
+      return MPDG_OK;
+    }
+  if (op->degree > 2)
+    return fail(MPDG_ERR_UNSUPPORTED, "temperature-dependent material supports FE_Q degree 1..2");
+  if (!(mat->liquid_density > 0 && mat->liquid_specific_heat > 0 && mat->liquid_conductivity > 0 &&
+        mat->solid_density > 0 && mat->solid_specific_heat > 0 && mat->solid_conductivity > 0) ||
+      (!mat->sharp && !(mat->liquidus_temperature > mat->solidus_temperature)))
+    return fail(MPDG_ERR_ARG, "material parameters must be positive and the liquidus above the solidus");
+  // the solid-phase kernel's bricks may outnumber the flags allocated for the constant-material ones
+  int shape[3];
+  heat_solid_brick_shape<float>(op->degree, shape);
+  long long nb = 1;
+  for (int d = 0; d < 3; ++d)
+    nb *= (op->m[d] + shape[d] - 1) / shape[d];
+  if (nb > op->sync_cap)
+    {
+      unsigned *fresh = nullptr;
+      MPDG_CUDA(cudaStreamSynchronize(op->stream));
+      if (cudaMalloc(&fresh, sizeof(unsigned) * (3 + nb)) != cudaSuccess)
+        return fail(MPDG_ERR_NOMEM, "brick flags");
+      MPDG_CUDA(cudaMemset(fresh, 0, sizeof(unsigned) * (3 + nb)));
+      MPDG_CUDA(cudaFree(op->d_sync));
+      op->d_sync   = fresh;
+      op->sync_cap = nb;
+      op->epoch    = 0;
+    }
+  SolidMaterial m;
+  m.rho_l      = mat->liquid_density;
+  m.cp_l       = mat->liquid_specific_heat;
+  m.k_l        = mat->liquid_conductivity;
+  m.rho_s      = mat->solid_density;
+  m.cp_s       = mat->solid_specific_heat;
+  m.k_s        = mat->solid_conductivity;
+  m.t_liquidus = mat->liquidus_temperature;
+  m.t_solidus  = mat->solidus_temperature;
+  m.sharp      = mat->sharp ? 1 : 0;
+  op->smat     = m;
+  op->solid    = true;
+  return MPDG_OK;
+}
+
+int
+mpdg_op_set_old_temperature(mpdg_op *op, const double *temperature_old)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_HEAT)
+    return fail(MPDG_ERR_ARG, "the old temperature belongs to the heat operator");
+  op->d_temp_old = temperature_old;
   return MPDG_OK;
 }
 
@@ -998,7 +1132,7 @@ mpdg_op_vmult_host(mpdg_op *op, double *dst_host, const double *src_host)
   if (!ds || !dd)
     return fail(MPDG_ERR_NOMEM, "staging vectors");
   const size_t bytes = sizeof(double) * op->ndofs;
-  if (op->kind == MPDG_HEAT && op->d_mask == nullptr && !op->tangent_faces() && op->m[2] >= 16 &&
+  if (op->kind == MPDG_HEAT && op->d_mask == nullptr && !op->tangent_faces() && !op->solid && op->m[2] >= 16 &&
       op->ndofs >= (1 << 22))
     return vmult_host_slabs(op, dst_host, src_host, ds, dd);
   MPDG_CUDA(cudaMemcpyAsync(ds, src_host, bytes, cudaMemcpyHostToDevice, op->stream));
@@ -1038,6 +1172,31 @@ mpdg_op_create_rhs(mpdg_op *op, double *dst, const double *a, const double *b, c
     return fail(MPDG_ERR_ZERO_DT, "time increment must be positive (ExcZeroTimeIncrement)");
   if (!dst || !a)
     return fail(MPDG_ERR_ARG, "create_rhs needs dst and its first input");
+  if (op->kind == MPDG_HEAT && op->solid)
+    {
+      // dst += M q - int rho c_p(T) (T - T_old) / dt phi - int k(T) grad T . grad phi (+ faces)
+      if (!b)
+        return fail(MPDG_ERR_ARG, "create_rhs with temperature-dependent material needs T_old");
+      if (c)
+        if (int e = apply<double>(op, (int)OutMode::Add, 1.0, dst, c, nullptr, 0, 1))
+          return e;
+      if (int e = solid_apply<double>(op, (int)OutMode::Add, 1.0, dst, nullptr, nullptr, 0, nullptr, true, a, b))
+        return e;
+      if (heat_faces_active(op->fbc, 1))
+        {
+          HeatFaceLaunch<double> f;
+          f.degree = op->degree;
+          f.mode   = 1;
+          for (int d = 0; d < 3; ++d)
+            f.hlen[d] = op->h[d];
+          f.grid = op->grid();
+          f.bc   = op->fbc;
+          f.temp = a;
+          f.dst  = dst;
+          MPDG_CUDA(heat_faces<double>(f, op->stream));
+        }
+      return MPDG_OK;
+    }
   if (op->kind == MPDG_HEAT)
     {
       // v = (rho c_p/dt)(T_old - T) + q ; dst += M v - K_k T   (plain reads, free rows)
@@ -1274,8 +1433,9 @@ mpdg_adjoint_heat(mpdg_op *op, const double *log_k, const double *qhat, double a
     return e;
   if (!log_k || !qhat || !T_target || !prm || prm->n_steps < 1)
     return fail(MPDG_ERR_ARG, "invalid argument to mpdg_adjoint_heat");
-  if (heat_faces_active(op->fbc, 1))
-    return fail(MPDG_ERR_UNSUPPORTED, "the adjoint covers operators without boundary-face terms");
+  if (heat_faces_active(op->fbc, 1) || op->solid)
+    return fail(MPDG_ERR_UNSUPPORTED, "the adjoint covers operators without boundary-face terms or "
+                                      "temperature-dependent material");
   double *invd = nullptr;
   if (int e = adjoint_setup(op, log_k, &invd))
     return e;

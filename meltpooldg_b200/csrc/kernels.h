@@ -75,6 +75,44 @@ namespace mpdg
     const int    *skip = nullptr;
   };
 
+  // ---- temperature-dependent material (solid / liquid phases, heat_solid.cu), FE_Q(1, 2)
+  struct SolidMaterial
+  {
+    double rho_l = 1.0, cp_l = 1.0, k_l = 1.0; // liquid
+    double rho_s = 1.0, cp_s = 1.0, k_s = 1.0; // solid
+    double t_liquidus = 1.0, t_solidus = 0.0;
+    int    sharp = 0;                          // 0 mushy zone, 1 sharp transition at t_solidus
+  };
+
+  template <typename T>
+  struct HeatSolidLaunch
+  {
+    int           degree = 2;
+    int           mode   = 0;     // OutMode of the tangent apply
+    int           rhs    = 0;     // 1: dst += residual part of create_rhs (Add), src unused
+    double        scale  = 1.0;   // tangent: dst (+)= scale * A src
+    double        dt     = 1.0;
+    double        hlen[3]{};
+    SolidMaterial mat{};
+    GridDesc      grid{};         // nbr from heat_solid_brick_shape
+    SyncDesc      sync{};
+    const T      *src      = nullptr;
+    const T      *temp     = nullptr; // linearisation temperature (plain reads)
+    const T      *temp_old = nullptr;
+    T            *dst      = nullptr;
+    const T      *b        = nullptr;
+    int           mask_src = 1;
+    const int    *skip     = nullptr;
+  };
+
+  template <typename T>
+  void heat_solid_brick_shape(int K, int shape[3]);
+  template <typename T>
+  cudaError_t heat_solid_apply(const HeatSolidLaunch<T> &h, cudaStream_t s);
+  // adds the tangent's diagonal on the free rows of diag (FP64)
+  cudaError_t heat_solid_diagonal(const GridDesc &g, int K, const SolidMaterial &mat, double dt, const double hlen[3],
+                                  const double *temp, const double *temp_old, double *diag, cudaStream_t s);
+
   // whether mode (0 tangent / 2 diagonal, 1 rhs) has any face to integrate
   bool heat_faces_active(const HeatFaceBC &bc, int mode);
 

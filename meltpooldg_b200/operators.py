@@ -194,6 +194,25 @@ class HeatDiffuseOperator(OperatorMatrixFree):
             bc.neumann_flux[i] = float(neumann_flux[i])
         check(lib().mpdg_op_set_heat_bc(self._h, C.byref(bc)))
 
+    def set_solidification(self, liquid=(1.0, 1.0, 1.0), solid=(1.0, 1.0, 1.0), liquidus_temperature: float = 1.0,
+                           solidus_temperature: float = 0.0, sharp: bool = False, enabled: bool = True) -> None:
+        """Temperature-dependent material (MaterialTypes::liquid_solid, no latent heat); liquid and
+        solid are (density, specific heat capacity, thermal conductivity)."""
+        if not enabled:
+            check(lib().mpdg_op_set_solidification(self._h, None))
+            return
+        m = L.SolidLiquid()
+        m.liquid_density, m.liquid_specific_heat, m.liquid_conductivity = (float(v) for v in liquid)
+        m.solid_density, m.solid_specific_heat, m.solid_conductivity = (float(v) for v in solid)
+        m.liquidus_temperature, m.solidus_temperature = float(liquidus_temperature), float(solidus_temperature)
+        m.sharp = 1 if sharp else 0
+        check(lib().mpdg_op_set_solidification(self._h, C.byref(m)))
+
+    def set_old_temperature(self, temperature_old_device) -> None:
+        """Old temperature of the solidification tangent (kept by reference)."""
+        self._temperature_old = temperature_old_device
+        check(lib().mpdg_op_set_old_temperature(self._h, _ptr(temperature_old_device)))
+
     def set_temperature(self, temperature_device) -> None:
         """Linearisation temperature of the radiation tangent (kept by reference, as the reference's
         operator keeps a const reference to its temperature vector)."""

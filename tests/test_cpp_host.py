@@ -30,6 +30,7 @@ def test_cpp_host_layer_compiles_and_links(tmp_path):
     build_program(tmp_path)
     build_program(tmp_path, "heat_radiation")
     build_program(tmp_path, "heat_predictor")
+    build_program(tmp_path, "heat_solidification")
 
 
 @pytest.mark.gpu
@@ -151,3 +152,52 @@ def test_cpp_predictors_match_oracle(tmp_path):
         finals[kind] = data[-1, 1]
     for kind, T in finals.items():
         assert np.max(np.abs(T - finals["none"])) <= 1e-9 * np.max(np.abs(T)), kind
+
+
+def oracle_solidification_steps():
+    """The time steps of tests/cpp/heat_solidification.cpp on the oracle: Newton on
+    oracle/solidification.py, each linear step by Jacobi-GMRES (scipy) to 1e-13, to a correction
+    below 1e-12 of the temperature."""
+    from scipy.sparse.linalg import LinearOperator, gmres
+
+    from oracle.oracle import Mesh as OMesh
+    from oracle.solidification import SolidLiquid, diagonal, residual, tangent_apply
+
+    om = OMesh(2, (8, 8, 8))
+    cm = om.face_mask(0b000001)
+    mat = SolidLiquid((7.4, 0.8, 30.0), (7.9, 0.6, 20.0), 1700.0, 1600.0)
+    n, dt = om.ndofs, 2e-3
+    X, _, _ = om.coords()
+    T = 1500.0 + 250.0 * X
+    steps = []
+    for _ in range(3):
+        T_old = T.copy()
+        for _ in range(30):
+            r = residual(om, cm, mat, dt, T, T_old)
+            Tl = T.copy()
+            A = LinearOperator((n, n), matvec=lambda v, Tl=Tl: tangent_apply(om, cm, mat, dt, Tl, T_old, v)
+                               + np.where(cm != 0, v, 0.0))
+            d = diagonal(om, cm, mat, dt, Tl, T_old)
+            d[cm != 0] = 1.0
+            dT, info = gmres(A, r, rtol=1e-13, atol=0.0, restart=60, maxiter=200,
+                             M=LinearOperator((n, n), matvec=lambda v, d=d: v / d))
+            assert info == 0
+            T = T + np.where(cm != 0, 0.0, dT)
+            if np.linalg.norm(dT) <= 1e-12 * np.linalg.norm(T):
+                break
+        steps.append(T.copy())
+    return np.array(steps)
+
+
+@pytest.mark.gpu
+def test_cpp_newton_with_solidification_matches_oracle(tmp_path):
+    exe = build_program(tmp_path, "heat_solidification")
+    out = str(tmp_path / "T.bin")
+    r = subprocess.run([exe, out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    ref = oracle_solidification_steps()
+    got = np.fromfile(out, dtype=np.float64).reshape(ref.shape)
+    for s in range(ref.shape[0]):
+        assert np.max(np.abs(got[s] - ref[s])) <= 1e-9 * np.max(np.abs(ref[s]))
+    # part of the block crosses the mushy zone
+    assert np.any((ref[-1] > 1600.0) & (ref[-1] < 1700.0))

@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--case", default=None,
                     help="run one named case for profiling and exit: apply_<degree>_<cells>_<f64|f32>, "
-                         "faces_<degree>_<cells>_<f64|f32>, supg_<degree>_<cells>_<f64|f32>, "
+                         "faces_<degree>_<cells>_<f64|f32>, supg_<degree>_<cells>_<f64|f32>, solid_<degree>_<cells>_<f64|f32>, "
                          "(e.g. apply_2_128_f32) or solve_fp64 / solve_mixed (128^3 FE_Q(2) CG to 1e-8)")
     return ap.parse_args()
 
@@ -97,7 +97,7 @@ def run_case(name):
         e1.record(stream)
         torch.cuda.synchronize()
         print(json.dumps({"case": name, "us_per_inverse_diagonal": e0.elapsed_time(e1) / 10 * 1e3}), flush=True)
-    elif name.startswith("faces_") or name.startswith("supg_"):
+    elif name.startswith("faces_") or name.startswith("supg_") or name.startswith("solid_"):
         # one apply with and without the extra terms: heat with convection (x faces) and radiation
         # (y, z faces); advection-diffusion with SUPG (tau_c = h_c / max |v|)
         _, deg, cells, prec = name.split("_")
@@ -112,6 +112,13 @@ def run_case(name):
                                                        convection_temperature_infinity=300.0,
                                                        radiation_faces=0b111100, emissivity=0.6,
                                                        radiation_temperature_infinity=300.0)
+        elif name.startswith("solid_"):
+            mesh = Mesh(int(deg), (int(cells),) * 3, dirichlet_faces=0b000001)
+            op = HeatDiffuseOperator(mesh, rho_cp=1.0, dt=1e-3, conductivity=1.0, stream=stream.cuda_stream)
+            T = torch.tensor(1650.0 + 90.0 * uniform_dofs(mesh, seed=5), device="cuda")
+            op.set_temperature(T)
+            op.set_old_temperature(T - 2.0)
+            extra = lambda: op.set_solidification((7.4, 0.8, 30.0), (7.9, 0.6, 20.0), 1700.0, 1600.0)  # noqa: E731
         else:
             from meltpooldg_b200.operators import AdvectionDiffusionOperator
 

@@ -14,10 +14,10 @@
 // (0 at f_s = 0 or 1).  No latent heat (apparent capacity).
 //
 // Per cell (one thread), quadrature form in registers: the values of u, T and T_old at the Gauss
-// points (three sweeps of the 1-D basis each), the mass-like term pointwise, then direction by
-// direction the flux with the collocation derivative on the Gauss points and its transpose, and
-// the transposed basis sweeps back to the nodes; cells add into the brick accumulator in shared
-// memory and the brick is written as in the other brick kernels.
+// points (three sweeps of the 1-D basis each), the mass-like term pointwise, then Gauss point by
+// Gauss point the conductivity (once), the three gradients by the collocation derivative and the
+// flux tested with its transpose, and the transposed basis sweeps back to the nodes; cells add into
+// the brick accumulator in shared memory and the brick is written as in the other brick kernels.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,6 +25,13 @@
 
 #include "brick.cuh"
 #include "kernels.h"
+
+#ifndef MPDG_SOLID_MINB_F64
+#define MPDG_SOLID_MINB_F64 2
+#endif
+#ifndef MPDG_SOLID_MINB_F32
+#define MPDG_SOLID_MINB_F32 4
+#endif
 
 namespace mpdg
 {
@@ -36,6 +43,35 @@ namespace mpdg
       T   rho_l, cp_l, k_l, rho_s, cp_s, k_s, t_liquidus, t_solidus, inv_mushy;
       int sharp;
     };
+
+    // solid fraction, cubic blend weight and its temperature derivative at temperature t
+    template <typename T>
+    __device__ __forceinline__ void
+    solid_fraction(const SolidMat<T> &m, T t, T &fs, T &w, T &dw)
+    {
+      if (m.sharp)
+        fs = t < m.t_solidus ? T(1) : T(0);
+      else
+        fs = fmin(fmax((m.t_liquidus - t) * m.inv_mushy, T(0)), T(1));
+      w  = (T(3) - T(2) * fs) * fs * fs;
+      dw = (fs == T(0) || fs == T(1)) ? T(0) : -m.inv_mushy * (T(6) * fs - T(6) * fs * fs);
+    }
+    template <typename T>
+    __device__ __forceinline__ T
+    solid_blend(T fs, T w, T vl, T vs)
+    {
+      return fs == T(0) ? vl : (fs == T(1) ? vs : vl + (vs - vl) * w);
+    }
+    // k and dk/dT at temperature t
+    template <typename T>
+    __device__ __forceinline__ void
+    solid_conductivity(const SolidMat<T> &m, T t, T &k, T &dk)
+    {
+      T fs, w, dw;
+      solid_fraction(m, t, fs, w, dw);
+      k  = solid_blend(fs, w, m.k_l, m.k_s);
+      dk = (m.k_s - m.k_l) * dw;
+    }
 
     // rho c_p, k and their temperature derivatives at temperature t
     template <typename T>
@@ -81,7 +117,7 @@ namespace mpdg
       static constexpr int NT = BX * BY * BZ;
       using BR                = Brick<K, BX, BY, BZ, NT>;
       static constexpr size_t bytes = sizeof(T) * 4 * (size_t)BR::NPTS; // u, T, T_old, accumulator
-      static constexpr int    MINB  = sizeof(T) == 8 ? 1 : 2;
+      static constexpr int    MINB  = sizeof(T) == 8 ? MPDG_SOLID_MINB_F64 : MPDG_SOLID_MINB_F32; // CTAs per SM
     };
 
     // v = M v along direction D of an N^3 array (TR: M^T)
@@ -108,53 +144,6 @@ namespace mpdg
                 for (int k = 0; k < N; ++k)
                   s = fma(TR ? M[k * N + r] : M[r * N + k], in[k], s);
                 v[base + r * S] = s;
-              }
-          }
-    }
-
-    // flux of direction D: R += D_d^T f, f = JxW (k grad_d u + dk grad_d T u) / h_d (tangent) or
-    // -JxW k grad_d T / h_d (residual), gradients through the collocation derivative
-    template <typename T, int N, int D, bool RHS>
-    __device__ __forceinline__ void
-    solid_flux(const SolidArgs<T, N> &a, const T *uq, const T *tq, T *R)
-    {
-      constexpr int S     = D == 0 ? 1 : (D == 1 ? N : N * N);
-      const T       inv_h = T(1) / a.h[D];
-#pragma unroll
-      for (int aa = 0; aa < N; ++aa)
-#pragma unroll
-        for (int c = 0; c < N; ++c)
-          {
-            const int base = D == 0 ? (aa * N + c) * N : (D == 1 ? aa * N * N + c : aa * N + c);
-            T         f[N];
-#pragma unroll
-            for (int r = 0; r < N; ++r)
-              {
-                T gt = T(0), gu = T(0);
-#pragma unroll
-                for (int k = 0; k < N; ++k)
-                  {
-                    gt = fma(a.D[r * N + k], tq[base + k * S], gt);
-                    if constexpr (!RHS)
-                      gu = fma(a.D[r * N + k], uq[base + k * S], gu);
-                  }
-                const int q = base + r * S;
-                T         rc, k, drc, dk;
-                solid_material(a.m, tq[q], rc, k, drc, dk);
-                const T jw = a.det * a.w3[q] * inv_h * inv_h;
-                if constexpr (RHS)
-                  f[r] = -jw * k * gt;
-                else
-                  f[r] = jw * (k * gu + dk * gt * uq[q]);
-              }
-#pragma unroll
-            for (int r = 0; r < N; ++r)
-              {
-                T s = R[base + r * S];
-#pragma unroll
-                for (int k = 0; k < N; ++k)
-                  s = fma(a.D[k * N + r], f[k], s);
-                R[base + r * S] = s;
               }
           }
     }
@@ -229,9 +218,46 @@ namespace mpdg
               else
                 R[q] = jw * (rc + drc * (tq[q] - R[q])) * uq[q];
             }
-          solid_flux<T, N, 0, RHS>(a, uq, tq, R);
-          solid_flux<T, N, 1, RHS>(a, uq, tq, R);
-          solid_flux<T, N, 2, RHS>(a, uq, tq, R);
+          // fluxes point by point: the conductivity once per Gauss point, the three gradients by
+          // the collocation derivative along each direction, the test by its transpose
+          const T ih2[3] = {T(1) / (a.h[0] * a.h[0]), T(1) / (a.h[1] * a.h[1]), T(1) / (a.h[2] * a.h[2])};
+#pragma unroll
+          for (int qz = 0; qz < N; ++qz)
+#pragma unroll
+            for (int qy = 0; qy < N; ++qy)
+#pragma unroll
+              for (int qx = 0; qx < N; ++qx)
+                {
+                  const int q = (qz * N + qy) * N + qx;
+                  T         gt[3] = {T(0), T(0), T(0)}, gu[3] = {T(0), T(0), T(0)};
+#pragma unroll
+                  for (int k = 0; k < N; ++k)
+                    {
+                      const int qk[3] = {(qz * N + qy) * N + k, (qz * N + k) * N + qx, (k * N + qy) * N + qx};
+                      const T   dd[3] = {a.D[qx * N + k], a.D[qy * N + k], a.D[qz * N + k]};
+#pragma unroll
+                      for (int d = 0; d < 3; ++d)
+                        {
+                          gt[d] = fma(dd[d], tq[qk[d]], gt[d]);
+                          if constexpr (!RHS)
+                            gu[d] = fma(dd[d], uq[qk[d]], gu[d]);
+                        }
+                    }
+                  T k, dk;
+                  solid_conductivity(a.m, tq[q], k, dk);
+                  const T jw = a.det * a.w3[q];
+                  T       f[3];
+#pragma unroll
+                  for (int d = 0; d < 3; ++d)
+                    f[d] = RHS ? -jw * ih2[d] * k * gt[d] : jw * ih2[d] * (k * gu[d] + dk * gt[d] * uq[q]);
+#pragma unroll
+                  for (int k2 = 0; k2 < N; ++k2)
+                    {
+                      R[(qz * N + qy) * N + k2] = fma(a.D[qx * N + k2], f[0], R[(qz * N + qy) * N + k2]);
+                      R[(qz * N + k2) * N + qx] = fma(a.D[qy * N + k2], f[1], R[(qz * N + k2) * N + qx]);
+                      R[(k2 * N + qy) * N + qx] = fma(a.D[qz * N + k2], f[2], R[(k2 * N + qy) * N + qx]);
+                    }
+                }
           solid_sweep<T, N, 2, true>(R, a.B);
           solid_sweep<T, N, 1, true>(R, a.B);
           solid_sweep<T, N, 0, true>(R, a.B);

@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--case", default=None,
                     help="run one named case for profiling and exit: apply_<degree>_<cells>_<f64|f32>, "
                          "faces_<degree>_<cells>_<f64|f32>, supg_<degree>_<cells>_<f64|f32>, solid_<degree>_<cells>_<f64|f32>, "
-                         "(e.g. apply_2_128_f32) or solve_fp64 / solve_mixed (128^3 FE_Q(2) CG to 1e-8)")
+                         "(e.g. apply_2_128_f32), solve_fp64 / solve_mixed (128^3 FE_Q(2) CG to 1e-8), advection, adjoint")
     return ap.parse_args()
 
 
@@ -147,6 +147,8 @@ def run_case(name):
         print(json.dumps(out), flush=True)
     elif name == "advection":
         print(json.dumps({"case": name, **run_advection(torch, stream)}), flush=True)
+    elif name == "adjoint":
+        print(json.dumps({"case": name, **run_adjoint(torch, stream)}), flush=True)
     elif name in ("solve_fp64", "solve_mixed"):
         out = run_solves(torch, stream, modes=(name[6:],))
         print(json.dumps({"case": name, **out}), flush=True)

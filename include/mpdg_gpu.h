@@ -59,7 +59,10 @@ enum mpdg_status
 enum mpdg_op_kind
 {
   MPDG_HEAT    = 0, /* (rho c_p/dt) M + div(k grad), source/heat/heat_diffuse_operator.cpp      */
-  MPDG_ADVDIFF = 1  /* M/dt + theta (v.grad + eps K), source/level_set/advection_diffusion_operator.cpp */
+  MPDG_ADVDIFF = 1, /* M/dt + theta (v.grad + eps K), source/level_set/advection_diffusion_operator.cpp */
+  MPDG_REINIT  = 2  /* M/dt + div(D grad), D = eps_t I + (eps_n - eps_t) n n^T: conservative level-set
+                       reinitialisation, source/level_set/olsson_CG_operator.cpp (FE_Q(1, 2); set the
+                       normal field with mpdg_op_set_reinit) */
 };
 
 enum mpdg_solver_kind
@@ -201,6 +204,18 @@ MPDG_API int mpdg_op_set_heat_bc(mpdg_op *op, const mpdg_heat_bc *bc);
    create_rhs), tau_c = (coefficient < 0 ? 1 / max_q |v| (0 if below 1e-6) : coefficient) times the
    cell diameter / sqrt(3).  enabled = 0 switches it off (ConvectionStabilizationType::none). */
 MPDG_API int mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient);
+/* Reinitialisation operator (MPDG_REINIT; source/level_set/olsson_CG_operator.cpp, no wetting
+   boundary faces, no interface penalty): normal and tangential diffusion lengths (the reference's
+   normal_diffusion_length / tangential_diffusion_length, equal for all cells of a uniform mesh),
+   the normalisation tolerance (normalize divides by |n| above it and by the tolerance below,
+   include/meltpooldg/utilities/dealii_tensor.hpp:175-191) and the normal field: three DEVICE arrays
+   of n_dofs entries on the operator's lattice, read plainly and kept by reference.  vmult applies
+   dpsi/dt (mass) + eps_n (grad dpsi . n) n + eps_t (grad dpsi - (grad dpsi . n) n) (:438-470);
+   create_rhs(dst, psi_old) OVERWRITES dst with int [(1 - psi_old^2)/2 n - D grad psi_old] . grad phi
+   and zeroes the constrained rows (:197-260); the inverse diagonal uses the advection rule
+   (:357-436). */
+MPDG_API int mpdg_op_set_reinit(mpdg_op *op, double eps_normal, double eps_tangential, double normal_tolerance,
+                                const double *nx, const double *ny, const double *nz);
 /* The linearisation temperature of the radiation tangent and diagonal (the operator's const
    reference to the temperature vector, heat_diffuse_operator.hpp:121-135): a DEVICE array of
    n_dofs entries that the caller keeps alive and current; NULL detaches it.  vmult and the

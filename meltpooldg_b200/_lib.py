@@ -22,6 +22,7 @@ MPDG_ERR_NOMEM = 7
 
 MPDG_HEAT = 0
 MPDG_ADVDIFF = 1
+MPDG_REINIT = 2
 MPDG_CG = 0
 MPDG_GMRES = 1
 MPDG_PRECOND_IDENTITY = 0
@@ -155,6 +156,7 @@ SIGNATURES = [
     ("mpdg_op_set_heat_bc", [P, C.POINTER(HeatBC)], C.c_int),
     ("mpdg_vec_dot", [P, P, P, P], C.c_int),
     ("mpdg_op_set_supg", [P, C.c_int, D], C.c_int),
+    ("mpdg_op_set_reinit", [P, D, D, D, P, P, P], C.c_int),
     ("mpdg_op_distribute_constraints", [P, P, P], C.c_int),
     ("mpdg_vec_alloc", [P, C.POINTER(C.c_void_p)], C.c_int),
     ("mpdg_vec_free", [P], C.c_int),

@@ -90,6 +90,8 @@ struct mpdg_op
   const double *d_temp_old = nullptr; // T_old of the solidification tangent (not owned)
   long long     sync_cap = 0;         // brick flags allocated in d_sync (after the 3 counters)
   int           supg = 0;         // SUPG stabilisation (advection-diffusion)
+  double        eps_n = 0.0, eps_t = 0.0, ntol = 1e-16; // reinitialisation
+  const double *d_normal[3]{};                           // reinitialisation normal field (not owned)
   double        supg_coef = 0.0;
   const double *d_temp = nullptr; // linearisation temperature of the radiation tangent (not owned)
   int       brick[3]{}, nbr[3]{};
@@ -218,6 +220,29 @@ namespace
     return p;
   }
 
+  template <typename T>
+  ReinitLaunch<T>
+  reinit_launch(const mpdg_op *op, double scale, const T *src, T *dst, int mask_src)
+  {
+    ReinitLaunch<T> r;
+    r.degree           = op->degree;
+    r.scale            = scale;
+    r.dt               = op->dt;
+    r.eps_normal       = op->eps_n;
+    r.eps_tangential   = op->eps_t;
+    r.normal_tolerance = op->ntol;
+    for (int d = 0; d < 3; ++d)
+      {
+        r.hlen[d]   = op->h[d];
+        r.normal[d] = op->d_normal[d];
+      }
+    r.grid     = op->grid<T>();
+    r.src      = src;
+    r.dst      = dst;
+    r.mask_src = mask_src;
+    return r;
+  }
+
   // Temperature-dependent material: the tangent (rhs = false) or the residual part of create_rhs
   // (rhs = true, dst +=, src unused) with the operator's temperature and old temperature.  FP32
   // applies read FP32 copies of both.
@@ -322,6 +347,17 @@ namespace
             MPDG_CUDA(heat_faces<T>(f, op->stream));
           }
       }
+    else if (op->kind == MPDG_REINIT)
+      {
+        if (!op->d_normal[0] || !op->d_normal[1] || !op->d_normal[2])
+          return fail(MPDG_ERR_ARG, "the reinitialisation operator needs its normal field (mpdg_op_set_reinit)");
+        // dst prepared for the atomics of the cell kernel: 0 (Set) or b (BPlus); Add adds in place
+        if (mode == (int)OutMode::Set)
+          MPDG_CUDA(vec_fill<T>(dst, T(0), op->ndofs, op->stream));
+        else if (mode == (int)OutMode::BPlus && dst != b)
+          MPDG_CUDA(cudaMemcpyAsync(dst, b, sizeof(T) * op->ndofs, cudaMemcpyDeviceToDevice, op->stream));
+        MPDG_CUDA(reinit_integrate<T>(reinit_launch<T>(op, scale, src, dst, mask_src), 0, op->stream));
+      }
     else
       {
         AdvLaunch<T> h;
@@ -387,6 +423,24 @@ namespace
       }
     else
       {
+        if (op->kind == MPDG_REINIT)
+          {
+            if (!op->d_normal[0] || !op->d_normal[1] || !op->d_normal[2])
+              return fail(MPDG_ERR_ARG, "the reinitialisation operator needs its normal field (mpdg_op_set_reinit)");
+            double *r64 = std::is_same<T, double>::value ? reinterpret_cast<double *>(diag) : op->vec<double>("reinit_diag");
+            if (!r64)
+              return fail(MPDG_ERR_NOMEM, "diagonal work vector");
+            MPDG_CUDA(vec_fill<double>(r64, 0.0, op->ndofs, op->stream));
+            ReinitLaunch<double> r = reinit_launch<double>(op, 1.0, nullptr, nullptr, 0);
+            r.diag                 = r64;
+            MPDG_CUDA(reinit_integrate<double>(r, 2, op->stream));
+            MPDG_CUDA(vec_set_constrained<double>(r64, 1.0, g, op->stream));
+            MPDG_CUDA(vec_absmax<double>(r64, op->ndofs, op->d_scal, op->reducer(), op->stream));
+            MPDG_CUDA(vec_invert_rel<double>(r64, op->d_scal, op->ndofs, op->stream));
+            if (!std::is_same<T, double>::value)
+              MPDG_CUDA(vec_convert<T, double>(diag, r64, op->ndofs, op->stream));
+            return MPDG_OK;
+          }
         // the SUPG part sums terms of both signs: an FP32 diagonal is computed in FP64 and rounded once
         double *d64 = std::is_same<T, double>::value ? reinterpret_cast<double *>(diag)
                                                      : (op->supg ? op->vec<double>("supg_diag") : nullptr);
@@ -699,8 +753,10 @@ mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op
   if (!mesh || !params || !out)
     return fail(MPDG_ERR_ARG, "null argument to mpdg_op_create");
   *out = nullptr;
-  if (params->kind != MPDG_HEAT && params->kind != MPDG_ADVDIFF)
+  if (params->kind != MPDG_HEAT && params->kind != MPDG_ADVDIFF && params->kind != MPDG_REINIT)
     return fail(MPDG_ERR_ARG, "unknown operator kind");
+  if (params->kind == MPDG_REINIT && (mesh->degree < 1 || mesh->degree > 2))
+    return fail(MPDG_ERR_UNSUPPORTED, "reinitialisation operator: FE_Q degree must be 1..2");
   if (params->kind == MPDG_HEAT && (mesh->degree < 1 || mesh->degree > 4))
     return fail(MPDG_ERR_UNSUPPORTED, "heat operator: FE_Q degree must be 1..4");
   if (params->kind == MPDG_ADVDIFF && (mesh->degree < 1 || mesh->degree > 2))
@@ -982,6 +1038,25 @@ mpdg_op_set_old_temperature(mpdg_op *op, const double *temperature_old)
 }
 
 int
+mpdg_op_set_reinit(mpdg_op *op, double eps_normal, double eps_tangential, double normal_tolerance, const double *nx,
+                   const double *ny, const double *nz)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_REINIT)
+    return fail(MPDG_ERR_ARG, "mpdg_op_set_reinit applies to the reinitialisation operator");
+  if (!(eps_normal >= 0.0) || !(eps_tangential >= 0.0) || !(normal_tolerance > 0.0) || !nx || !ny || !nz)
+    return fail(MPDG_ERR_ARG, "diffusion lengths >= 0, a positive tolerance and three normal components");
+  op->eps_n       = eps_normal;
+  op->eps_t       = eps_tangential;
+  op->ntol        = normal_tolerance;
+  op->d_normal[0] = nx;
+  op->d_normal[1] = ny;
+  op->d_normal[2] = nz;
+  return MPDG_OK;
+}
+
+int
 mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient)
 {
   if (int e = check_op(op))
@@ -1172,6 +1247,15 @@ mpdg_op_create_rhs(mpdg_op *op, double *dst, const double *a, const double *b, c
     return fail(MPDG_ERR_ZERO_DT, "time increment must be positive (ExcZeroTimeIncrement)");
   if (!dst || !a)
     return fail(MPDG_ERR_ARG, "create_rhs needs dst and its first input");
+  if (op->kind == MPDG_REINIT)
+    {
+      // olsson_CG_operator.cpp:197-260: dst is overwritten, constrained rows end at 0
+      if (!op->d_normal[0] || !op->d_normal[1] || !op->d_normal[2])
+        return fail(MPDG_ERR_ARG, "the reinitialisation operator needs its normal field (mpdg_op_set_reinit)");
+      MPDG_CUDA(vec_fill<double>(dst, 0.0, op->ndofs, op->stream));
+      MPDG_CUDA(reinit_integrate<double>(reinit_launch<double>(op, 1.0, a, dst, 0), 1, op->stream));
+      return MPDG_OK;
+    }
   if (op->kind == MPDG_HEAT && op->solid)
     {
       // dst += M q - int rho c_p(T) (T - T_old) / dt phi - int k(T) grad T . grad phi (+ faces)

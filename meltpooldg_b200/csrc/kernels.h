@@ -113,6 +113,25 @@ namespace mpdg
   cudaError_t heat_solid_diagonal(const GridDesc &g, int K, const SolidMaterial &mat, double dt, const double hlen[3],
                                   const double *temp, const double *temp_old, double *diag, cudaStream_t s);
 
+  // ---- conservative level-set reinitialisation (Olsson, reinit.cu), FE_Q(1, 2)
+  template <typename T>
+  struct ReinitLaunch
+  {
+    int           degree = 1;
+    double        scale = 1.0, dt = 1.0, eps_normal = 0.0, eps_tangential = 0.0, normal_tolerance = 1e-16;
+    double        hlen[3]{};
+    GridDesc      grid{};
+    const T      *src = nullptr;
+    const double *normal[3]{};
+    T            *dst  = nullptr;
+    double       *diag = nullptr;
+    int           mask_src = 1;
+  };
+  // mode 0: dst += scale * A src on free rows; 1: dst += the rhs integrand of psi_old = src (plain);
+  // 2: diag += the tangent's diagonal on free rows
+  template <typename T>
+  cudaError_t reinit_integrate(const ReinitLaunch<T> &h, int mode, cudaStream_t s);
+
   // whether mode (0 tangent / 2 diagonal, 1 rhs) has any face to integrate
   bool heat_faces_active(const HeatFaceBC &bc, int mode);
 

@@ -240,6 +240,25 @@ class AdvectionDiffusionOperator(OperatorMatrixFree):
         check(lib().mpdg_op_set_supg(self._h, 1 if type == "SUPG" else 0, float(coefficient)))
 
 
+class OlssonOperator(OperatorMatrixFree):
+    """Conservative level-set reinitialisation operator (source/level_set/olsson_CG_operator.cpp):
+    M/dt + div(D grad), D = eps_t I + (eps_n - eps_t) n n^T with the unit normal of a normal field."""
+
+    def __init__(self, mesh: Mesh, dt: float, eps_normal: float, eps_tangential: float,
+                 normal_tolerance: float = 1e-16, stream=None):
+        p = L.OpParams()
+        p.kind = L.MPDG_REINIT
+        p.dt = float(dt)
+        super().__init__(mesh, p, stream)
+        self.eps_normal, self.eps_tangential, self.normal_tolerance = eps_normal, eps_tangential, normal_tolerance
+
+    def set_normal(self, nx, ny, nz) -> None:
+        """Normal field (three device vectors on the lattice, kept by reference)."""
+        self._normal = (nx, ny, nz)
+        check(lib().mpdg_op_set_reinit(self._h, float(self.eps_normal), float(self.eps_tangential),
+                                       float(self.normal_tolerance), _ptr(nx), _ptr(ny), _ptr(nz)))
+
+
 @dataclass
 class LinearSolverData:
     """include/meltpooldg/linear_algebra/linear_solver_data.hpp:37-47 (defaults preserved)."""

@@ -1,0 +1,90 @@
+"""Conservative level-set reinitialisation operator (Olsson) -- CPU oracle.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/ as the checker of the GPU reinitialisation kernels,
+never by the product path.
+
+Restates source/level_set/olsson_CG_operator.cpp in its default configuration (no wetting boundary
+faces, no interface penalty):
+* tangent (:438-470): dpsi / dt tested with phi, eps_n (grad dpsi . n) n + eps_t (grad dpsi -
+  (grad dpsi . n) n) tested with grad phi; dpsi with Dirichlet entries 0;
+* rhs (:197-260): [c(psi) n - eps_n (grad psi . n) n - eps_t (grad psi - (grad psi . n) n)] tested
+  with grad phi, c(psi) = (1 - psi^2) / 2 (:24-29), psi read plainly, dst overwritten, constrained
+  rows 0;
+* n = normalize(n_h, tol): n_h / |n_h| above tol, n_h / tol otherwise
+  (include/meltpooldg/utilities/dealii_tensor.hpp:175-191); n_h read plainly.
+Per cell with QGauss(k+1), vectorised over the cells with numpy.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle.oracle import Mesh
+from oracle.supg import _cells, _dof_index, tables
+
+
+def _setup(mesh: Mesh, cmask, normal, tol):
+    qp, qw, B, G, _ = tables(mesh.degree)
+    h = [mesh.length[d] / mesh.m[d] for d in range(3)]
+    free = np.ones(mesh.ndofs, bool) if cmask is None else np.asarray(cmask) == 0
+    cx, cy, cz = _cells(mesh)
+    idx = _dof_index(mesh, cx, cy, cz)
+    ev = lambda Z, Y, X, f: np.einsum("al,bj,ci,xlji->xabc", Z, Y, X, f)  # noqa: E731
+    nq = [ev(B, B, B, np.asarray(c, dtype=np.float64)[idx]) for c in normal]
+    norm = np.sqrt(nq[0] ** 2 + nq[1] ** 2 + nq[2] ** 2)
+    inv = np.where(norm > tol, 1.0 / np.where(norm > 0, norm, 1.0), 1.0 / tol)
+    n = [c * inv for c in nq]
+    W = h[0] * h[1] * h[2] * np.einsum("a,b,c->abc", qw, qw, qw)[None]
+    return B, G, h, idx, free, n, W, ev
+
+
+def _grad(ev, B, G, h, c):
+    return [ev(B, B, G, c) / h[0], ev(B, G, B, c) / h[1], ev(G, B, B, c) / h[2]]
+
+
+def _scatter(mesh, B, G, h, idx, free, val, flux):
+    te = lambda Z, Y, X, F: np.einsum("al,bj,ci,xabc->xlji", Z, Y, X, F)  # noqa: E731
+    loc = te(B, B, G, flux[0]) / h[0] + te(B, G, B, flux[1]) / h[1] + te(G, B, B, flux[2]) / h[2]
+    if val is not None:
+        loc = loc + te(B, B, B, val)
+    out = np.zeros(mesh.ndofs)
+    keep = free[idx]
+    np.add.at(out, idx[keep], loc[keep])
+    return out
+
+
+def tangent_apply(mesh: Mesh, cmask, dt, eps_n, eps_t, normal, tol, u) -> np.ndarray:
+    B, G, h, idx, free, n, W, ev = _setup(mesh, cmask, normal, tol)
+    uc = np.where(free, u, 0.0)[idx]
+    uq = ev(B, B, B, uc)
+    g = _grad(ev, B, G, h, uc)
+    gn = g[0] * n[0] + g[1] * n[1] + g[2] * n[2]
+    flux = [W * (eps_t * g[d] + (eps_n - eps_t) * gn * n[d]) for d in range(3)]
+    return _scatter(mesh, B, G, h, idx, free, W * uq / dt, flux)
+
+
+def create_rhs(mesh: Mesh, cmask, eps_n, eps_t, normal, tol, psi_old) -> np.ndarray:
+    B, G, h, idx, free, n, W, ev = _setup(mesh, cmask, normal, tol)
+    pc = np.asarray(psi_old, dtype=np.float64)[idx]
+    pq = ev(B, B, B, pc)
+    g = _grad(ev, B, G, h, pc)
+    gn = g[0] * n[0] + g[1] * n[1] + g[2] * n[2]
+    cf = 0.5 * (1.0 - pq * pq)
+    flux = [W * (cf * n[d] - eps_t * g[d] - (eps_n - eps_t) * gn * n[d]) for d in range(3)]
+    return _scatter(mesh, B, G, h, idx, free, None, flux)
+
+
+def diagonal(mesh: Mesh, cmask, dt, eps_n, eps_t, normal, tol) -> np.ndarray:
+    """Diagonal of the tangent (0 on constrained rows)."""
+    B, G, h, idx, free, n, W, ev = _setup(mesh, cmask, normal, tol)
+    o = lambda Z, Y, X: np.einsum("al,bj,ci->abclji", Z, Y, X)[None]  # noqa: E731
+    phi = o(B, B, B)
+    dphi = [o(B, B, G) / h[0], o(B, G, B) / h[1], o(G, B, B) / h[2]]
+    e = lambda a: a[..., None, None, None]  # noqa: E731
+    pn = sum(e(n[d]) * dphi[d] for d in range(3))
+    pp = sum(dp * dp for dp in dphi)
+    term = e(W / dt) * phi * phi + e(W) * (eps_t * pp + (eps_n - eps_t) * pn * pn)
+    loc = term.sum(axis=(1, 2, 3))
+    out = np.zeros(mesh.ndofs)
+    keep = free[idx]
+    np.add.at(out, idx[keep], loc[keep])
+    return out

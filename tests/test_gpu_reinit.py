@@ -1,0 +1,97 @@
+"""Conservative level-set reinitialisation operator (Olsson) on the GPU against oracle/reinit.py,
+through the C ABI: vmult (FP64, FP32), create_rhs (overwriting), the inverse diagonal, a CG solve
+and the argument checks."""
+import numpy as np
+import pytest
+
+from meltpooldg_b200.inputs import uniform_dofs
+from oracle.reinit import create_rhs, diagonal, tangent_apply
+from tests.gpu_util import meshes, rel_err, to_gpu
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(1, (9, 7, 5), 0b000001), (2, (9, 8, 5), 0b010011), (2, (16, 16, 16), 0), (1, (17, 5, 3), 0)]
+EPS_N, EPS_T, DT, TOL = 0.05, 0.01, 1e-2, 1e-3
+
+
+def setup(degree, m, faces):
+    from meltpooldg_b200.operators import OlssonOperator
+
+    om, gm, cm = meshes(degree, m, faces=faces, length=(1.0, 0.9, 1.1))
+    X, Y, Z = om.coords()
+    # radial normal field through the domain (zero length at its centre: the tolerance branch)
+    normal = [X - 0.5, Y - 0.45, Z - 0.55]
+    g = OlssonOperator(gm, dt=DT, eps_normal=EPS_N, eps_tangential=EPS_T, normal_tolerance=TOL)
+    nd = [to_gpu(c) for c in normal]
+    g.set_normal(*nd)
+    return g, om, cm, normal, nd
+
+
+@pytest.mark.parametrize("degree,m,faces", CASES)
+def test_reinit_vmult_matches_oracle(degree, m, faces):
+    import torch
+
+    g, om, cm, normal, keep = setup(degree, m, faces)
+    x = uniform_dofs(om, seed=1)
+    ref = tangent_apply(om, cm, DT, EPS_N, EPS_T, normal, TOL, x)
+    xd = to_gpu(x)
+    yd = torch.full_like(xd, np.nan)
+    g.vmult(yd, xd)
+    assert rel_err(yd.cpu().numpy(), ref) <= 1e-12
+    y32 = torch.empty(om.ndofs, dtype=torch.float32, device="cuda")
+    g.vmult(y32, to_gpu(x, torch.float32))
+    assert rel_err(y32.cpu().numpy(), ref) <= 2e-6
+
+
+@pytest.mark.parametrize("degree,m,faces", CASES)
+def test_reinit_create_rhs_and_diagonal(degree, m, faces):
+    import torch
+
+    g, om, cm, normal, keep = setup(degree, m, faces)
+    psi = np.tanh(4.0 * uniform_dofs(om, seed=3))
+    ref = create_rhs(om, cm, EPS_N, EPS_T, normal, TOL, psi)
+    dst = to_gpu(uniform_dofs(om, seed=4))  # overwritten
+    g.create_rhs(dst, to_gpu(psi))
+    assert rel_err(dst.cpu().numpy(), ref) <= 1e-12
+    d = diagonal(om, cm, DT, EPS_N, EPS_T, normal, TOL)
+    if cm is not None:
+        d[cm != 0] = 1.0
+    linf = max(1.0, np.max(np.abs(d)))
+    inv = np.where(np.abs(d) > 1e-14 * linf, 1.0 / d, 1.0)
+    dd = torch.empty(om.ndofs, dtype=torch.float64, device="cuda")
+    g.compute_inverse_diagonal_from_matrixfree(dd)
+    assert rel_err(dd.cpu().numpy(), inv) <= 1e-12
+
+
+def test_reinit_cg_reaches_the_oracle_residual():
+    import torch
+
+    from meltpooldg_b200.operators import LinearSolver, LinearSolverData
+
+    g, om, cm, normal, keep = setup(2, (12, 10, 9), 0b010011)
+    b = uniform_dofs(om, seed=9)
+    b[cm != 0] = 0.0
+    x = torch.zeros(om.ndofs, dtype=torch.float64, device="cuda")
+    LinearSolver.solve(g, x, to_gpu(b), LinearSolverData("CG", "Diagonal", max_iterations=2000, rel_tolerance=1e-10))
+    xs = x.cpu().numpy()
+    r = b - tangent_apply(om, cm, DT, EPS_N, EPS_T, normal, TOL, xs)
+    assert np.linalg.norm(r) <= 2e-10 * np.linalg.norm(b)
+
+
+def test_reinit_argument_checks():
+    import torch
+
+    from meltpooldg_b200._lib import MPDG_ERR_ARG, MPDG_ERR_UNSUPPORTED, MpdgError
+    from meltpooldg_b200.operators import Mesh, OlssonOperator
+
+    with pytest.raises(MpdgError) as e:
+        OlssonOperator(Mesh(3, (2, 2, 2)), dt=1e-2, eps_normal=0.1, eps_tangential=0.1)
+    assert e.value.code == MPDG_ERR_UNSUPPORTED
+    g = OlssonOperator(Mesh(1, (4, 4, 4)), dt=1e-2, eps_normal=0.1, eps_tangential=0.1)
+    x = torch.zeros(g.n_dofs, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    with pytest.raises(MpdgError) as e:
+        g.vmult(y, x)  # no normal field yet
+    assert e.value.code == MPDG_ERR_ARG
+    g.set_normal(x + 1.0, x, x)
+    g.vmult(y, x)

@@ -269,6 +269,37 @@ namespace mpdg
                                const double velocity[12])
       : OperatorMatrixFree(mesh, params(dt, theta, diffusivity, velocity))
     {}
+    // AdvectionDiffusionData::conv_stab (type SUPG or none, coefficient < 0: h_c / max |v|)
+    void
+    set_convection_stabilization(bool supg, double coefficient)
+    {
+      check(mpdg_op_set_supg(handle(), supg ? 1 : 0, coefficient));
+    }
+  };
+
+  // OlssonOperator (source/level_set/olsson_CG_operator.cpp), default configuration: create_rhs
+  // overwrites dst (create_rhs(dst, psi_old)); the normal field is three device arrays kept by
+  // reference
+  class OlssonOperator : public OperatorMatrixFree
+  {
+  public:
+    static mpdg_op_params
+    params(double dt)
+    {
+      mpdg_op_params p{};
+      p.kind = MPDG_REINIT;
+      p.dt   = dt;
+      return p;
+    }
+    OlssonOperator(const mpdg_mesh_desc &mesh, double dt)
+      : OperatorMatrixFree(mesh, params(dt))
+    {}
+    void
+    set_normal(double eps_normal, double eps_tangential, double normal_tolerance, const double *nx, const double *ny,
+               const double *nz)
+    {
+      check(mpdg_op_set_reinit(handle(), eps_normal, eps_tangential, normal_tolerance, nx, ny, nz));
+    }
   };
 
   // ---- linear solver -----------------------------------------------------------------------------

@@ -216,6 +216,21 @@ MPDG_API int mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient);
    (:357-436). */
 MPDG_API int mpdg_op_set_reinit(mpdg_op *op, double eps_normal, double eps_tangential, double normal_tolerance,
                                 const double *nx, const double *ny, const double *nz);
+
+/* Right-hand sides of the level set's projections, FE_Q(1, 2), on the lattice and constraint set of
+   op (any kind; the projection itself is M + damping K, a heat operator with rho_cp = dt = 1 and
+   conductivity = the reference's cell-size-dependent damping, solved per component), no narrow band:
+   - NormalVectorOperator::create_rhs (source/level_set/normal_vector_operator.cpp:160-240):
+     n_d += int (grad psi)_d phi, or the gradient normalised (|.| > 1e-16, else divided by 1e-16) when
+     normalized != 0; accumulating, psi read plainly;
+   - CurvatureOperator::create_rhs (source/level_set/curvature_operator.cpp:190-255):
+     dst = -int div(n) phi with n = normalize(n_i, normal_tolerance) applied to every DoF value of
+     the normal field first; dst overwritten.
+   Constrained rows are not written (stay 0 in the curvature rhs). */
+MPDG_API int mpdg_level_set_normal_rhs(mpdg_op *op, const double *psi, int normalized, double *nx, double *ny,
+                                       double *nz);
+MPDG_API int mpdg_level_set_curvature_rhs(mpdg_op *op, const double *nx, const double *ny, const double *nz,
+                                          double normal_tolerance, double *dst);
 /* The linearisation temperature of the radiation tangent and diagonal (the operator's const
    reference to the temperature vector, heat_diffuse_operator.hpp:121-135): a DEVICE array of
    n_dofs entries that the caller keeps alive and current; NULL detaches it.  vmult and the

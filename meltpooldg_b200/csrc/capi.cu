@@ -1057,6 +1057,36 @@ mpdg_op_set_reinit(mpdg_op *op, double eps_normal, double eps_tangential, double
 }
 
 int
+mpdg_level_set_normal_rhs(mpdg_op *op, const double *psi, int normalized, double *nx, double *ny, double *nz)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!psi || !nx || !ny || !nz)
+    return fail(MPDG_ERR_ARG, "null argument to mpdg_level_set_normal_rhs");
+  if (op->degree > 2)
+    return fail(MPDG_ERR_UNSUPPORTED, "the level-set right-hand sides support FE_Q degree 1..2");
+  MPDG_CUDA(level_set_rhs(op->grid(), op->degree, op->h, 0, normalized ? 1 : 0, 0.0, psi, nullptr, nullptr, nx, ny,
+                          nz, op->stream));
+  return MPDG_OK;
+}
+
+int
+mpdg_level_set_curvature_rhs(mpdg_op *op, const double *nx, const double *ny, const double *nz, double normal_tolerance,
+                             double *dst)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!nx || !ny || !nz || !dst || !(normal_tolerance > 0.0))
+    return fail(MPDG_ERR_ARG, "invalid argument to mpdg_level_set_curvature_rhs");
+  if (op->degree > 2)
+    return fail(MPDG_ERR_UNSUPPORTED, "the level-set right-hand sides support FE_Q degree 1..2");
+  MPDG_CUDA(vec_fill<double>(dst, 0.0, op->ndofs, op->stream));
+  MPDG_CUDA(level_set_rhs(op->grid(), op->degree, op->h, 1, 0, normal_tolerance, nx, ny, nz, dst, nullptr, nullptr,
+                          op->stream));
+  return MPDG_OK;
+}
+
+int
 mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient)
 {
   if (int e = check_op(op))

@@ -131,6 +131,11 @@ namespace mpdg
   // 2: diag += the tangent's diagonal on free rows
   template <typename T>
   cudaError_t reinit_integrate(const ReinitLaunch<T> &h, int mode, cudaStream_t s);
+  // normal-vector (mode 0: out_d += int grad_d psi phi, normalised on request) and curvature (mode 1:
+  // out0 += -int div(normalize(n_i, tol)) phi) right-hand sides, FE_Q(1, 2), free rows only
+  cudaError_t level_set_rhs(const GridDesc &g, int K, const double hlen[3], int mode, int normalized, double tol,
+                            const double *in0, const double *in1, const double *in2, double *out0, double *out1,
+                            double *out2, cudaStream_t s);
 
   // whether mode (0 tangent / 2 diagonal, 1 rhs) has any face to integrate
   bool heat_faces_active(const HeatFaceBC &bc, int mode);

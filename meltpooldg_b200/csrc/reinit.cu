@@ -203,6 +203,173 @@ namespace mpdg
     }
   } // namespace
 
+  namespace
+  {
+    // Right-hand sides of the normal-vector and curvature projections (one thread per cell):
+    //   mode 0: dst_d += int g_d phi, g = grad psi, or normalize(grad psi, 1e-16) when normalized
+    //           (normal_vector_operator.cpp:160-240, no narrow band)
+    //   mode 1: dst   += -int div(n) phi with n = normalize(n_i, tol) at every DoF
+    //           (curvature_operator.cpp:190-255, no narrow band)
+    template <int K>
+    __global__ void __launch_bounds__(128)
+    level_set_rhs_kernel(const GridDesc g, const double *B, const double *G, const double *w, double det, double ihx,
+                         double ihy, double ihz, int mode, int normalized, double tol, const double *in0,
+                         const double *in1, const double *in2, double *out0, double *out1, double *out2)
+    {
+      constexpr int   N = K + 1, N3 = N * N * N;
+      const double    ih[3] = {ihx, ihy, ihz};
+      const int       m0 = g.m[0], m1 = g.m[1];
+      const long long ncell = (long long)m0 * m1 * g.m[2];
+      for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
+        {
+          const int cx = (int)(c % m0), cy = (int)((c / m0) % m1), cz = (int)(c / ((long long)m0 * m1));
+          long long idx[N3];
+          bool      con[N3];
+          double    v[3][N3], R[3][N3];
+#pragma unroll
+          for (int l = 0; l < N; ++l)
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+#pragma unroll
+              for (int i = 0; i < N; ++i)
+                {
+                  const int       q = (l * N + j) * N + i;
+                  const int       I = K * cx + i, J = K * cy + j, L = K * cz + l;
+                  const long long id = (long long)I + (long long)g.n[0] * ((long long)J + (long long)g.n[1] * L);
+                  idx[q]            = id;
+                  con[q]            = is_constrained(g, I, J, L, id);
+                  if (mode == 0)
+                    v[0][q] = in0[id];
+                  else
+                    {
+                      const double a = in0[id], b = in1[id], e = in2[id];
+                      const double nn = sqrt(a * a + b * b + e * e), s = nn > tol ? 1.0 / nn : 1.0 / tol;
+                      v[0][q] = a * s, v[1][q] = b * s, v[2][q] = e * s;
+                    }
+#pragma unroll
+                  for (int d = 0; d < 3; ++d)
+                    R[d][q] = 0.0;
+                }
+          for (int qz = 0; qz < N; ++qz)
+            for (int qy = 0; qy < N; ++qy)
+              for (int qx = 0; qx < N; ++qx)
+                {
+                  double gv[3] = {0.0, 0.0, 0.0}, div = 0.0;
+#pragma unroll
+                  for (int l = 0; l < N; ++l)
+#pragma unroll
+                    for (int j = 0; j < N; ++j)
+#pragma unroll
+                      for (int i = 0; i < N; ++i)
+                        {
+                          const int    q  = (l * N + j) * N + i;
+                          const double bx = B[qx * N + i], by = B[qy * N + j], bz = B[qz * N + l];
+                          const double p[3] = {G[qx * N + i] * ih[0] * by * bz, bx * G[qy * N + j] * ih[1] * bz,
+                                               bx * by * G[qz * N + l] * ih[2]};
+                          if (mode == 0)
+                            {
+#pragma unroll
+                              for (int d = 0; d < 3; ++d)
+                                gv[d] += p[d] * v[0][q];
+                            }
+                          else
+                            div += p[0] * v[0][q] + p[1] * v[1][q] + p[2] * v[2][q];
+                        }
+                  if (mode == 0 && normalized)
+                    {
+                      const double nn = sqrt(gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2]);
+                      const double s  = nn > 1e-16 ? 1.0 / nn : 1e16;
+#pragma unroll
+                      for (int d = 0; d < 3; ++d)
+                        gv[d] *= s;
+                    }
+                  const double jw = det * w[qx] * w[qy] * w[qz];
+#pragma unroll
+                  for (int l = 0; l < N; ++l)
+#pragma unroll
+                    for (int j = 0; j < N; ++j)
+#pragma unroll
+                      for (int i = 0; i < N; ++i)
+                        {
+                          const double phi = B[qx * N + i] * B[qy * N + j] * B[qz * N + l] * jw;
+                          if (mode == 0)
+                            {
+#pragma unroll
+                              for (int d = 0; d < 3; ++d)
+                                R[d][(l * N + j) * N + i] += gv[d] * phi;
+                            }
+                          else
+                            R[0][(l * N + j) * N + i] -= div * phi;
+                        }
+                }
+#pragma unroll
+          for (int q = 0; q < N3; ++q)
+            if (!con[q])
+              {
+                atomicAdd(out0 + idx[q], R[0][q]);
+                if (mode == 0)
+                  {
+                    atomicAdd(out1 + idx[q], R[1][q]);
+                    atomicAdd(out2 + idx[q], R[2][q]);
+                  }
+              }
+        }
+    }
+
+    // 1-D tables of degree K in device memory for the level-set rhs kernels (uploaded once per device)
+    const double *
+    level_set_tables(int K)
+    {
+      static double *dev[8][3] = {}; // [device][degree]
+      int            d         = 0;
+      if (cudaGetDevice(&d) != cudaSuccess || d >= 8)
+        return nullptr;
+      if (!dev[d][K])
+        {
+          const Tables1D &t = tables(K);
+          const int       n = t.n;
+          double          h[3 * MAX_N * MAX_N]{};
+          for (int i = 0; i < n * n; ++i)
+            {
+              h[i]         = t.B[i];
+              h[n * n + i] = t.G[i];
+            }
+          for (int q = 0; q < n; ++q)
+            h[2 * n * n + q] = t.qw[q];
+          double *p = nullptr;
+          if (cudaMalloc(&p, sizeof(h)) != cudaSuccess || cudaMemcpy(p, h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess)
+            return nullptr;
+          dev[d][K] = p;
+        }
+      return dev[d][K];
+    }
+  } // namespace
+
+  cudaError_t
+  level_set_rhs(const GridDesc &g, int K, const double hlen[3], int mode, int normalized, double tol,
+                const double *in0, const double *in1, const double *in2, double *out0, double *out1, double *out2,
+                cudaStream_t s)
+  {
+    if (K < 1 || K > 2)
+      return cudaErrorInvalidValue;
+    const double *tab = level_set_tables(K);
+    if (!tab)
+      return cudaErrorMemoryAllocation;
+    const int       n      = K + 1;
+    const long long ncell  = (long long)g.m[0] * g.m[1] * g.m[2];
+    const int       blocks = (int)std::max<long long>(1, std::min<long long>((ncell + 127) / 128, 148LL * 16));
+    const double    det    = hlen[0] * hlen[1] * hlen[2];
+    if (K == 1)
+      level_set_rhs_kernel<1><<<blocks, 128, 0, s>>>(g, tab, tab + n * n, tab + 2 * n * n, det, 1.0 / hlen[0],
+                                                      1.0 / hlen[1], 1.0 / hlen[2], mode, normalized, tol, in0, in1,
+                                                      in2, out0, out1, out2);
+    else
+      level_set_rhs_kernel<2><<<blocks, 128, 0, s>>>(g, tab, tab + n * n, tab + 2 * n * n, det, 1.0 / hlen[0],
+                                                      1.0 / hlen[1], 1.0 / hlen[2], mode, normalized, tol, in0, in1,
+                                                      in2, out0, out1, out2);
+    return cudaGetLastError();
+  }
+
   template <typename T>
   cudaError_t
   reinit_integrate(const ReinitLaunch<T> &h, int mode, cudaStream_t s)

@@ -156,6 +156,15 @@ class OperatorMatrixFree:
         check(lib().mpdg_op_create_rhs_and_apply_dirichlet(self._h, _ptr(rhs), _ptr(a), _ptr(b), _ptr(c),
                                                           _ptr(dirichlet_values), 1 if zero_out else 0))
 
+    def level_set_normal_rhs(self, psi, nx, ny, nz, normalized: bool = False) -> None:
+        """NormalVectorOperator::create_rhs on this operator's lattice: n_d += int (grad psi)_d phi."""
+        check(lib().mpdg_level_set_normal_rhs(self._h, _ptr(psi), 1 if normalized else 0, _ptr(nx), _ptr(ny), _ptr(nz)))
+
+    def level_set_curvature_rhs(self, dst, nx, ny, nz, normal_tolerance: float) -> None:
+        """CurvatureOperator::create_rhs on this operator's lattice: dst = -int div(n) phi."""
+        check(lib().mpdg_level_set_curvature_rhs(self._h, _ptr(nx), _ptr(ny), _ptr(nz), float(normal_tolerance),
+                                                 _ptr(dst)))
+
     def device_errors(self) -> int:
         return lib().mpdg_op_device_errors(self._h)
 

@@ -88,3 +88,51 @@ def diagonal(mesh: Mesh, cmask, dt, eps_n, eps_t, normal, tol) -> np.ndarray:
     keep = free[idx]
     np.add.at(out, idx[keep], loc[keep])
     return out
+
+
+def normal_rhs(mesh: Mesh, cmask, psi, normalized: bool = False):
+    """NormalVectorOperator::create_rhs (source/level_set/normal_vector_operator.cpp:160-240, no
+    narrow band): int g_d phi with g = grad psi, or g normalised (divided by 1e-16 at or below it)."""
+    qp, qw, B, G, _ = tables(mesh.degree)
+    h = [mesh.length[d] / mesh.m[d] for d in range(3)]
+    free = np.ones(mesh.ndofs, bool) if cmask is None else np.asarray(cmask) == 0
+    cx, cy, cz = _cells(mesh)
+    idx = _dof_index(mesh, cx, cy, cz)
+    ev = lambda Z, Y, X, f: np.einsum("al,bj,ci,xlji->xabc", Z, Y, X, f)  # noqa: E731
+    pc = np.asarray(psi, dtype=np.float64)[idx]
+    g = _grad(ev, B, G, h, pc)
+    if normalized:
+        nn = np.sqrt(g[0] ** 2 + g[1] ** 2 + g[2] ** 2)
+        s = np.where(nn > 1e-16, 1.0 / np.where(nn > 0, nn, 1.0), 1e16)
+        g = [c * s for c in g]
+    W = h[0] * h[1] * h[2] * np.einsum("a,b,c->abc", qw, qw, qw)[None]
+    te = lambda Z, Y, X, F: np.einsum("al,bj,ci,xabc->xlji", Z, Y, X, F)  # noqa: E731
+    out = []
+    for d in range(3):
+        o = np.zeros(mesh.ndofs)
+        keep = free[idx]
+        np.add.at(o, idx[keep], te(B, B, B, W * g[d])[keep])
+        out.append(o)
+    return out
+
+
+def curvature_rhs(mesh: Mesh, cmask, normal, tol):
+    """CurvatureOperator::create_rhs (source/level_set/curvature_operator.cpp:190-255, no narrow
+    band): -int div(n) phi with n = normalize(n_i, tol) at every DoF; constrained rows 0."""
+    qp, qw, B, G, _ = tables(mesh.degree)
+    h = [mesh.length[d] / mesh.m[d] for d in range(3)]
+    free = np.ones(mesh.ndofs, bool) if cmask is None else np.asarray(cmask) == 0
+    cx, cy, cz = _cells(mesh)
+    idx = _dof_index(mesh, cx, cy, cz)
+    nv = [np.asarray(c, dtype=np.float64) for c in normal]
+    nn = np.sqrt(nv[0] ** 2 + nv[1] ** 2 + nv[2] ** 2)
+    s = np.where(nn > tol, 1.0 / np.where(nn > 0, nn, 1.0), 1.0 / tol)
+    nv = [c * s for c in nv]
+    ev = lambda Z, Y, X, f: np.einsum("al,bj,ci,xlji->xabc", Z, Y, X, f)  # noqa: E731
+    div = (ev(B, B, G, nv[0][idx]) / h[0] + ev(B, G, B, nv[1][idx]) / h[1] + ev(G, B, B, nv[2][idx]) / h[2])
+    W = h[0] * h[1] * h[2] * np.einsum("a,b,c->abc", qw, qw, qw)[None]
+    te = lambda Z, Y, X, F: np.einsum("al,bj,ci,xabc->xlji", Z, Y, X, F)  # noqa: E731
+    out = np.zeros(mesh.ndofs)
+    keep = free[idx]
+    np.add.at(out, idx[keep], te(B, B, B, -W * div)[keep])
+    return out

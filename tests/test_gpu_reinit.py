@@ -95,3 +95,47 @@ def test_reinit_argument_checks():
     assert e.value.code == MPDG_ERR_ARG
     g.set_normal(x + 1.0, x, x)
     g.vmult(y, x)
+
+
+@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0), (2, (9, 8, 5), 0b010011), (2, (16, 16, 16), 0)])
+def test_level_set_rhs_and_normal_projection(degree, m, faces):
+    """The normal-vector and curvature right-hand sides against the oracle, and the normal projection
+    (M + damping K) n_d = rhs_d solved with a heat operator (rho_cp = dt = 1, k = damping)."""
+    import torch
+
+    from meltpooldg_b200.operators import HeatDiffuseOperator, LinearSolver, LinearSolverData
+    from oracle.oracle import Operator as OOp
+    from oracle.reinit import curvature_rhs, normal_rhs
+
+    om, gm, cm = meshes(degree, m, faces=faces, length=(1.0, 0.9, 1.1))
+    X, Y, Z = om.coords()
+    dist = np.sqrt((X - 0.5) ** 2 + (Y - 0.45) ** 2 + (Z - 0.55) ** 2) - 0.3
+    psi = np.tanh(dist / 0.05)
+    damping = 4e-3
+    g = HeatDiffuseOperator(gm, rho_cp=1.0, dt=1.0, conductivity=damping)
+    # the normalised gradient is checked on a field whose gradient never vanishes: far from the
+    # interface the tanh profile's gradient is at the rounding level of psi (and the distance
+    # function's interpolant has cells where it cancels by symmetry), so its direction is noise there
+    smooth = 0.8 * X - 0.5 * Y + 0.3 * Z + 0.05 * np.sin(3.0 * X) * np.cos(2.0 * Y)
+    for normalized, field in ((False, psi), (True, smooth)):
+        ref = normal_rhs(om, cm, field, normalized)
+        pre = 1e-5 * uniform_dofs(om, seed=11)  # the rhs accumulates (constrained rows keep pre)
+        nd = [to_gpu(pre) for _ in range(3)]
+        g.level_set_normal_rhs(to_gpu(field), *nd, normalized=normalized)
+        for d in range(3):
+            assert rel_err(nd[d].cpu().numpy() - pre, ref[d]) <= 1e-11
+    # the projection, then the curvature rhs of the projected normal
+    o = OOp(om, "heat", cmask=cm, rho_cp=1.0, dt=1.0, k=damping)
+    ref = normal_rhs(om, cm, psi)
+    normal = []
+    for d in range(3):
+        b = to_gpu(ref[d])
+        x = torch.zeros_like(b)
+        LinearSolver.solve(g, x, b, LinearSolverData("CG", "Diagonal", rel_tolerance=1e-12))
+        xs = x.cpu().numpy()
+        assert np.linalg.norm(ref[d] - o.vmult(xs)) <= 1e-11 * np.linalg.norm(ref[d])
+        normal.append(xs)
+    c_ref = curvature_rhs(om, cm, normal, 1e-6)
+    c = to_gpu(np.full(om.ndofs, 7.0))  # overwritten
+    g.level_set_curvature_rhs(c, *[to_gpu(v) for v in normal], normal_tolerance=1e-6)
+    assert rel_err(c.cpu().numpy(), c_ref) <= 1e-12

@@ -46,3 +46,24 @@ def test_diagonal_is_the_tangents():
                     for i in range(mesh.ndofs)])
     assert np.max(np.abs(d - ref)) <= 1e-12 * np.max(np.abs(ref))
     assert np.all(d[cmask != 0] == 0)
+
+
+def test_normal_and_curvature_rhs_of_simple_fields():
+    from oracle.reinit import curvature_rhs, normal_rhs
+
+    mesh = Mesh(2, (3, 2, 4), length=(0.6, 0.8, 1.2))
+    X, Y, Z = mesh.coords()
+    vol = 0.6 * 0.8 * 1.2
+    # linear level set: the gradient is constant, so each component sums to a_d * volume
+    a = (0.3, -1.2, 0.7)
+    n = normal_rhs(mesh, None, a[0] * X + a[1] * Y + a[2] * Z + 0.1)
+    for d in range(3):
+        assert abs(n[d].sum() - a[d] * vol) <= 1e-13
+    nn = normal_rhs(mesh, None, a[0] * X + a[1] * Y + a[2] * Z, normalized=True)
+    norm = np.sqrt(sum(c * c for c in a))
+    for d in range(3):
+        assert abs(nn[d].sum() - a[d] / norm * vol) <= 1e-13
+    # a normal field below the tolerance is divided by it: n = (alpha x, 0, 0) / tol, div = alpha / tol
+    alpha, tol = 1e-4, 1.0
+    c = curvature_rhs(mesh, None, [alpha * X, 0 * X, 0 * X], tol)
+    assert abs(c.sum() + alpha / tol * vol) <= 1e-15

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "brick.cuh"
 #include "kernels.h"
@@ -320,10 +321,12 @@ namespace mpdg
     const double *
     level_set_tables(int K)
     {
-      static double *dev[8][3] = {}; // [device][degree]
-      int            d         = 0;
-      if (cudaGetDevice(&d) != cudaSuccess || d >= 8)
+      static std::mutex mtx;
+      static double    *dev[64][3] = {}; // [device][degree]
+      int               d          = 0;
+      if (cudaGetDevice(&d) != cudaSuccess || d >= 64)
         return nullptr;
+      std::lock_guard<std::mutex> lock(mtx);
       if (!dev[d][K])
         {
           const Tables1D &t = tables(K);

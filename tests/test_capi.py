@@ -75,3 +75,35 @@ def test_header_compiles_as_c_and_cpp(tmp_path):
     r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-I",
                         os.path.join(root, "include"), str(src_cc)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes structures of meltpooldg_b200/_lib.py have the sizes and field offsets of the C
+    structures in include/mpdg_gpu.h (compiled with the host C compiler)."""
+    import ctypes as C
+    import subprocess
+
+    from meltpooldg_b200 import _lib as L
+
+    structs = {"mpdg_mesh_desc": L.MeshDesc, "mpdg_op_params": L.OpParams, "mpdg_heat_bc": L.HeatBC,
+               "mpdg_solid_liquid": L.SolidLiquid, "mpdg_solver_params": L.SolverParams,
+               "mpdg_solve_info": L.SolveInfo, "mpdg_mixed_params": L.MixedParams,
+               "mpdg_adjoint_params": L.AdjointParams, "mpdg_adjoint_result": L.AdjointResult}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "mpdg_gpu.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = str(tmp_path / "layout")
+    r = subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", exe],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)

@@ -107,3 +107,23 @@ def test_struct_layouts_match_the_header(tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """Without the CUDA library the Python operators raise instead of falling back to the CPU."""
+    import subprocess
+    import sys
+
+    code = (
+        "from meltpooldg_b200.operators import HeatDiffuseOperator, Mesh\n"
+        "try:\n"
+        "    HeatDiffuseOperator(Mesh(2, (2, 2, 2)), rho_cp=1.0, dt=1e-3)\n"
+        "except ImportError as e:\n"
+        "    print('ImportError', e)\n"
+        "else:\n"
+        "    print('no error')\n"
+    )
+    env = dict(os.environ, MPDG_LIB_PATH=str(tmp_path / "absent.so"))
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.startswith("ImportError") and "absent.so" in r.stdout, r.stdout

@@ -67,3 +67,44 @@ def test_normal_and_curvature_rhs_of_simple_fields():
     alpha, tol = 1e-4, 1.0
     c = curvature_rhs(mesh, None, [alpha * X, 0 * X, 0 * X], tol)
     assert abs(c.sum() + alpha / tol * vol) <= 1e-15
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_anisotropic_cell_against_direct_assembly(degree):
+    """Single cell, varying normal: the tangent matrix M/dt + int grad(phi_i) . D grad(phi_j) with
+    D = eps_t I + (eps_n - eps_t) n n^T, and the rhs int [c(psi) n - D grad psi] . grad(phi_i), built
+    point by point from numpy's Lagrange polynomials and Gauss-Legendre rule."""
+    from tests.assembled import element_1d
+
+    origin, length = (0.1, -0.2, 0.3), (0.5, 0.4, 0.7)
+    mesh = Mesh(degree, (1, 1, 1), origin=origin, length=length)
+    dt, eps_n, eps_t, tol = 1e-2, 0.05, 0.01, 1e-12
+    nodes, xq, wq, V, D = element_1d(degree)
+    n = degree + 1
+    h = np.array(length)
+    nh = radial_normal(mesh)
+    psi = np.random.default_rng(4).uniform(-0.9, 0.9, mesh.ndofs)
+    A = np.zeros((n ** 3, n ** 3))
+    rhs = np.zeros(n ** 3)
+    for a in range(n):
+        for b in range(n):
+            for c in range(n):
+                W = wq[a] * wq[b] * wq[c] * np.prod(h)
+                phi = np.array([V[c, i] * V[b, j] * V[a, l] for l in range(n) for j in range(n) for i in range(n)])
+                grad = np.array([[D[c, i] * V[b, j] * V[a, l] / h[0], V[c, i] * D[b, j] * V[a, l] / h[1],
+                                  V[c, i] * V[b, j] * D[a, l] / h[2]]
+                                 for l in range(n) for j in range(n) for i in range(n)])
+                nq = np.array([phi @ nh[d] for d in range(3)])
+                nq = nq / max(np.linalg.norm(nq), tol)
+                Dm = eps_t * np.eye(3) + (eps_n - eps_t) * np.outer(nq, nq)
+                A += W * (np.outer(phi, phi) / dt + grad @ Dm @ grad.T)
+                pq = phi @ psi
+                gp = grad.T @ psi
+                rhs += W * grad @ (0.5 * (1.0 - pq * pq) * nq - Dm @ gp)
+    u = np.random.default_rng(5).uniform(-1, 1, mesh.ndofs)
+    got = tangent_apply(mesh, None, dt, eps_n, eps_t, nh, tol, u)
+    assert np.max(np.abs(got - A @ u)) <= 1e-12 * np.max(np.abs(A @ u))
+    r = create_rhs(mesh, None, eps_n, eps_t, nh, tol, psi)
+    assert np.max(np.abs(r - rhs)) <= 1e-12 * np.max(np.abs(rhs))
+    d = diagonal(mesh, None, dt, eps_n, eps_t, nh, tol)
+    assert np.max(np.abs(d - np.diag(A))) <= 1e-12 * np.max(np.abs(np.diag(A)))

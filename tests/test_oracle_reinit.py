@@ -108,3 +108,26 @@ def test_anisotropic_cell_against_direct_assembly(degree):
     assert np.max(np.abs(r - rhs)) <= 1e-12 * np.max(np.abs(rhs))
     d = diagonal(mesh, None, dt, eps_n, eps_t, nh, tol)
     assert np.max(np.abs(d - np.diag(A))) <= 1e-12 * np.max(np.abs(np.diag(A)))
+
+
+def test_curvature_rhs_of_a_sphere_converges_to_two_over_r():
+    """Nodal normals of a sphere centred outside the box, n = (x - c) / |x - c|, have div n = 2 / r:
+    the sum of the curvature rhs tends to -int 2 / |x - c| dx (reference integral from a 12-point
+    Gauss rule per cell of an 8^3 grid), and the error falls at least 4x per mesh halving."""
+    from oracle.reinit import curvature_rhs
+
+    c = np.array([-0.4, 1.3, 0.6])
+    xg, wg = np.polynomial.legendre.leggauss(12)
+    pts = np.concatenate([(j + 0.5 * (xg + 1.0)) / 8.0 for j in range(8)])
+    wts = np.tile(0.5 * wg / 8.0, 8)
+    P = np.stack(np.meshgrid(pts, pts, pts, indexing="ij"), axis=-1)
+    Wt = np.einsum("a,b,c->abc", wts, wts, wts)
+    exact = -np.sum(Wt * 2.0 / np.linalg.norm(P - c, axis=-1))
+    err = []
+    for m in (2, 4, 8):
+        mesh = Mesh(2, (m, m, m))
+        X, Y, Z = mesh.coords()
+        r = np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2)
+        got = curvature_rhs(mesh, None, [(X - c[0]) / r, (Y - c[1]) / r, (Z - c[2]) / r], 1e-12).sum()
+        err.append(abs(got - exact))
+    assert err[1] <= err[0] / 4 and err[2] <= err[1] / 4 and err[2] <= 1e-5 * abs(exact), (err, exact)

@@ -190,6 +190,21 @@ namespace mpdg
     {
       check(mpdg_op_distribute_constraints(op_, dst, values));
     }
+    // NormalVectorOperator::create_rhs (normal_vector_operator.cpp:160-240) on this lattice:
+    // n_d += int (grad psi)_d phi, the gradient normalised when normalized is true
+    void
+    level_set_normal_rhs(const double *psi, double *nx, double *ny, double *nz, bool normalized = false) const
+    {
+      check(mpdg_level_set_normal_rhs(op_, psi, normalized ? 1 : 0, nx, ny, nz));
+    }
+    // CurvatureOperator::create_rhs (curvature_operator.cpp:190-255) on this lattice:
+    // dst = -int div(n) phi with n normalised at every DoF (overwrites dst)
+    void
+    level_set_curvature_rhs(double *dst, const double *nx, const double *ny, const double *nz,
+                            double normal_tolerance) const
+    {
+      check(mpdg_level_set_curvature_rhs(op_, nx, ny, nz, normal_tolerance, dst));
+    }
     mpdg_op *
     handle() const
     {

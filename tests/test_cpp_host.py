@@ -31,6 +31,7 @@ def test_cpp_host_layer_compiles_and_links(tmp_path):
     build_program(tmp_path, "heat_radiation")
     build_program(tmp_path, "heat_predictor")
     build_program(tmp_path, "heat_solidification")
+    build_program(tmp_path, "level_set_step")
 
 
 @pytest.mark.gpu

@@ -65,11 +65,17 @@ class Mesh:
         return d
 
 
-def _ptr(t) -> Optional[int]:
+def _ptr(t, n: Optional[int] = None, dtype=None) -> Optional[int]:
+    """Device address of a contiguous CUDA tensor, checked to hold at least n entries of dtype
+    (either check skipped when None), so that no kernel is handed a buffer it would overrun."""
     if t is None:
         return None
     if not t.is_cuda or not t.is_contiguous():
         raise ValueError("vectors must be contiguous CUDA tensors")
+    if dtype is not None and t.dtype != dtype:
+        raise TypeError(f"expected a {dtype} vector, got {t.dtype}")
+    if n is not None and t.numel() < n:
+        raise ValueError(f"vector of {t.numel()} entries where {n} are needed")
     return t.data_ptr()
 
 
@@ -93,6 +99,12 @@ class OperatorMatrixFree:
             except Exception:  # interpreter shutdown
                 pass
             self._h = None
+
+    def _v(self, t, dtype=None, n: Optional[int] = None) -> Optional[int]:
+        """_ptr of a vector of this operator: n_dofs entries (or n) of dtype (float64 by default)."""
+        import torch
+
+        return _ptr(t, self.mesh.ndofs if n is None else n, torch.float64 if dtype is None else dtype)
 
     def set_stream(self, stream_handle: int) -> None:
         check(lib().mpdg_op_set_stream(self._h, C.c_void_p(stream_handle)))
@@ -122,48 +134,51 @@ class OperatorMatrixFree:
         import torch
 
         if src.dtype == torch.float64:
-            check(lib().mpdg_op_vmult(self._h, _ptr(dst), _ptr(src)))
+            check(lib().mpdg_op_vmult(self._h, self._v(dst), self._v(src)))
         elif src.dtype == torch.float32:
-            check(lib().mpdg_op_vmult_f32(self._h, _ptr(dst), _ptr(src)))
+            check(lib().mpdg_op_vmult_f32(self._h, self._v(dst, torch.float32), self._v(src, torch.float32)))
         else:
             raise TypeError("vmult needs float64 or float32 vectors")
 
     def vmult_add(self, dst, src, scale: float = 1.0) -> None:
-        check(lib().mpdg_op_vmult_add(self._h, _ptr(dst), _ptr(src), float(scale)))
+        check(lib().mpdg_op_vmult_add(self._h, self._v(dst), self._v(src), float(scale)))
 
     def residual(self, r, b, x) -> None:
-        check(lib().mpdg_op_residual(self._h, _ptr(r), _ptr(b), _ptr(x)))
+        check(lib().mpdg_op_residual(self._h, self._v(r), self._v(b), self._v(x)))
 
     def vmult_host(self, dst: np.ndarray, src: np.ndarray) -> None:
-        assert dst.dtype == np.float64 and src.dtype == np.float64
+        for a in (dst, src):
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.size < self.mesh.ndofs:
+                raise ValueError(f"host vectors must be C-contiguous float64 arrays of {self.mesh.ndofs} entries")
         check(lib().mpdg_op_vmult_host(self._h, dst.ctypes.data, src.ctypes.data))
 
     def compute_inverse_diagonal_from_matrixfree(self, diag) -> None:
         import torch
 
         if diag.dtype == torch.float64:
-            check(lib().mpdg_op_compute_inverse_diagonal(self._h, _ptr(diag)))
+            check(lib().mpdg_op_compute_inverse_diagonal(self._h, self._v(diag)))
         else:
-            check(lib().mpdg_op_compute_inverse_diagonal_f32(self._h, _ptr(diag)))
+            check(lib().mpdg_op_compute_inverse_diagonal_f32(self._h, self._v(diag, torch.float32)))
 
     def create_rhs(self, dst, a, b=None, c=None) -> None:
-        check(lib().mpdg_op_create_rhs(self._h, _ptr(dst), _ptr(a), _ptr(b), _ptr(c)))
+        check(lib().mpdg_op_create_rhs(self._h, self._v(dst), self._v(a), self._v(b), self._v(c)))
 
     def create_rhs_and_apply_dirichlet(self, rhs, a, dirichlet_values, b=None, c=None, zero_out: bool = True) -> None:
         """create_rhs_and_apply_dirichlet_matrixfree (utilities_matrixfree.hpp:33-100): rhs (=|+=)
         -A x_D + create_rhs(a, b, c) without the Dirichlet constraints, then constrained rows 0;
         x_D = dirichlet_values on constrained DoFs, 0 elsewhere."""
-        check(lib().mpdg_op_create_rhs_and_apply_dirichlet(self._h, _ptr(rhs), _ptr(a), _ptr(b), _ptr(c),
-                                                          _ptr(dirichlet_values), 1 if zero_out else 0))
+        check(lib().mpdg_op_create_rhs_and_apply_dirichlet(self._h, self._v(rhs), self._v(a), self._v(b), self._v(c),
+                                                          self._v(dirichlet_values), 1 if zero_out else 0))
 
     def level_set_normal_rhs(self, psi, nx, ny, nz, normalized: bool = False) -> None:
         """NormalVectorOperator::create_rhs on this operator's lattice: n_d += int (grad psi)_d phi."""
-        check(lib().mpdg_level_set_normal_rhs(self._h, _ptr(psi), 1 if normalized else 0, _ptr(nx), _ptr(ny), _ptr(nz)))
+        check(lib().mpdg_level_set_normal_rhs(self._h, self._v(psi), 1 if normalized else 0, self._v(nx), self._v(ny),
+                                               self._v(nz)))
 
     def level_set_curvature_rhs(self, dst, nx, ny, nz, normal_tolerance: float) -> None:
         """CurvatureOperator::create_rhs on this operator's lattice: dst = -int div(n) phi."""
-        check(lib().mpdg_level_set_curvature_rhs(self._h, _ptr(nx), _ptr(ny), _ptr(nz), float(normal_tolerance),
-                                                 _ptr(dst)))
+        check(lib().mpdg_level_set_curvature_rhs(self._h, self._v(nx), self._v(ny), self._v(nz),
+                                                 float(normal_tolerance), self._v(dst)))
 
     def device_errors(self) -> int:
         return lib().mpdg_op_device_errors(self._h)
@@ -185,7 +200,7 @@ class HeatDiffuseOperator(OperatorMatrixFree):
         super().__init__(mesh, p, stream)
 
     def set_conductivity(self, k_cells_device) -> None:
-        check(lib().mpdg_op_set_conductivity(self._h, _ptr(k_cells_device)))
+        check(lib().mpdg_op_set_conductivity(self._h, self._v(k_cells_device, n=self.mesh.ncells)))
 
     def set_boundary_conditions(self, convection_faces: int = 0, convection_coefficient: float = 0.0,
                                 convection_temperature_infinity: float = 0.0, radiation_faces: int = 0,
@@ -220,13 +235,13 @@ class HeatDiffuseOperator(OperatorMatrixFree):
     def set_old_temperature(self, temperature_old_device) -> None:
         """Old temperature of the solidification tangent (kept by reference)."""
         self._temperature_old = temperature_old_device
-        check(lib().mpdg_op_set_old_temperature(self._h, _ptr(temperature_old_device)))
+        check(lib().mpdg_op_set_old_temperature(self._h, self._v(temperature_old_device)))
 
     def set_temperature(self, temperature_device) -> None:
         """Linearisation temperature of the radiation tangent (kept by reference, as the reference's
         operator keeps a const reference to its temperature vector)."""
         self._temperature = temperature_device
-        check(lib().mpdg_op_set_temperature(self._h, _ptr(temperature_device)))
+        check(lib().mpdg_op_set_temperature(self._h, self._v(temperature_device)))
 
 
 class AdvectionDiffusionOperator(OperatorMatrixFree):
@@ -265,7 +280,7 @@ class OlssonOperator(OperatorMatrixFree):
         """Normal field (three device vectors on the lattice, kept by reference)."""
         self._normal = (nx, ny, nz)
         check(lib().mpdg_op_set_reinit(self._h, float(self.eps_normal), float(self.eps_tangential),
-                                       float(self.normal_tolerance), _ptr(nx), _ptr(ny), _ptr(nz)))
+                                       float(self.normal_tolerance), self._v(nx), self._v(ny), self._v(nz)))
 
 
 @dataclass
@@ -311,8 +326,10 @@ class LinearSolver:
         if hist is not None:
             info.history = hist.ctypes.data
             info.history_capacity = hist.size
+        if solution.dtype not in (torch.float64, torch.float32):
+            raise TypeError("solve needs float64 or float32 vectors")
         fn = lib().mpdg_solve if solution.dtype == torch.float64 else lib().mpdg_solve_f32
-        rc = fn(op._h, _ptr(solution), _ptr(rhs), C.byref(p), C.byref(info))
+        rc = fn(op._h, op._v(solution, solution.dtype), op._v(rhs, solution.dtype), C.byref(p), C.byref(info))
         stats = SolveStats(info.iterations, info.initial_residual, info.final_residual,
                            hist[: info.iterations + 1] if hist is not None else np.zeros(0))
         check(rc)
@@ -331,7 +348,7 @@ class LinearSolver:
         hist = np.zeros(max_outer + 2)
         info.history = hist.ctypes.data
         info.history_capacity = hist.size
-        rc = lib().mpdg_solve_mixed(op._h, _ptr(solution), _ptr(rhs), C.byref(p), C.byref(info))
+        rc = lib().mpdg_solve_mixed(op._h, op._v(solution), op._v(rhs), C.byref(p), C.byref(info))
         stats = SolveStats(info.iterations, info.initial_residual, info.final_residual,
                            hist[: info.iterations + 1], info.inner_iterations)
         check(rc)

@@ -127,3 +127,39 @@ def test_missing_library_fails_loudly(tmp_path):
     r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert r.stdout.startswith("ImportError") and "absent.so" in r.stdout, r.stdout
+
+
+def test_vector_checks_before_any_kernel():
+    """The Python layer refuses vectors that are too short or of the wrong type before a pointer
+    reaches the library (a short buffer would be overrun on the device)."""
+    import pytest
+    import torch
+
+    from meltpooldg_b200.operators import _ptr
+
+    class FakeCuda:
+        is_cuda = True
+
+        def __init__(self, n, dtype, contiguous=True):
+            self.n, self.dtype, self.contiguous = n, dtype, contiguous
+
+        def is_contiguous(self):
+            return self.contiguous
+
+        def numel(self):
+            return self.n
+
+        def data_ptr(self):
+            return 4096
+
+    assert _ptr(None, 10, torch.float64) is None
+    assert _ptr(FakeCuda(10, torch.float64), 10, torch.float64) == 4096
+    assert _ptr(FakeCuda(12, torch.float32), 10, torch.float32) == 4096  # a longer buffer is fine
+    with pytest.raises(ValueError):
+        _ptr(FakeCuda(9, torch.float64), 10, torch.float64)
+    with pytest.raises(TypeError):
+        _ptr(FakeCuda(10, torch.float32), 10, torch.float64)
+    with pytest.raises(ValueError):
+        _ptr(FakeCuda(10, torch.float64, contiguous=False), 10, torch.float64)
+    with pytest.raises(ValueError):
+        _ptr(torch.zeros(10, dtype=torch.float64), 10, torch.float64)  # host memory

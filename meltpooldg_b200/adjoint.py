@@ -18,7 +18,7 @@ from dataclasses import dataclass
 
 from . import _lib as L
 from ._lib import check, lib
-from .operators import HeatDiffuseOperator, _ptr
+from .operators import HeatDiffuseOperator
 
 
 @dataclass
@@ -38,18 +38,21 @@ class TransientHeatAdjoint:
 
     def forward(self, log_k, qhat, amplitude: float, T_out) -> None:
         """States T_1..T_N into T_out (N x n_dofs, float64 CUDA tensor)."""
-        check(lib().mpdg_heat_forward(self.op._h, _ptr(log_k), _ptr(qhat), float(amplitude), C.byref(self.p),
-                                      _ptr(T_out)))
+        cells, states = self.op.mesh.ncells, self.p.n_steps * self.op.mesh.ndofs
+        check(lib().mpdg_heat_forward(self.op._h, self.op._v(log_k, n=cells), self.op._v(qhat, n=states),
+                                      float(amplitude), C.byref(self.p), self.op._v(T_out, n=states)))
 
     def objective_and_gradient(self, log_k, qhat, amplitude: float, target, grad_log_k=None):
         """(J, dJ/dA, stats); fills grad_log_k (n_cells float64 CUDA tensor) unless it is None."""
         res = L.AdjointResult()
-        check(lib().mpdg_adjoint_heat(self.op._h, _ptr(log_k), _ptr(qhat), float(amplitude), _ptr(target),
-                                      C.byref(self.p), _ptr(grad_log_k), C.byref(res)))
+        cells, states = self.op.mesh.ncells, self.p.n_steps * self.op.mesh.ndofs
+        check(lib().mpdg_adjoint_heat(self.op._h, self.op._v(log_k, n=cells), self.op._v(qhat, n=states),
+                                      float(amplitude), self.op._v(target, n=states), C.byref(self.p),
+                                      self.op._v(grad_log_k, n=cells), C.byref(res)))
         return res.objective, res.grad_amplitude, AdjointStats(res.forward_solves, res.adjoint_solves,
                                                                res.cg_iterations)
 
 
 def cell_stiffness_form(op: HeatDiffuseOperator, lam, T, form) -> None:
     """form_c = lam_c^T K_c T_c (unit conductivity) for every cell."""
-    check(lib().mpdg_heat_cell_stiffness_form(op._h, _ptr(lam), _ptr(T), _ptr(form)))
+    check(lib().mpdg_heat_cell_stiffness_form(op._h, op._v(lam), op._v(T), op._v(form, n=op.mesh.ncells)))

@@ -12,7 +12,14 @@ and no latent heat:
   temperature derivative -(v_s - v_l)(6 f_s - 6 f_s^2) / (T_liquidus - T_solidus), 0 at f_s = 0, 1;
 * tangent (:1029-1050): (rho c_p / dt + d(rho c_p)/dT (T - T_old) / dt) u tested with phi,
   k grad u + dk/dT grad T u tested with grad phi; u with Dirichlet entries 0, T and T_old plain;
-* residual part of create_rhs (:485-527): -rho c_p(T) (T - T_old) / dt phi - k(T) grad T . grad phi.
+* residual part of create_rhs (:485-527): -rho c_p(T) (T - T_old) / dt phi - k(T) grad T . grad phi;
+* latent heat of fusion L > 0 (include/meltpooldg/core/material.hpp:654-655): the specific heat gains
+  an apparent capacity C(f_s) over the mushy zone and its derivative gains dC/dT
+  (material.templates.hpp:561-614; source/heat/apparent_capacity.cpp:157-300), zero at f_s <= 0 and
+  f_s >= 1, in one of three shapes, each of integral L over [T_solidus, T_liquidus]:
+  "constant" L / dT; "poly4_bell" L (2 / dT) b(1 - 2 f_s) with b(x) = 15/16 (1 - x^2)^2;
+  "qlq" (the default) a tent of peak 2 L / dT at the mid temperature, each flank linear with
+  quadratic, zero-slope ends of width dT / 6, evaluated at T = T_liquidus - f_s dT.
 Per cell with QGauss(k+1), vectorised over the cells with numpy.
 """
 from __future__ import annotations
@@ -33,6 +40,47 @@ class SolidLiquid:
     liquidus_temperature: float = 1.0
     solidus_temperature: float = 0.0
     sharp: bool = False
+    latent_heat: float = 0.0  # latent heat of fusion per unit mass; > 0 adds the apparent capacity
+    capacity_type: str = "qlq"  # "qlq" | "poly4_bell" | "constant"
+
+
+def _zero_slope_ramp(x, x1, x2, y1, y2, delta):
+    """Value and derivative of the ramp from (x1, y1) to (x2, y2) that is flat at both ends: a
+    quadratic on [x1, x1 + delta], a line of slope s = (y2 - y1) / (x2 - x1 - delta) in between,
+    and a quadratic on [x2 - delta, x2]; value and slope are continuous."""
+    s = (y2 - y1) / (x2 - x1 - delta)
+    lo, hi = x < x1 + delta, x > x2 - delta
+    val = np.where(lo, y1 + 0.5 * s * (x - x1) ** 2 / delta,
+                   np.where(hi, y2 - 0.5 * s * (x2 - x) ** 2 / delta, y1 + s * (x - x1 - 0.5 * delta)))
+    der = np.where(lo, s * (x - x1) / delta, np.where(hi, s * (x2 - x) / delta, s))
+    return val, der
+
+
+def apparent_capacity(m: SolidLiquid, fs):
+    """Apparent specific heat capacity of the latent heat and its temperature derivative at the
+    solid fractions fs (0 where fs <= 0 or fs >= 1 and where latent_heat is 0)."""
+    fs = np.asarray(fs, dtype=np.float64)
+    if m.latent_heat <= 0.0:
+        return np.zeros_like(fs), np.zeros_like(fs)
+    Ts, Tl, L = m.solidus_temperature, m.liquidus_temperature, m.latent_heat
+    dT = Tl - Ts
+    inside = (fs > 0.0) & (fs < 1.0)
+    if m.capacity_type == "constant":
+        c, dc = np.full_like(fs, L / dT), np.zeros_like(fs)
+    elif m.capacity_type == "poly4_bell":
+        r = 2.0 / dT
+        x = 1.0 - 2.0 * fs
+        c = L * r * (15.0 / 16.0) * (1.0 - x * x) ** 2
+        dc = L * r * r * (15.0 / 4.0) * (x * x - 1.0) * x
+    elif m.capacity_type == "qlq":
+        T = Tl - fs * dT
+        Tp, peak, delta = 0.5 * (Ts + Tl), 2.0 * L / dT, dT / 6.0
+        up, dup = _zero_slope_ramp(T, Ts, Tp, 0.0, peak, delta)
+        down, ddown = _zero_slope_ramp(T, Tp, Tl, peak, 0.0, delta)
+        c, dc = np.where(T <= Tp, up, down), np.where(T <= Tp, dup, ddown)
+    else:
+        raise ValueError(f"unknown apparent capacity type {m.capacity_type}")
+    return np.where(inside, c, 0.0), np.where(inside, dc, 0.0)
 
 
 def material(m: SolidLiquid, T: np.ndarray):
@@ -55,8 +103,9 @@ def material(m: SolidLiquid, T: np.ndarray):
         return np.where(end, 0.0, (vs - vl) * dw)
 
     (rl, cl, kl), (rs, cs, ks) = m.liquid, m.solid
-    rho, cp = pr(rl, rs), pr(cl, cs)
-    return rho * cp, pr(kl, ks), dpr(rl, rs) * cp + rho * dpr(cl, cs), dpr(kl, ks)
+    ca, dca = apparent_capacity(m, fs)
+    rho, cp, dcp = pr(rl, rs), pr(cl, cs) + ca, dpr(cl, cs) + dca
+    return rho * cp, pr(kl, ks), dpr(rl, rs) * cp + rho * dcp, dpr(kl, ks)
 
 
 def _fields(mesh: Mesh, cmask, u, T, Told, plain_u: bool):

@@ -131,3 +131,64 @@ def test_curvature_rhs_of_a_sphere_converges_to_two_over_r():
         got = curvature_rhs(mesh, None, [(X - c[0]) / r, (Y - c[1]) / r, (Z - c[2]) / r], 1e-12).sum()
         err.append(abs(got - exact))
     assert err[1] <= err[0] / 4 and err[2] <= err[1] / 4 and err[2] <= 1e-5 * abs(exact), (err, exact)
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3])
+def test_wetting_faces_are_the_boundary_flux(degree):
+    """With a constant normal, D is constant and for a quadratic u integration by parts gives
+    int_boundary (D grad u . n_f) phi = int D grad u . grad phi + tr(D H_u) int phi exactly: the wetting
+    tangent on all six faces equals the cell diffusion apply plus tr(D H_u) times the lumped mass."""
+    from oracle.reinit import wetting_tangent_apply
+
+    mesh = Mesh(degree, (3, 2, 4), origin=(0.1, -0.2, 0.3), length=(0.6, 0.5, 0.8))
+    X, Y, Z = mesh.coords()
+    a = np.array([0.3, -0.5, 0.8]) / np.linalg.norm([0.3, -0.5, 0.8])
+    normal = [np.full(mesh.ndofs, c) for c in a]
+    eps_n, eps_t, tol = 0.05, 0.01, 1e-12
+    if degree == 1:  # bilinear terms only: H_u has no diagonal
+        u = -0.4 * X * Y + 0.2 * Y * Z + X - 0.5
+        H = np.array([[0.0, -0.4, 0.0], [-0.4, 0.0, 0.2], [0.0, 0.2, 0.0]])
+    else:
+        u = 0.7 * X * X - 0.4 * X * Y + 1.3 * Z * Z + 0.2 * Y * Z + X - 0.5
+        H = np.array([[1.4, -0.4, 0.0], [-0.4, 0.0, 0.2], [0.0, 0.2, 2.6]])
+    D = eps_t * np.eye(3) + (eps_n - eps_t) * np.outer(a, a)
+    Ku = tangent_apply(mesh, None, 1e300, eps_n, eps_t, normal, tol, u)  # the 1/dt mass term vanishes
+    M1 = tangent_apply(mesh, None, 1.0, 0.0, 0.0, normal, tol, np.ones(mesh.ndofs))
+    ref = Ku + np.sum(D * H) * M1
+    got = wetting_tangent_apply(mesh, None, 63, eps_n, eps_t, normal, tol, u)
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+    # additive over faces
+    parts = sum(wetting_tangent_apply(mesh, None, 1 << f, eps_n, eps_t, normal, tol, u) for f in range(6))
+    assert np.max(np.abs(parts - got)) <= 1e-13 * np.max(np.abs(got))
+
+
+def test_wetting_rhs_linearisation_and_compressive_flux():
+    from oracle.reinit import wetting_rhs, wetting_tangent_apply
+
+    mesh = Mesh(2, (3, 3, 2), length=(0.9, 0.6, 0.5))
+    cmask = mesh.face_mask(0b000100)
+    n = radial_normal(mesh)
+    eps_n, eps_t, tol = 0.05, 0.01, 1e-12
+    faces = 0b110011
+    rng = np.random.default_rng(7)
+    psi = rng.uniform(-0.9, 0.9, mesh.ndofs)
+    du = np.where(cmask == 0, rng.uniform(-1, 1, mesh.ndofs), 0.0)
+    # the diffusive part is linear in psi: rhs(psi + du) - rhs(psi) = -tangent(du) + compressive change
+    zero_c = lambda p: wetting_rhs(mesh, cmask, faces, eps_n, eps_t, n, tol, p)  # noqa: E731
+    e = 1e-6
+    fd = (zero_c(psi + e * du) - zero_c(psi - e * du)) / (2 * e)
+    tan = wetting_tangent_apply(mesh, cmask, faces, eps_n, eps_t, n, tol, du)
+    comp = fd + tan  # what is left is the derivative of the compressive flux, int -psi du n.n_f phi
+    assert np.all(comp[cmask != 0] == 0) and np.all(tan[cmask != 0] == 0)
+    assert np.max(np.abs(comp)) > 1e-3 * np.max(np.abs(tan))
+    # at psi = 0 that derivative vanishes (c'(0) = 0), so the tangent is minus the rhs derivative
+    fd0 = (zero_c(e * du) - zero_c(-e * du)) / (2 * e)
+    assert np.max(np.abs(fd0 + tan)) <= 1e-8 * np.max(np.abs(tan))
+    # a constant psi = p on one face: only c(p) n.n_f is left; its sum is c(p) times the flux of n
+    p = 0.3
+    a = np.array([0.6, 0.0, 0.8])
+    const = [np.full(mesh.ndofs, c) for c in a]
+    r = wetting_rhs(mesh, None, 1 << 1, eps_n, eps_t, const, tol, np.full(mesh.ndofs, p))
+    assert abs(r.sum() - 0.5 * (1 - p * p) * a[0] * 0.6 * 0.5) <= 1e-14
+    r = wetting_rhs(mesh, None, 1 << 4, eps_n, eps_t, const, tol, np.full(mesh.ndofs, p))
+    assert abs(r.sum() + 0.5 * (1 - p * p) * a[2] * 0.9 * 0.6) <= 1e-14

@@ -96,9 +96,19 @@ def diagonal(mesh: Mesh, cmask, dt, eps_n, eps_t, normal, tol) -> np.ndarray:
     return out
 
 
-def normal_rhs(mesh: Mesh, cmask, psi, normalized: bool = False):
-    """NormalVectorOperator::create_rhs (source/level_set/normal_vector_operator.cpp:160-240, no
-    narrow band): int g_d phi with g = grad psi, or g normalised (divided by 1e-16 at or below it)."""
+def _band_mask(ev, B, idx, level_set, narrow_band):
+    """Narrow-band mask at the Gauss points: 1 where |level set| < narrow_band, else 0
+    (include/meltpooldg/level_set/level_set_tools.hpp:357-368); 1 everywhere without a band."""
+    if narrow_band is None:
+        return 1.0
+    lq = ev(B, B, B, np.asarray(level_set, dtype=np.float64)[idx])
+    return np.where(np.abs(lq) >= narrow_band, 0.0, 1.0)
+
+
+def normal_rhs(mesh: Mesh, cmask, psi, normalized: bool = False, narrow_band=None):
+    """NormalVectorOperator::create_rhs (source/level_set/normal_vector_operator.cpp:160-240):
+    int g_d phi with g = grad psi, or g normalised (divided by 1e-16 at or below it); with a
+    narrow band the gradient is masked by |psi| < narrow_band at each point first."""
     qp, qw, B, G, _ = tables(mesh.degree)
     h = [mesh.length[d] / mesh.m[d] for d in range(3)]
     free = np.ones(mesh.ndofs, bool) if cmask is None else np.asarray(cmask) == 0
@@ -106,7 +116,8 @@ def normal_rhs(mesh: Mesh, cmask, psi, normalized: bool = False):
     idx = _dof_index(mesh, cx, cy, cz)
     ev = lambda Z, Y, X, f: np.einsum("al,bj,ci,xlji->xabc", Z, Y, X, f)  # noqa: E731
     pc = np.asarray(psi, dtype=np.float64)[idx]
-    g = _grad(ev, B, G, h, pc)
+    mask = _band_mask(ev, B, idx, psi, narrow_band)
+    g = [c * mask for c in _grad(ev, B, G, h, pc)]
     if normalized:
         nn = np.sqrt(g[0] ** 2 + g[1] ** 2 + g[2] ** 2)
         s = np.where(nn > 1e-16, 1.0 / np.where(nn > 0, nn, 1.0), 1e16)
@@ -122,9 +133,10 @@ def normal_rhs(mesh: Mesh, cmask, psi, normalized: bool = False):
     return out
 
 
-def curvature_rhs(mesh: Mesh, cmask, normal, tol):
-    """CurvatureOperator::create_rhs (source/level_set/curvature_operator.cpp:190-255, no narrow
-    band): -int div(n) phi with n = normalize(n_i, tol) at every DoF; constrained rows 0."""
+def curvature_rhs(mesh: Mesh, cmask, normal, tol, level_set=None, narrow_band=None):
+    """CurvatureOperator::create_rhs (source/level_set/curvature_operator.cpp:190-255):
+    -int div(n) phi with n = normalize(n_i, tol) at every DoF, masked by |level_set| < narrow_band
+    at each point when a band is given; constrained rows 0."""
     qp, qw, B, G, _ = tables(mesh.degree)
     h = [mesh.length[d] / mesh.m[d] for d in range(3)]
     free = np.ones(mesh.ndofs, bool) if cmask is None else np.asarray(cmask) == 0
@@ -136,6 +148,7 @@ def curvature_rhs(mesh: Mesh, cmask, normal, tol):
     nv = [c * s for c in nv]
     ev = lambda Z, Y, X, f: np.einsum("al,bj,ci,xlji->xabc", Z, Y, X, f)  # noqa: E731
     div = (ev(B, B, G, nv[0][idx]) / h[0] + ev(B, G, B, nv[1][idx]) / h[1] + ev(G, B, B, nv[2][idx]) / h[2])
+    div = div * _band_mask(ev, B, idx, level_set, narrow_band)
     W = h[0] * h[1] * h[2] * np.einsum("a,b,c->abc", qw, qw, qw)[None]
     te = lambda Z, Y, X, F: np.einsum("al,bj,ci,xabc->xlji", Z, Y, X, F)  # noqa: E731
     out = np.zeros(mesh.ndofs)
@@ -218,3 +231,20 @@ def wetting_tangent_apply(mesh: Mesh, cmask, faces: int, eps_n, eps_t, normal, t
 def wetting_rhs(mesh: Mesh, cmask, faces: int, eps_n, eps_t, normal, tol, psi) -> np.ndarray:
     """Wetting boundary faces' part of create_rhs (psi read plainly, constrained rows 0)."""
     return _wetting(mesh, cmask, faces, eps_n, eps_t, normal, tol, psi, rhs=True)
+
+
+def projection_apply(mesh: Mesh, cmask, damping, u, level_set=None, narrow_band=None) -> np.ndarray:
+    """The normal-vector / curvature projection operator M + damping K per component
+    (normal_vector_operator.cpp:326-358, curvature_operator.cpp:337-369), u with Dirichlet entries
+    0; with a narrow band both terms are masked by |level_set| < narrow_band at each point."""
+    qp, qw, B, G, _ = tables(mesh.degree)
+    h = [mesh.length[d] / mesh.m[d] for d in range(3)]
+    free = np.ones(mesh.ndofs, bool) if cmask is None else np.asarray(cmask) == 0
+    cx, cy, cz = _cells(mesh)
+    idx = _dof_index(mesh, cx, cy, cz)
+    ev = lambda Z, Y, X, f: np.einsum("al,bj,ci,xlji->xabc", Z, Y, X, f)  # noqa: E731
+    W = h[0] * h[1] * h[2] * np.einsum("a,b,c->abc", qw, qw, qw)[None]
+    W = W * _band_mask(ev, B, idx, level_set, narrow_band)
+    uc = np.where(free, u, 0.0)[idx]
+    g = _grad(ev, B, G, h, uc)
+    return _scatter(mesh, B, G, h, idx, free, W * ev(B, B, B, uc), [W * damping * c for c in g])

@@ -192,3 +192,56 @@ def test_wetting_rhs_linearisation_and_compressive_flux():
     assert abs(r.sum() - 0.5 * (1 - p * p) * a[0] * 0.6 * 0.5) <= 1e-14
     r = wetting_rhs(mesh, None, 1 << 4, eps_n, eps_t, const, tol, np.full(mesh.ndofs, p))
     assert abs(r.sum() + 0.5 * (1 - p * p) * a[2] * 0.9 * 0.6) <= 1e-14
+
+
+def _sub_box(degree, m, length, cells_x):
+    """The box of the first cells_x cell layers in x and the lattice indices of its DoFs in the full
+    mesh."""
+    h = length[0] / m[0]
+    sub = Mesh(degree, (cells_x, m[1], m[2]), length=(cells_x * h, length[1], length[2]))
+    n_full = [degree * c + 1 for c in m]
+    nx = degree * cells_x + 1
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(n_full[1]), np.arange(n_full[2]), indexing="ij")
+    order = np.argsort((i + nx * (j + n_full[1] * k)).ravel())
+    full = (i + n_full[0] * (j + n_full[1] * k)).ravel()[order]
+    return sub, full, h
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_narrow_band_is_the_operator_on_the_band(degree):
+    """A level set x and a band |x| < 2 h: every Gauss point of the first two cell layers is inside,
+    every other one outside, so the masked projection operator and right-hand sides equal the
+    unmasked ones of the two-layer box (the C++ oracle's heat operator for M + damping K)."""
+    from oracle.reinit import curvature_rhs, normal_rhs, projection_apply
+
+    m, length, damping = (5, 3, 2), (1.0, 0.6, 0.4), 0.02
+    mesh = Mesh(degree, m, length=length)
+    sub, full, h = _sub_box(degree, m, length, 2)
+    X, Y, Z = mesh.coords()
+    rng = np.random.default_rng(9)
+    u = rng.uniform(-1, 1, mesh.ndofs)
+    # without a band the projection operator is the heat operator with rho_cp = dt = 1, k = damping
+    cmask = mesh.face_mask(0b001000)
+    o = Operator(mesh, "heat", cmask=cmask, rho_cp=1.0, dt=1.0, k=damping)
+    ou = o.vmult(u)
+    assert np.max(np.abs(projection_apply(mesh, cmask, damping, u) - ou)) <= 1e-12 * np.max(np.abs(ou))
+    got = projection_apply(mesh, None, damping, u, level_set=X, narrow_band=2 * h)
+    ref = np.zeros(mesh.ndofs)
+    ref[full] = Operator(sub, "heat", rho_cp=1.0, dt=1.0, k=damping).vmult(u[full])
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+    # the normal rhs of the level set x and the curvature rhs of a smooth normal field, banded by x
+    band = 2 * h
+    got = normal_rhs(mesh, None, X, narrow_band=band)
+    sX = sub.coords()[0]
+    for d in range(3):
+        ref = np.zeros(mesh.ndofs)
+        ref[full] = normal_rhs(sub, None, sX)[d]
+        assert np.max(np.abs(got[d] - ref)) <= 1e-13
+    normal = [1.0 + 0.2 * Y, Z - 0.3 * X, X * Y + 0.1]
+    got = curvature_rhs(mesh, None, normal, 1e-10, level_set=X, narrow_band=band)
+    ref = np.zeros(mesh.ndofs)
+    ref[full] = curvature_rhs(sub, None, [c[full] for c in normal], 1e-10)
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+    # a band wider than the level set's range masks nothing
+    wide = curvature_rhs(mesh, None, normal, 1e-10, level_set=X, narrow_band=10.0)
+    assert np.array_equal(wide, curvature_rhs(mesh, None, normal, 1e-10))

@@ -259,11 +259,13 @@ def committed_traffic():
 
 
 def cpu_baseline(mesh, kc, src, seconds=15.0):
-    """The oracle (CPU restatement of the reference apply) on the same workload, all host threads."""
+    """The oracle (CPU restatement of the reference apply) on the same workload, all host threads,
+    built with -march=native on this host."""
     from oracle.oracle import Mesh as OMesh
     from oracle.oracle import Operator as OOp
-    from oracle.oracle import num_threads
+    from oracle.oracle import host_cpu, num_threads, use_native_build
 
+    use_native_build()
     om = OMesh(4, (64, 64, 64))
     op = OOp(om, "heat", cmask=om.face_mask(63), rho_cp=1.0, dt=1e-3, k_cell=kc)
     op.vmult(src)  # warm-up
@@ -277,18 +279,20 @@ def cpu_baseline(mesh, kc, src, seconds=15.0):
             break
     t = statistics.median(times)
     return {"value": mesh.ndofs / t / 1e9, "unit": UNIT, "cores": num_threads(), "kind": "port",
-            "sample": f"{len(times)} full applies of the workload (median), oracle C++ restatement, OpenMP"}
+            "host": host_cpu(), "build": "g++ -O3 -march=native -fopenmp",
+            "sample": f"{len(times)} full applies of the workload (median), oracle C++ restatement, OpenMP "
+                      "over every host thread"}
 
 
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
     from oracle.oracle import Mesh as OMesh
     from oracle.oracle import Operator as OOp
-    from oracle.oracle import num_threads
+    from oracle.oracle import host_cpu, num_threads, use_native_build
 
+    use_native_build()
     mesh, kc, src = make_inputs()
     om = OMesh(4, (64, 64, 64))
     op = OOp(om, "heat", cmask=om.face_mask(63), rho_cp=1.0, dt=1e-3, k_cell=kc)
@@ -309,6 +313,7 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(WORKLOAD, parallelism="cpu"),
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": num_threads(), "kind": "port",
+                             "host": host_cpu(), "build": "g++ -O3 -march=native -fopenmp",
                              "sample": f"{done} full applies of the workload, oracle C++ restatement "
                                        "(the reference needs deal.II, absent on this image)"},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -552,7 +557,6 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
-            subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
             cpu = cpu_baseline(mesh, kc, src)
         except Exception as exc:
             cpu = {"error": repr(exc)}

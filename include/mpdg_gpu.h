@@ -335,12 +335,17 @@ MPDG_API int mpdg_heat_cell_stiffness_form(mpdg_op *op, const double *lam, const
      - Every call clears the ticket and flags it uses (stream-ordered, before its kernel).  All calls
        on a device share the one array, so calls that overlap on the GPU (different streams or host
        threads without ordering) race and give wrong results: order them.
-     - A bounded device wait that gives up records an error word in the scratch array, which this
-       entry point does not read back. */
+     - A bounded device wait that gives up records an error word in the scratch array; read it
+       with mpdg_heat_vmult_noalloc_errors after the call (every call clears it first). */
 #define MPDG_NOALLOC_SCRATCH_BYTES (256 * 1024)
 #define MPDG_NOALLOC_MAX_BRICKS ((MPDG_NOALLOC_SCRATCH_BYTES - 256) / 4)
 MPDG_API int mpdg_heat_vmult_noalloc(const mpdg_mesh_desc *mesh, const mpdg_op_params *params,
                                      const double *k_cells_dev, double *dst, const double *src, void *cuda_stream);
+/* The error word of the allocation-free vmult on the current device, read after the work already
+   enqueued on cuda_stream (the call synchronises that stream) and then cleared: 0 when every bounded
+   wait of the last call ended normally, nonzero when one gave up (that call's dst is then not
+   valid).  Copies from and to the fixed scratch array; allocates nothing. */
+MPDG_API int mpdg_heat_vmult_noalloc_errors(void *cuda_stream, int *error_word);
 
 /* create_rhs_and_apply_dirichlet_matrixfree (include/meltpooldg/linear_algebra/utilities_matrixfree.hpp:33-100):
    with the Dirichlet constraints switched off (the no-BC DoF set), temp = -A x_D + create_rhs(a, b, c)
@@ -370,8 +375,25 @@ MPDG_API int mpdg_op_distribute_constraints(mpdg_op *op, double *dst, const doub
 MPDG_API int mpdg_vec_alloc(mpdg_op *op, double **x);
 MPDG_API int mpdg_vec_free(double *x);
 
-/* Number of error words raised by bounded device waits since the last call (and reset). */
+/* The error code recorded by a bounded device wait that gave up (1) or by a stale brick ticket (2)
+   since the last call, 0 when none; reading resets it. */
 MPDG_API int mpdg_op_device_errors(mpdg_op *op);
+
+/* Failure injection for tests; no counterpart in the reference (its MPI ranks have no device-side
+   waits).  The apply kernels deal bricks out through a ticket counter and wait, bounded, for the
+   per-brick flags of their lower neighbours; these hooks make such a wait run out on purpose
+   without faulting or hanging the GPU.
+   mpdg_op_test_set_wait_limit: sleeps (about 32 ns each) before a wait of this handle's kernels gives
+   up and records its error word; 0 restores the default (2^22).
+   mpdg_op_test_set_ticket: writes the brick ticket counter, stream-ordered and synchronised, as a
+   counter left behind by an aborted launch would look.  A following apply deals out bricks from
+   that value on: bricks below it are never processed, so their upper neighbours' waits give up, and
+   tickets past the last brick are reported and skipped.  The last CTA of that launch resets the
+   counter, so later launches are normal again.
+   mpdg_op_n_bricks: bricks of the handle's FP64 apply (the range of useful ticket values). */
+MPDG_API int mpdg_op_test_set_wait_limit(mpdg_op *op, unsigned spins);
+MPDG_API int mpdg_op_test_set_ticket(mpdg_op *op, unsigned value);
+MPDG_API int mpdg_op_n_bricks(const mpdg_op *op);
 
 /* Description of the last error on the calling thread. */
 MPDG_API const char *mpdg_last_error(void);

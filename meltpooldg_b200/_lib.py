@@ -177,6 +177,9 @@ SIGNATURES = [
     ("mpdg_solve_f32", [P, P, P, C.POINTER(SolverParams), C.POINTER(SolveInfo)], C.c_int),
     ("mpdg_solve_mixed", [P, P, P, C.POINTER(MixedParams), C.POINTER(SolveInfo)], C.c_int),
     ("mpdg_op_device_errors", [P], C.c_int),
+    ("mpdg_op_test_set_wait_limit", [P, C.c_uint], C.c_int),
+    ("mpdg_op_test_set_ticket", [P, C.c_uint], C.c_int),
+    ("mpdg_op_n_bricks", [P], C.c_int),
     ("mpdg_adjoint_heat", [P, P, P, D, P, C.POINTER(AdjointParams), P, C.POINTER(AdjointResult)], C.c_int),
     ("mpdg_heat_forward", [P, P, P, D, C.POINTER(AdjointParams), P], C.c_int),
     ("mpdg_heat_cell_stiffness_form", [P, P, P, P], C.c_int),
@@ -185,6 +188,7 @@ SIGNATURES = [
     ("mpdg_vec_axpby", [P, P, D, P, D], C.c_int),
     ("mpdg_vec_norm", [P, P, C.POINTER(D)], C.c_int),
     ("mpdg_heat_vmult_noalloc", [P, P, P, P, P, P], C.c_int),
+    ("mpdg_heat_vmult_noalloc_errors", [P, C.POINTER(C.c_int)], C.c_int),
     ("mpdg_last_error", [], C.c_char_p),
 ]
 OPTIONAL = []

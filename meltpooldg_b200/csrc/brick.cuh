@@ -49,13 +49,18 @@ namespace mpdg
                                  // holds the previous slab's contributions and is only added into
   };
 
+  constexpr unsigned SPIN_LIMIT    = 1u << 22; // x 32 ns sleeps: ~0.1-0.2 s
+  constexpr int      ERR_FLAG_WAIT = 1;
+  constexpr int      ERR_TICKET    = 2;
+
   struct SyncDesc
   {
-    unsigned *ticket; // brick ticket counter (0 between launches)
-    unsigned *done;   // finished-CTA counter (0 between launches)
-    unsigned *flags;  // per-brick init flags (== epoch when initialised)
-    unsigned  epoch;  // launch epoch (never 0)
-    int      *error;  // set to a nonzero code when a bounded wait gives up
+    unsigned *ticket;                  // brick ticket counter (0 between launches)
+    unsigned *done;                    // finished-CTA counter (0 between launches)
+    unsigned *flags;                   // per-brick init flags (== epoch when initialised)
+    unsigned  epoch;                   // launch epoch (never 0)
+    int      *error;                   // set to a nonzero code when a bounded wait gives up
+    unsigned  spin_limit = SPIN_LIMIT; // sleeps before a wait gives up
   };
 
   // Optional fused dot product of an apply dst = A src: the kernel sums src^T A src cell by cell and
@@ -85,10 +90,6 @@ namespace mpdg
       devices.fetch_or(bit);
     return e;
   }
-
-  constexpr unsigned SPIN_LIMIT    = 1u << 22; // x 32 ns sleeps: ~0.1-0.2 s
-  constexpr int      ERR_FLAG_WAIT = 1;
-  constexpr int      ERR_TICKET    = 2;
 
   __device__ __forceinline__ long long
   lattice_index(const GridDesc &g, int I, int J, int L)
@@ -494,7 +495,7 @@ namespace mpdg
             unsigned       it = 0;
             while (ld_acquire(s.flags + nb) != s.epoch)
               {
-                if (++it > SPIN_LIMIT)
+                if (++it > s.spin_limit)
                   {
                     atomicExch(s.error, ERR_FLAG_WAIT);
                     break;

@@ -100,6 +100,7 @@ struct mpdg_op
   unsigned *d_sync = nullptr; // [0] ticket, [1] done, [2] reducer counter, [3..] flags
   int      *d_err  = nullptr;
   unsigned  epoch  = 0;
+  unsigned  spin_limit = SPIN_LIMIT; // bound of every spin wait of this handle's kernels
   double   *d_red  = nullptr; // reducer partials
   double   *d_part = nullptr; // one partial per brick for the fused CG dot product (heat)
   double   *d_scal = nullptr; // 64 scalars
@@ -138,6 +139,7 @@ struct mpdg_op
     s.flags  = d_sync + 3;
     s.epoch  = epoch;
     s.error  = d_err;
+    s.spin_limit = spin_limit;
     return s;
   }
   bool
@@ -1758,6 +1760,34 @@ mpdg_vec_free(double *x)
   if (x && cudaFree(x) != cudaSuccess)
     return fail(MPDG_ERR_CUDA, "cudaFree in mpdg_vec_free");
   return MPDG_OK;
+}
+
+int
+mpdg_op_test_set_wait_limit(mpdg_op *op, unsigned spins)
+{
+  if (int e = check_op(op))
+    return e;
+  op->spin_limit = spins ? spins : SPIN_LIMIT;
+  return MPDG_OK;
+}
+
+int
+mpdg_op_test_set_ticket(mpdg_op *op, unsigned value)
+{
+  if (int e = check_op(op))
+    return e;
+  // stream-ordered: the next launch on the handle's stream finds this counter
+  MPDG_CUDA(cudaMemcpyAsync(op->d_sync, &value, sizeof(unsigned), cudaMemcpyHostToDevice, op->stream));
+  MPDG_CUDA(cudaStreamSynchronize(op->stream));
+  return MPDG_OK;
+}
+
+int
+mpdg_op_n_bricks(const mpdg_op *op)
+{
+  if (!op)
+    return -1;
+  return op->nbr[0] * op->nbr[1] * op->nbr[2];
 }
 
 int

@@ -153,3 +153,26 @@ mpdg_heat_vmult_noalloc(const mpdg_mesh_desc *mesh, const mpdg_op_params *params
     return reject(MPDG_ERR_CUDA, std::string("heat apply launch: ") + cudaGetErrorString(e));
   return MPDG_OK;
 }
+
+extern "C" MPDG_API int
+mpdg_heat_vmult_noalloc_errors(void *cuda_stream, int *error_word)
+{
+  // Reads the wait error word (scratch word 3) after the calls already enqueued on cuda_stream and
+  // clears it.  Copies to and from the symbol: no device memory is allocated.
+  if (!error_word)
+    return reject(MPDG_ERR_ARG, "null argument to mpdg_heat_vmult_noalloc_errors");
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  int          word   = 0;
+  const int    zero   = 0;
+  const size_t off    = 3 * sizeof(unsigned);
+  cudaError_t  e = cudaMemcpyFromSymbolAsync(&word, mpdg_noalloc_scratch, sizeof(int), off, cudaMemcpyDeviceToHost,
+                                             stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyToSymbolAsync(mpdg_noalloc_scratch, &zero, sizeof(int), off, cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess)
+    return reject(MPDG_ERR_CUDA, std::string("reading the scratch error word: ") + cudaGetErrorString(e));
+  *error_word = word;
+  return MPDG_OK;
+}

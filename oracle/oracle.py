@@ -57,6 +57,41 @@ class OrcOp(C.Structure):
 _lib = None
 
 
+def use_native_build() -> str:
+    """Switch this process to liborc_native.so (-march=native, built here on first use), for the timed
+    CPU baseline; must run before the first oracle call.  Returns the library path."""
+    global _LIB_PATH
+    if _lib is not None:
+        raise RuntimeError("the oracle library is already loaded")
+    # always rebuilt: a copy built on another host may use instructions this one lacks
+    native = os.path.join(_HERE, "liborc_native.so")
+    if os.path.exists(native):
+        os.remove(native)
+    subprocess.run(["make", "-s", "-C", _HERE, "native"], check=True)
+    _LIB_PATH = native
+    return native
+
+
+def host_cpu() -> dict:
+    """Host CPU description for the baseline record: logical CPUs, physical cores, model name."""
+    info = {"logical_cpus": os.cpu_count()}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=20).stdout
+        kv = {}
+        for ln in out.splitlines():
+            if ":" in ln:
+                k, v = ln.split(":", 1)
+                kv[k.strip()] = v.strip()
+        info["model"] = kv.get("Model name")
+        tpc, cps, sockets = (int(kv.get(k, "0") or 0) for k in ("Thread(s) per core", "Core(s) per socket", "Socket(s)"))
+        if cps and sockets:
+            info["physical_cores"] = cps * sockets
+        info["threads_per_core"] = tpc
+    except Exception:
+        pass
+    return info
+
+
 def lib():
     global _lib
     if _lib is None:

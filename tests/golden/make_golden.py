@@ -1,7 +1,7 @@
 """Extract the reference's golden norms into tests/golden/reference_logs.json.
 
-Run in a checkout where the MeltPoolDG sources are available (default /root/reference); the
-output is committed so that nothing at test time reads the reference tree.
+Usage: python tests/golden/make_golden.py <path to a MeltPoolDG source tree>.  The output is
+committed so that nothing at test time reads the reference tree.
 
 Sources (paths inside the MeltPoolDG tree):
   applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/
@@ -15,7 +15,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py <path to a MeltPoolDG source tree>")
+REF = sys.argv[1]
 CASES = {
     "heat_unidirectional_2d_q1": (
         "applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/"

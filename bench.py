@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--case", default=None,
                     help="run one named case for profiling and exit: apply_<degree>_<cells>_<f64|f32>, "
                          "faces_<degree>_<cells>_<f64|f32>, supg_<degree>_<cells>_<f64|f32>, solid_<degree>_<cells>_<f64|f32>, "
-                         "(e.g. apply_2_128_f32), solve_fp64 / solve_mixed (128^3 FE_Q(2) CG to 1e-8), advection, adjoint")
+                         "(e.g. apply_2_128_f32), solve (128^3 FE_Q(2) FP64 vs mixed CG), cg_f64 / cg_f32 / cg_f64_3pass "
+                         "(one CG solve), advection, adjoint")
     return ap.parse_args()
 
 
@@ -149,9 +150,34 @@ def run_case(name):
         print(json.dumps({"case": name, **run_advection(torch, stream)}), flush=True)
     elif name == "adjoint":
         print(json.dumps({"case": name, **run_adjoint(torch, stream)}), flush=True)
-    elif name in ("solve_fp64", "solve_mixed"):
-        out = run_solves(torch, stream, modes=(name[6:],))
-        print(json.dumps({"case": name, **out}), flush=True)
+    elif name == "solve":
+        print(json.dumps({"case": name, **run_solves(torch, stream, repeats=2)}), flush=True)
+    elif name.startswith("cg_"):
+        # one Jacobi-CG solve to 1e-8 on the 128^3 FE_Q(2) problem in FP64 or FP32, for profiling
+        from meltpooldg_b200.inputs import normal_cells, uniform_dofs
+        from meltpooldg_b200.operators import LinearSolver, LinearSolverData
+
+        mesh = Mesh(2, (128, 128, 128), dirichlet_faces=63)
+        kc = np.exp(normal_cells(mesh, seed=3, sigma=0.5))
+        op = HeatDiffuseOperator(mesh, rho_cp=1.0, dt=1e-3, conductivity_cells=kc, stream=stream.cuda_stream)
+        if name.endswith("3pass"):
+            from meltpooldg_b200 import _lib as L
+
+            L.lib().mpdg_op_set_cg_variant(op._h, 0)
+        dt = torch.float32 if "f32" in name else torch.float64
+        bd = torch.tensor(uniform_dofs(mesh, seed=3, cmask=mesh_mask(mesh)), dtype=dt, device="cuda")
+        res = {}
+        for rep in range(2):
+            x = torch.zeros_like(bd)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = LinearSolver.solve(op, x, bd, LinearSolverData("CG", "Diagonal", rel_tolerance=1e-5 if dt == torch.float32 else 1e-8))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            res = {"ms": e0.elapsed_time(e1), "iterations": st.iterations,
+                   "us_per_iteration": e0.elapsed_time(e1) * 1e3 / max(st.iterations, 1)}
+        print(json.dumps({"case": name, **res}), flush=True)
     else:
         raise SystemExit(f"unknown case {name}")
 
@@ -320,9 +346,17 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_solves(torch, stream, modes=("fp64", "mixed")):
-    """CG solve time to 1e-8: FP64 Jacobi-CG vs FP32-inner/FP64-outer defect correction on the
-    128^3 FE_Q(2) problem (dt 1e-3, k = exp(N(0,0.5^2)) seed 3, b = U[-1,1] seed 3)."""
+SOLVE_TOL = 5e-10  # relative residual that keeps the solution error at or below 1e-8 on this problem
+
+
+def run_solves(torch, stream, repeats=5):
+    """Jacobi-CG on the 128^3 FE_Q(2) problem (dt 1e-3, k = exp(N(0,0.5^2)) seed 3, b = U[-1,1] seed 3):
+    the plain FP64 solve against the FP32-inner / FP64-outer defect correction (inner CG to 1e-4).
+    Both arms stop at the relative residual SOLVE_TOL, which keeps their error against a 1e-12 FP64
+    solution at or below 1e-8 (a residual of 1e-8 bounds the error only up to the condition number,
+    about 15 here); each arm is timed `repeats` times (median, min, max).  One run of each at the
+    residual 1e-8 is reported for reference.  The error figures are against an FP64 CG solve to
+    1e-12; the test suite compares the same solves with the oracle's CG solution."""
     from meltpooldg_b200.inputs import normal_cells, uniform_dofs
     from meltpooldg_b200.operators import HeatDiffuseOperator, LinearSolver, LinearSolverData, Mesh
 
@@ -331,35 +365,55 @@ def run_solves(torch, stream, modes=("fp64", "mixed")):
     b = uniform_dofs(mesh, seed=3, cmask=mesh_mask(mesh))
     op = HeatDiffuseOperator(mesh, rho_cp=1.0, dt=1e-3, conductivity_cells=kc, stream=stream.cuda_stream)
     bd = torch.tensor(b, device="cuda")
-    out = {"workload": "heat_cg_q2_128cube", "dofs": mesh.ndofs, "tol": 1e-8}
-    res = {}
-    for mode in modes + modes:
+    out = {"workload": "heat_cg_q2_128cube", "dofs": mesh.ndofs, "tol": SOLVE_TOL, "repeats": repeats,
+           "inner_rel_tol": 1e-4}
+
+    def one(mode, tol):
         x = torch.zeros_like(bd)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         if mode == "fp64":
-            st = LinearSolver.solve(op, x, bd, LinearSolverData("CG", "Diagonal", rel_tolerance=1e-8))
-            its = st.iterations
+            st = LinearSolver.solve(op, x, bd, LinearSolverData("CG", "Diagonal", rel_tolerance=tol))
+            its, outer = st.iterations, None
         else:
-            st = LinearSolver.solve_mixed(op, x, bd, outer_rel_tol=1e-8, inner_rel_tol=1e-4)
-            its = st.inner_iterations
+            st = LinearSolver.solve_mixed(op, x, bd, outer_rel_tol=tol, inner_rel_tol=1e-4,
+                                          inexact_last=(mode == "mixed_inexact"))
+            its, outer = st.inner_iterations, st.iterations
         e1.record(stream)
         torch.cuda.synchronize()
-        res[mode] = (e0.elapsed_time(e1), its, x)
-    # error of both against a tightly converged FP64 solve
+        return e0.elapsed_time(e1), its, outer, x
+
     xr = torch.zeros_like(bd)
     LinearSolver.solve(op, xr, bd, LinearSolverData("CG", "Diagonal", rel_tolerance=1e-12))
     nr = torch.linalg.norm(xr).item()
+    nb = torch.linalg.norm(bd).item()
+    modes = ("fp64", "mixed", "mixed_inexact")
+    one("fp64", SOLVE_TOL)  # warm-up of every kernel and work vector
+    one("mixed_inexact", SOLVE_TOL)
+    times = {m: [] for m in modes}
+    last = {}
+    for _ in range(repeats):
+        for mode in modes:
+            ms, its, outer, x = one(mode, SOLVE_TOL)
+            times[mode].append(ms)
+            last[mode] = (its, outer, x)
     for mode in modes:
-        ms, its, x = res[mode]
+        its, outer, x = last[mode]
         r = torch.empty_like(bd)
         op.residual(r, bd, x)
-        out[mode] = {"ms": ms, "iterations": its,
-                     "rel_residual": torch.linalg.norm(r).item() / torch.linalg.norm(bd).item(),
+        t = sorted(times[mode])
+        out[mode] = {"ms": statistics.median(t), "ms_min": t[0], "ms_max": t[-1], "iterations": its,
+                     "outer_iterations": outer, "rel_residual": torch.linalg.norm(r).item() / nb,
                      "rel_error_vs_fp64_1e-12": torch.linalg.norm(x - xr).item() / nr}
-    if "fp64" in res and "mixed" in res:
-        out["speedup_mixed_vs_fp64"] = res["fp64"][0] / res["mixed"][0]
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
+    out["speedup_mixed_inexact_vs_fp64"] = out["fp64"]["ms"] / out["mixed_inexact"]["ms"]
+    at_1e8 = {}
+    for mode in ("fp64", "mixed"):
+        ms, its, outer, x = one(mode, 1e-8)
+        at_1e8[mode] = {"ms": ms, "iterations": its,
+                        "rel_error_vs_fp64_1e-12": torch.linalg.norm(x - xr).item() / nr}
+    out["at_residual_1e-8"] = at_1e8
     return out
 
 

@@ -135,6 +135,10 @@ typedef struct mpdg_mixed_params
   int32_t max_inner;
   int32_t solver;          /* mpdg_solver_kind of the inner solver                         */
   int32_t restart;         /* inner GMRES basis size                                       */
+  int32_t inexact_last;    /* 0: every inner solve reduces its residual by inner_rel_tol;
+                              1: an inner solve needs no more than the outer tolerance asks
+                              for: it stops at max(inner_rel_tol, 0.5 outer_tol / |r|)   */
+  int32_t reserved;
 } mpdg_mixed_params;
 
 typedef struct mpdg_adjoint_params
@@ -231,6 +235,26 @@ MPDG_API int mpdg_level_set_normal_rhs(mpdg_op *op, const double *psi, int norma
                                        double *nz);
 MPDG_API int mpdg_level_set_curvature_rhs(mpdg_op *op, const double *nx, const double *ny, const double *nz,
                                           double normal_tolerance, double *dst);
+/* Inflow/outflow condition of the advection-diffusion operator
+   (AdvectionDiffusionOperation::create_inflow_outflow_constraints,
+   source/level_set/advection_diffusion_operation.cpp:369-499, with the operator's set_inflow_outflow_bc
+   and do_pre_vmult / do_post_vmult, source/level_set/advection_diffusion_operator.cpp:536-578).
+   faces: 6-bit mask of the box faces that carry the condition (bit 2d low / 2d+1 high face of dim d,
+   0 removes it).  Every support point of such a face where the outward normal n and the velocity v
+   satisfy n . v <= 0 is an inflow DoF (Dirichlet DoFs excluded); values: DEVICE array of n_dofs
+   holding the condition's function at the lattice points, read at the inflow DoFs during this call.
+   With the condition set, vmult treats the inflow DoFs as identity rows (src reads 0 there, dst_i =
+   src_i), the inverse diagonal is 1 there, and mpdg_op_create_rhs_and_apply_dirichlet lifts the
+   inflow values as additional inhomogeneous constraints (its apply runs without the hooks) and
+   zeroes those rows of the right-hand side.  mpdg_op_distribute_inflow writes the values into x
+   (the solve's last step, advection_diffusion_operation.cpp:288-296); mpdg_op_n_inflow counts the
+   inflow DoFs; mpdg_op_set_inflow_outflow_pre_post switches the vmult / diagonal hooks
+   (set_apply_inflow_outflow_constraints_pre_post_matrix_free). */
+MPDG_API int     mpdg_op_set_inflow_outflow(mpdg_op *op, uint32_t faces, const double *values);
+MPDG_API int64_t mpdg_op_n_inflow(const mpdg_op *op);
+MPDG_API int     mpdg_op_set_inflow_outflow_pre_post(mpdg_op *op, int enabled);
+MPDG_API int     mpdg_op_distribute_inflow(mpdg_op *op, double *x);
+
 /* The linearisation temperature of the radiation tangent and diagonal (the operator's const
    reference to the temperature vector, heat_diffuse_operator.hpp:121-135): a DEVICE array of
    n_dofs entries that the caller keeps alive and current; NULL detaches it.  vmult and the
@@ -392,6 +416,15 @@ MPDG_API int mpdg_op_device_errors(mpdg_op *op);
    counter, so later launches are normal again.
    mpdg_op_n_bricks: bricks of the handle's FP64 apply (the range of useful ticket values). */
 MPDG_API int mpdg_op_test_set_wait_limit(mpdg_op *op, unsigned spins);
+/* Selects the implementation of the Jacobi-CG iteration behind mpdg_solve / mpdg_solve_f32 / the
+   inner solves of mpdg_solve_mixed (LinearSolver::solve with SolverCG, linear_solver.hpp:106-110):
+   fused != 0 (the default) runs one sweep per iteration where the operator allows it (heat, FE_Q(2),
+   Dirichlet on whole faces only, no boundary-face terms, constant material): the vector updates, the
+   preconditioner, the operator apply and the dot products of an iteration in one launch, with the
+   next step lengths from a recurrence of the dot products.  fused == 0 runs the three-pass
+   iteration (p update, apply with the fused p.Ap, x/r update).  Both follow SolverCG's iterates and
+   ReductionControl's test. */
+MPDG_API int mpdg_op_set_cg_variant(mpdg_op *op, int fused);
 MPDG_API int mpdg_op_test_set_ticket(mpdg_op *op, unsigned value);
 MPDG_API int mpdg_op_n_bricks(const mpdg_op *op);
 

@@ -119,6 +119,8 @@ class MixedParams(C.Structure):
         ("max_inner", C.c_int32),
         ("solver", C.c_int32),
         ("restart", C.c_int32),
+        ("inexact_last", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -163,6 +165,10 @@ SIGNATURES = [
     ("mpdg_vec_alloc", [P, C.POINTER(C.c_void_p)], C.c_int),
     ("mpdg_vec_free", [P], C.c_int),
     ("mpdg_op_set_temperature", [P, P], C.c_int),
+    ("mpdg_op_set_inflow_outflow", [P, C.c_uint32, P], C.c_int),
+    ("mpdg_op_n_inflow", [P], C.c_int64),
+    ("mpdg_op_set_inflow_outflow_pre_post", [P, C.c_int], C.c_int),
+    ("mpdg_op_distribute_inflow", [P, P], C.c_int),
     ("mpdg_op_set_solidification", [P, C.POINTER(SolidLiquid)], C.c_int),
     ("mpdg_op_set_old_temperature", [P, P], C.c_int),
     ("mpdg_op_vmult", [P, P, P], C.c_int),
@@ -178,6 +184,7 @@ SIGNATURES = [
     ("mpdg_solve_mixed", [P, P, P, C.POINTER(MixedParams), C.POINTER(SolveInfo)], C.c_int),
     ("mpdg_op_device_errors", [P], C.c_int),
     ("mpdg_op_test_set_wait_limit", [P, C.c_uint], C.c_int),
+    ("mpdg_op_set_cg_variant", [P, C.c_int], C.c_int),
     ("mpdg_op_test_set_ticket", [P, C.c_uint], C.c_int),
     ("mpdg_op_n_bricks", [P], C.c_int),
     ("mpdg_adjoint_heat", [P, P, P, D, P, C.POINTER(AdjointParams), P, C.POINTER(AdjointResult)], C.c_int),

@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmpdg_b200.so")
-SOURCES = ["tables.cpp", "heat.cu", "heat_solid.cu", "faces.cu", "reinit.cu", "adv.cu", "vec.cu", "adjoint.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["tables.cpp", "heat.cu", "heat_solid.cu", "faces.cu", "reinit.cu", "adv.cu", "vec.cu", "adjoint.cu", "cgfused.cu", "capi.cu", "noalloc.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",

@@ -20,6 +20,8 @@
 #include <vector>
 
 #include "mpdg_gpu.h"
+#include "cgfused.h"
+#include "tables.h"
 #include "kernels.h"
 
 using namespace mpdg;
@@ -90,6 +92,12 @@ struct mpdg_op
   const double *d_temp_old = nullptr; // T_old of the solidification tangent (not owned)
   long long     sync_cap = 0;         // brick flags allocated in d_sync (after the 3 counters)
   int           supg = 0;         // SUPG stabilisation (advection-diffusion)
+  // inflow/outflow condition (advection-diffusion): inflow DoFs are identity rows of vmult
+  uint8_t      *d_mask_io  = nullptr; // Dirichlet mask | inflow flags: the apply's read / write mask
+  long long    *d_in_idx   = nullptr; // inflow DoFs
+  double       *d_in_val   = nullptr; // their prescribed values
+  long long     n_inflow   = 0;
+  bool          inflow_prepost = true; // set_apply_inflow_outflow_constraints_pre_post_matrix_free
   double        eps_n = 0.0, eps_t = 0.0, ntol = 1e-16; // reinitialisation
   const double *d_normal[3]{};                           // reinitialisation normal field (not owned)
   double        supg_coef = 0.0;
@@ -101,6 +109,7 @@ struct mpdg_op
   int      *d_err  = nullptr;
   unsigned  epoch  = 0;
   unsigned  spin_limit = SPIN_LIMIT; // bound of every spin wait of this handle's kernels
+  bool      fused_cg   = true;       // one-sweep PCG iteration where the operator allows it
   double   *d_red  = nullptr; // reducer partials
   double   *d_part = nullptr; // one partial per brick for the fused CG dot product (heat)
   double   *d_scal = nullptr; // 64 scalars
@@ -374,14 +383,44 @@ namespace
         h.b        = b;
         h.mask_src = mask_src;
         h.skip     = skip;
+        // inflow rows (advection_diffusion_operator.cpp:543-578): src reads 0 there, the cell
+        // terms skip those rows, and the row is the identity
+        const bool hooks = which == 0 && op->n_inflow > 0 && op->with_bc && op->inflow_prepost;
+        if (hooks)
+          h.grid.cmask = op->d_mask_io;
         MPDG_CUDA(adv_apply<T>(h, op->stream));
+        if (hooks)
+          MPDG_CUDA(idx_add_scaled<T>(dst, src, op->d_in_idx, op->n_inflow, scale, op->stream));
       }
+    return MPDG_OK;
+  }
+
+  // inverse diagonal: 1 on the inflow rows (advection_diffusion_operator.cpp:440-445)
+  template <typename T>
+  int
+  inflow_unit_diagonal(mpdg_op *op, T *diag)
+  {
+    if (op->kind == MPDG_ADVDIFF && op->n_inflow > 0 && op->with_bc && op->inflow_prepost)
+      MPDG_CUDA(idx_set<T>(diag, op->d_in_idx, nullptr, op->n_inflow, T(1), op->stream));
     return MPDG_OK;
   }
 
   template <typename T>
   int
+  inverse_diagonal_cells(mpdg_op *op, T *diag);
+
+  template <typename T>
+  int
   inverse_diagonal(mpdg_op *op, T *diag)
+  {
+    if (int e = inverse_diagonal_cells<T>(op, diag))
+      return e;
+    return inflow_unit_diagonal<T>(op, diag);
+  }
+
+  template <typename T>
+  int
+  inverse_diagonal_cells(mpdg_op *op, T *diag)
   {
     const GridDesc g = op->grid();
     if (op->kind == MPDG_HEAT && (op->tangent_faces() || op->solid))
@@ -492,6 +531,133 @@ namespace
     return cap;
   }
 
+  // whether the one-sweep PCG iteration (cgfused.cu) covers this operator: heat, FE_Q(2), Dirichlet
+  // on whole faces only, no boundary-face terms, constant material
+  bool
+  fused_cg_applies(const mpdg_op *op)
+  {
+    return op->fused_cg && op->kind == MPDG_HEAT && op->degree == 2 && op->d_mask == nullptr && op->with_bc &&
+           !op->tangent_faces() && !op->solid;
+  }
+
+  // Preconditioned CG with one launch per iteration (cgfused.cu): the same iterates as cg_solve in
+  // exact arithmetic, vectors in the padded layout of the sweep, x copied in and out once per solve.
+  template <typename T>
+  int
+  cg_solve_fused(mpdg_op *op, T *x, const T *b, const T *invd, int max_it, double abs_tol, double rel_tol,
+                 mpdg_solve_info *info, const char *tag, bool x_zero)
+  {
+    const std::string t(tag);
+    FusedCG<T>        f;
+    for (int d = 0; d < 3; ++d)
+      {
+        f.m[d] = op->m[d];
+        f.n[d] = op->degree * op->m[d] + 1;
+      }
+    f.P0     = FusedCG<T>::padded_pitch(f.n[0]);
+    f.faces  = op->faces;
+    const HeatGeom geo = heat_geom(op, op->rho_cp / op->dt);
+    f.mass_coef = geo.mass_coef;
+    f.geo[0] = geo.cx;
+    f.geo[1] = geo.cy;
+    f.geo[2] = geo.cz;
+    f.kconst = op->k;
+    f.kcell  = op->kcell<T>();
+    int dev = 0, sms = 148;
+    MPDG_CUDA(cudaGetDevice(&dev));
+    MPDG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    f.plan(sms);
+    const long long plen = f.padded_len(), rows = (long long)f.n[1] * f.n[2];
+    T *X = op->vec<T>(t + "fX", plen), *D = op->vec<T>(t + "fD", plen);
+    T *R[2] = {op->vec<T>(t + "fR0", plen), op->vec<T>(t + "fR1", plen)};
+    T *P[2] = {op->vec<T>(t + "fP0", plen), op->vec<T>(t + "fP1", plen)};
+    T *V[2] = {op->vec<T>(t + "fV0", plen), op->vec<T>(t + "fV1", plen)};
+    double *part = op->vec<double>(t + "fpart", (size_t)5 * f.ntiles);
+    double *hist = op->vec<double>(t + "hist", (size_t)max_it + 2);
+    if (!X || !D || !R[0] || !R[1] || !P[0] || !P[1] || !V[0] || !V[1] || !part || !hist)
+      return fail(MPDG_ERR_NOMEM, "fused CG work vectors");
+    // r_0 = b - A x_0 (b itself for a zero initial guess), x_0 and the inverse diagonal, padded
+    if (x_zero)
+      MPDG_CUDA(pad_rows<T, T>(R[0], b, f.n[0], f.P0, rows, op->stream));
+    else
+      {
+        T *r = op->vec<T>(t + "r");
+        if (!r)
+          return fail(MPDG_ERR_NOMEM, "CG work vector");
+        if (int e = apply<T>(op, (int)OutMode::BPlus, -1.0, r, x, b, 1))
+          return e;
+        MPDG_CUDA(pad_rows<T, T>(R[0], r, f.n[0], f.P0, rows, op->stream));
+      }
+    if (x_zero)
+      MPDG_CUDA(vec_fill<T>(X, T(0), plen, op->stream));
+    else
+      MPDG_CUDA(pad_rows<T, T>(X, x, f.n[0], f.P0, rows, op->stream));
+    if (invd)
+      MPDG_CUDA(pad_rows<T, T>(D, invd, f.n[0], f.P0, rows, op->stream));
+    else
+      MPDG_CUDA(vec_fill<T>(D, T(1), plen, op->stream));
+    CUtensorMap mX, mD, mR[2], mP[2], mV[2];
+    int         me = f.make_map(&mX, X) | f.make_map(&mD, D);
+    for (int i = 0; i < 2; ++i)
+      me |= f.make_map(&mR[i], R[i]) | f.make_map(&mP[i], P[i]) | f.make_map(&mV[i], V[i]);
+    if (me)
+      return fail(MPDG_ERR_CUDA, "cuTensorMapEncodeTiled failed for the fused CG vectors");
+    CGState st{};
+    st.abs_tol = abs_tol;
+    st.rel_tol = rel_tol;
+    st.max_it  = max_it;
+    *op->h_cg  = st;
+    MPDG_CUDA(cudaMemcpyAsync(op->d_cg, op->h_cg, sizeof(CGState), cudaMemcpyHostToDevice, op->stream));
+    unsigned *counter = op->d_sync + 1;
+    MPDG_CUDA(f.sweep(true, mR[0], mV[0], mP[0], mX, mD, X, R[1], P[0], V[0], op->d_cg, part, counter, hist,
+                      op->d_err, op->spin_limit, op->stream));
+    long long k = 1; // next sweep
+    int       batch = 4, it_prev = 0;
+    double    res_prev = -1.0;
+    for (;;)
+      {
+        MPDG_CUDA(cudaMemcpyAsync(op->h_cg, op->d_cg, sizeof(CGState), cudaMemcpyDeviceToHost, op->stream));
+        MPDG_CUDA(cudaStreamSynchronize(op->stream));
+        const CGState &cur = *op->h_cg;
+        if (cur.done)
+          break;
+        if (k > 1)
+          {
+            batch    = next_cg_batch(batch, cur.it, cur.res, cur.tol, it_prev, it_prev == 0 ? cur.res0 : res_prev);
+            it_prev  = cur.it;
+            res_prev = cur.res;
+          }
+        for (int j = 0; j < batch; ++j, ++k)
+          {
+            const int i = (int)((k - 1) & 1), o = (int)(k & 1);
+            MPDG_CUDA(f.sweep(false, mR[i], mV[i], mP[i], mX, mD, X, R[o], P[o], V[o], op->d_cg, part, counter,
+                              hist, op->d_err, op->spin_limit, op->stream));
+          }
+      }
+    MPDG_CUDA(unpad_rows<T, T>(x, X, f.n[0], f.P0, rows, op->stream));
+    const CGState &fin = *op->h_cg;
+    if (info)
+      {
+        info->iterations       = fin.it;
+        info->status           = fin.done == 1 ? MPDG_OK : MPDG_ERR_NOT_CONVERGED;
+        info->initial_residual = fin.res0;
+        info->final_residual   = fin.res;
+        if (info->history && info->history_capacity > 0)
+          {
+            const int cnt = std::min(info->history_capacity, fin.it + 1);
+            MPDG_CUDA(cudaMemcpy(info->history, hist, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+          }
+      }
+    MPDG_CUDA(cudaStreamSynchronize(op->stream));
+    int dev_err = 0;
+    MPDG_CUDA(cudaMemcpy(&dev_err, op->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (dev_err)
+      return fail(MPDG_ERR_TIMEOUT, "a bounded device wait gave up during the CG solve");
+    if (fin.done != 1)
+      return fail(MPDG_ERR_NOT_CONVERGED, "CG did not converge in " + std::to_string(fin.it) + " iterations");
+    return MPDG_OK;
+  }
+
   // ---------------------------------------------------------------------------------------------
   // Preconditioned CG (dealii::SolverCG semantics), all scalars on the device.  x_zero: the caller
   // guarantees x == 0, so the initial residual is b itself and its apply is skipped; b_scratch (with
@@ -501,6 +667,8 @@ namespace
   cg_solve(mpdg_op *op, T *x, const T *b, const T *invd, int max_it, double abs_tol, double rel_tol,
            mpdg_solve_info *info, const char *tag, bool x_zero = false, T *b_scratch = nullptr)
   {
+    if (fused_cg_applies(op))
+      return cg_solve_fused<T>(op, x, b, invd, max_it, abs_tol, rel_tol, info, tag, x_zero);
     const long long n = op->ndofs;
     const std::string t(tag);
     T *r = x_zero && b_scratch == b ? b_scratch : op->vec<T>(t + "r");
@@ -865,6 +1033,9 @@ mpdg_op_destroy(mpdg_op *op)
     cudaStreamSynchronize(op->stream);
   else
     cudaDeviceSynchronize();
+  cudaFree(op->d_mask_io);
+  cudaFree(op->d_in_idx);
+  cudaFree(op->d_in_val);
   for (auto &kv : op->ws)
     cudaFree(kv.second.first);
   cudaFree(op->d_sync);
@@ -1097,6 +1268,120 @@ mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient)
     return fail(MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator");
   op->supg      = enabled ? 1 : 0;
   op->supg_coef = coefficient;
+  return MPDG_OK;
+}
+
+int
+mpdg_op_set_inflow_outflow(mpdg_op *op, uint32_t faces, const double *values)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_ADVDIFF)
+    return fail(MPDG_ERR_ARG, "inflow/outflow conditions belong to the advection-diffusion operator");
+  if (faces & ~63u)
+    return fail(MPDG_ERR_ARG, "inflow/outflow faces: a 6-bit mask of box faces");
+  if (faces && !values)
+    return fail(MPDG_ERR_ARG, "inflow/outflow conditions need their values on the lattice");
+  cudaFree(op->d_mask_io);
+  cudaFree(op->d_in_idx);
+  cudaFree(op->d_in_val);
+  op->d_mask_io = nullptr;
+  op->d_in_idx  = nullptr;
+  op->d_in_val  = nullptr;
+  op->n_inflow  = 0;
+  if (!faces)
+    return MPDG_OK;
+  // support points of the marked faces where the outward normal n and the (affine) velocity v
+  // satisfy n . v <= 0 (advection_diffusion_operation.cpp:369-499), Dirichlet DoFs excluded; the
+  // coordinates are origin + h (c + node_i), the last point origin + length
+  const int       K = op->degree, n[3] = {K * op->m[0] + 1, K * op->m[1] + 1, K * op->m[2] + 1};
+  const Tables1D &t = tables(K);
+  std::vector<double> xs[3];
+  for (int d = 0; d < 3; ++d)
+    {
+      xs[d].resize(n[d]);
+      for (int I = 0; I < n[d]; ++I)
+        {
+          const int c = std::min(I / K, op->m[d] - 1), i = I - K * c;
+          xs[d][I] = I == n[d] - 1 ? op->origin[d] + op->length[d] : op->origin[d] + op->h[d] * (c + t.nodes[i]);
+        }
+    }
+  std::vector<uint8_t> dmask;
+  if (op->d_mask)
+    {
+      dmask.resize(op->ndofs);
+      MPDG_CUDA(cudaMemcpy(dmask.data(), op->d_mask, op->ndofs, cudaMemcpyDeviceToHost));
+    }
+  std::vector<uint8_t>   flag(op->ndofs, 0);
+  std::vector<long long> idx;
+  for (int L = 0; L < n[2]; ++L)
+    for (int J = 0; J < n[1]; ++J)
+      for (int I = 0; I < n[0]; ++I)
+        {
+          const int  lat[3] = {I, J, L};
+          const long long q = I + (long long)n[0] * (J + (long long)n[1] * L);
+          bool       in     = false;
+          for (int f = 0; f < 6 && !in; ++f)
+            {
+              const int d = f / 2, side = f % 2;
+              if (!((faces >> f) & 1u) || lat[d] != (side ? n[d] - 1 : 0))
+                continue;
+              const double x = xs[0][I], y = xs[1][J], z = xs[2][L];
+              const double v = op->vel[d] + op->vel[3 + 3 * d] * x + op->vel[4 + 3 * d] * y + op->vel[5 + 3 * d] * z;
+              in             = (side ? v : -v) <= 0.0;
+            }
+          bool con = false;
+          for (int f = 0; f < 6; ++f)
+            if (((op->faces >> f) & 1u) && lat[f / 2] == (f % 2 ? n[f / 2] - 1 : 0))
+              con = true;
+          if (!dmask.empty() && dmask[q])
+            con = true;
+          if (in && !con)
+            {
+              flag[q] = 1;
+              idx.push_back(q);
+            }
+          if (con || in)
+            flag[q] = 1; // the apply's mask: Dirichlet and inflow DoFs
+        }
+  op->n_inflow = (long long)idx.size();
+  if (cudaMalloc(&op->d_mask_io, op->ndofs) != cudaSuccess ||
+      cudaMalloc(&op->d_in_idx, sizeof(long long) * std::max<size_t>(1, idx.size())) != cudaSuccess ||
+      cudaMalloc(&op->d_in_val, sizeof(double) * std::max<size_t>(1, idx.size())) != cudaSuccess)
+    return fail(MPDG_ERR_NOMEM, "inflow/outflow constraint storage");
+  MPDG_CUDA(cudaMemcpy(op->d_mask_io, flag.data(), op->ndofs, cudaMemcpyHostToDevice));
+  if (!idx.empty())
+    {
+      MPDG_CUDA(cudaMemcpy(op->d_in_idx, idx.data(), sizeof(long long) * idx.size(), cudaMemcpyHostToDevice));
+      MPDG_CUDA(idx_gather(op->d_in_val, values, op->d_in_idx, op->n_inflow, op->stream));
+      MPDG_CUDA(cudaStreamSynchronize(op->stream));
+    }
+  return MPDG_OK;
+}
+
+int64_t
+mpdg_op_n_inflow(const mpdg_op *op)
+{
+  return op ? op->n_inflow : -1;
+}
+
+int
+mpdg_op_set_inflow_outflow_pre_post(mpdg_op *op, int enabled)
+{
+  if (int e = check_op(op))
+    return e;
+  op->inflow_prepost = enabled != 0;
+  return MPDG_OK;
+}
+
+int
+mpdg_op_distribute_inflow(mpdg_op *op, double *x)
+{
+  if (int e = check_op(op))
+    return e;
+  if (!x)
+    return fail(MPDG_ERR_ARG, "null vector passed to mpdg_op_distribute_inflow");
+  MPDG_CUDA(idx_set<double>(x, op->d_in_idx, op->d_in_val, op->n_inflow, 0.0, op->stream));
   return MPDG_OK;
 }
 
@@ -1419,11 +1704,15 @@ mpdg_solve_mixed(mpdg_op *op, double *x, const double *b, const mpdg_mixed_param
       MPDG_CUDA(vec_fill<float>(e32, 0.0f, n, op->stream));
       mpdg_solve_info in{};
       int             rc;
+      // the correction of a residual already close to the outer tolerance needs only the reduction
+      // that reaches it (with a factor 2 to spare), never more than inner_rel_tol asks for
+      const double inner_tol =
+        prm->inexact_last ? std::min(0.5, std::max(prm->inner_rel_tol, 0.5 * tol / res)) : prm->inner_rel_tol;
       if (prm->solver == MPDG_GMRES)
-        rc = gmres_solve<float>(op, e32, r32, invd32, prm->max_inner, 0.0, prm->inner_rel_tol,
+        rc = gmres_solve<float>(op, e32, r32, invd32, prm->max_inner, 0.0, inner_tol,
                                 prm->restart > 0 ? prm->restart : 30, &in, "mi32_");
       else
-        rc = cg_solve<float>(op, e32, r32, invd32, prm->max_inner, 0.0, prm->inner_rel_tol, &in, "mi32_", true, r32);
+        rc = cg_solve<float>(op, e32, r32, invd32, prm->max_inner, 0.0, inner_tol, &in, "mi32_", true, r32);
       if (rc != MPDG_OK && rc != MPDG_ERR_NOT_CONVERGED)
         return rc;
       inner_total += in.iterations;
@@ -1666,6 +1955,10 @@ mpdg_op_create_rhs_and_apply_dirichlet(mpdg_op *op, double *rhs, const double *a
     return fail(MPDG_ERR_NOMEM, "lifting work vectors");
   const GridDesc with_bc = op->grid(); // the constraint set of the operator (dof_idx)
   MPDG_CUDA(vec_copy_constrained<double>(bc, dirichlet_values, with_bc, op->stream));
+  // inflow DoFs enter as additional inhomogeneous constraints (advection_diffusion_operation.cpp:
+  // 262-270 with utilities_matrixfree.hpp:63-68); the apply below runs without the inflow hooks
+  if (op->n_inflow > 0)
+    MPDG_CUDA(idx_set<double>(bc, op->d_in_idx, op->d_in_val, op->n_inflow, 0.0, op->stream));
   const bool saved = op->with_bc;
   op->with_bc      = false; // reset_dof_index(dof_no_bc_idx)
   int rc           = apply<double>(op, (int)OutMode::Set, -1.0, tmp, bc, nullptr, 1);
@@ -1675,6 +1968,8 @@ mpdg_op_create_rhs_and_apply_dirichlet(mpdg_op *op, double *rhs, const double *a
   if (rc != MPDG_OK)
     return rc;
   MPDG_CUDA(vec_axpby<double>(rhs, 1.0, tmp, zero_out ? 0.0 : 1.0, zero_out ? nullptr : rhs, op->ndofs, op->stream));
+  if (op->n_inflow > 0)
+    MPDG_CUDA(idx_set<double>(rhs, op->d_in_idx, nullptr, op->n_inflow, 0.0, op->stream));
   MPDG_CUDA(vec_set_constrained<double>(rhs, 0.0, with_bc, op->stream));
   return MPDG_OK;
 }
@@ -1779,6 +2074,15 @@ mpdg_op_test_set_ticket(mpdg_op *op, unsigned value)
   // stream-ordered: the next launch on the handle's stream finds this counter
   MPDG_CUDA(cudaMemcpyAsync(op->d_sync, &value, sizeof(unsigned), cudaMemcpyHostToDevice, op->stream));
   MPDG_CUDA(cudaStreamSynchronize(op->stream));
+  return MPDG_OK;
+}
+
+int
+mpdg_op_set_cg_variant(mpdg_op *op, int fused)
+{
+  if (int e = check_op(op))
+    return e;
+  op->fused_cg = fused != 0;
   return MPDG_OK;
 }
 

@@ -1,0 +1,757 @@
+// One launch per Jacobi-PCG iteration of the FE_Q(2) heat operator (dealii::SolverCG semantics,
+// include/meltpooldg/linear_algebra/linear_solver.hpp:106-110 with the Jacobi preconditioner of
+// preconditioner_jacobi.hpp:51-56): the vector updates, the preconditioner, the operator apply
+// (source/heat/heat_diffuse_operator.cpp:179-197, tangent :1029-1079) and every dot product of the
+// iteration happen in one sweep over the lattice.
+//
+// Recurrence.  Sweep k reads x_{k-1}, r_{k-1}, p_{k-1}, v_{k-1} = A p_{k-1} and the inverse diagonal
+// d, and with the step lengths a = alpha_{k-1}, b = beta_k of the previous sweep forms, per DoF,
+//   r_k = r_{k-1} - a v_{k-1},  x_k = x_{k-1} + a p_{k-1},  z_k = d r_k,  p_k = z_k + b p_{k-1},
+// then applies v_k = A p_k and sums
+//   S0 = r_k.z_k (rho_k),  S6 = r_k.r_k,  S1 = p_k.v_k,  S2 = z_k.v_k,  S3 = v_k.(d v_k).
+// The last CTA sets alpha_k = S0 / S1 and, since r_{k+1} = r_k - alpha_k v_k,
+//   rho_{k+1} = S0 - 2 alpha_k S2 + alpha_k^2 S3,  beta_{k+1} = rho_{k+1} / S0,
+// so the next sweep can form p_{k+1} without another pass.  |r_k| = sqrt(S6) is the residual that
+// SolverCG checks after iteration k (ReductionControl: |r_k| <= max(abs_tol, rel_tol |r_0|)).  Sweep 0
+// forms z_0, p_0 = z_0 and v_0 only.  Per iteration the sweep reads x, r, p, v, d and writes x, r,
+// p, v: s (9 N + N_c) bytes, against s (13 N + N_c) for separate update / apply / update passes.
+//
+// Tiles.  A CTA owns the lattice points of 32 x TY cells in x, y and a segment of TZ cell layers in
+// z, and marches through the segment layer by layer.  It also computes the cells of one halo layer
+// on its low side in x, y and z (a halo column warp, a halo row warp, a halo cell layer), so every
+// owned point receives all of its cell contributions inside the CTA: no atomics, no inter-CTA
+// waits, and each owned point's update and dot products are done by one thread.  The vectors use a
+// padded layout (x rows of P0 >= n0 + 1 entries, P0 a multiple of 8), so that every lattice plane
+// of a tile is one TMA box (cp.async.bulk.tensor.3d into shared memory, zero fill outside the
+// lattice).  Per layer: the two new lattice planes are staged by TMA while the previous layer's
+// cells compute; each point of a staged plane is updated (owned points also written out) and its
+// p_k goes to a ring of three planes; every thread then applies the fast-diagonalisation cell
+// operator (sumfac.cuh) to its cell's 27 values of p_k; x faces are combined by warp shuffles, y
+// faces through shared memory, z faces carried in registers; owned points of the finished planes
+// get v_k, S2 and S3.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+#include "cgfused.h"
+#include "sumfac.cuh"
+#include "tables.h"
+
+namespace mpdg
+{
+  namespace cgf
+  {
+    constexpr int K = 2, N = 3, NE = 2, NO = 1;
+    constexpr int TX   = 32;  // owned cells per tile in x (lanes)
+    constexpr int SX   = 72;  // staged x points per row: lattice x from 2 cx0 - 4 (TMA x alignment)
+    constexpr int XOFF = 4;   // staged x index of lattice point 2 cx0
+    constexpr int OXW  = 66;  // owned window in x: lattice x from 2 cx0 to 2 cx0 + 65
+    constexpr int NV   = 5;   // staged vectors: r, v, p, x, d
+
+    template <typename T, int TY>
+    struct Shape
+    {
+      static constexpr int RY    = 2 * TY + 3;  // staged rows: lattice y from 2 cy0 - 2
+      static constexpr int PLANE = SX * RY;     // staged points per plane
+      static constexpr int OYW   = 2 * TY + 1;  // owned window rows: lattice y from 2 cy0
+      static constexpr int OPL   = OXW * OYW;   // owned window points per plane
+      static constexpr int NW    = TY + 2;      // warps: TY main rows, halo row, halo column
+      static constexpr int NT    = 32 * NW;
+      static constexpr int NPAIR = (SX / 2 - 2) * RY; // point pairs per plane that cells read
+      // shared memory layout (bytes, 128-byte aligned sections)
+      static constexpr size_t align(size_t b) { return (b + 127) / 128 * 128; }
+      static constexpr size_t STAGE_B = align(sizeof(T) * PLANE);      // one vector, one plane
+      static constexpr size_t O_STAGE = 0;                              // [2 slots][NV] planes
+      static constexpr size_t O_PRING = O_STAGE + 2 * NV * STAGE_B;     // [3] planes of p_k
+      static constexpr size_t O_ZD    = O_PRING + 3 * STAGE_B;          // [3] owned planes of (z, d)
+      static constexpr size_t O_YX    = O_ZD + align(3 * sizeof(T) * 2 * OPL);
+      static constexpr size_t O_HX    = O_YX + align(sizeof(T) * (TY + 1) * 9 * 32);
+      static constexpr size_t O_RED   = O_HX + align(sizeof(T) * (TY + 1) * 9);
+      static constexpr size_t O_BAR   = O_RED + align(sizeof(double) * NW * 5);
+      static constexpr size_t BYTES   = O_BAR + 128;
+    };
+
+    template <typename T>
+    struct Sweep
+    {
+      int           m[3], n[3];
+      int           P0;          // padded x pitch (elements)
+      unsigned      faces;       // Dirichlet faces (bit 2d low, 2d+1 high of dim d)
+      int           tiles_x, tiles_y, TZ, ty;
+      T             alpha_m, cx, cy, cz; // mass coefficient, stiffness geometry factors
+      T             kconst;
+      const T      *kcell;
+      T             we[NE * NE], wo[NO * NO], lam[N];
+      T            *x;           // in place (owned points)
+      T            *r_out, *p_out, *v_out;
+      CGState      *st;
+      double       *part;        // 5 partial sums per tile
+      unsigned     *counter;     // last-CTA ticket (0 between launches)
+      double       *hist;
+      int          *err;
+      unsigned      spin_limit;
+    };
+
+    // ---- TMA / mbarrier primitives (sm_90+ PTX)
+    __device__ __forceinline__ unsigned
+    smem_u32(const void *p)
+    {
+      return (unsigned)__cvta_generic_to_shared(p);
+    }
+    __device__ __forceinline__ void
+    mbar_init(unsigned long long *bar, unsigned count)
+    {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    }
+    __device__ __forceinline__ void
+    mbar_expect_tx(unsigned long long *bar, unsigned bytes)
+    {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                   : "memory");
+    }
+    // bounded wait for the phase with the given parity; false when the limit ran out
+    __device__ __forceinline__ bool
+    mbar_wait(unsigned long long *bar, unsigned parity, unsigned limit)
+    {
+      const unsigned a = smem_u32(bar);
+      for (unsigned it = 0; it < limit; ++it)
+        {
+          unsigned ok;
+          asm volatile("{\n\t.reg .pred p;\n\t"
+                       "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                       "selp.u32 %0, 1, 0, p;\n\t}"
+                       : "=r"(ok)
+                       : "r"(a), "r"(parity)
+                       : "memory");
+          if (ok)
+            return true;
+        }
+      return false;
+    }
+    __device__ __forceinline__ void
+    tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, unsigned long long *bar)
+    {
+      asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                   " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+                   "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+                   : "memory");
+    }
+
+    template <typename T>
+    struct Pair;
+    template <>
+    struct Pair<double>
+    {
+      using V = double2;
+    };
+    template <>
+    struct Pair<float>
+    {
+      using V = float2;
+    };
+
+    __device__ __forceinline__ int
+    control_check(const CGState &st, int step, double value)
+    {
+      if (value <= st.rel_tol * st.res0)
+        return 1;
+      if (value <= st.abs_tol)
+        return 1;
+      if (step >= st.max_it || isnan(value))
+        return 2;
+      return 0;
+    }
+
+    template <typename T, int TY, bool FIRST>
+    __global__ void __launch_bounds__(Shape<T, TY>::NT, sizeof(T) == 4 ? 2 : 1)
+    heat_cg_sweep_kernel(const __grid_constant__ Sweep<T> a, const __grid_constant__ CUtensorMap tm_r,
+                         const __grid_constant__ CUtensorMap tm_v, const __grid_constant__ CUtensorMap tm_p,
+                         const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_d)
+    {
+      using S  = Shape<T, TY>;
+      using PV = typename Pair<T>::V;
+      extern __shared__ __align__(128) unsigned char smem[];
+      T                  *stage = reinterpret_cast<T *>(smem + S::O_STAGE);
+      T                  *pring = reinterpret_cast<T *>(smem + S::O_PRING);
+      PV                 *zd    = reinterpret_cast<PV *>(smem + S::O_ZD);
+      T                  *yx    = reinterpret_cast<T *>(smem + S::O_YX);
+      T                  *hx    = reinterpret_cast<T *>(smem + S::O_HX);
+      double             *red   = reinterpret_cast<double *>(smem + S::O_RED);
+      unsigned long long *bar   = reinterpret_cast<unsigned long long *>(smem + S::O_BAR);
+      __shared__ unsigned s_last;
+
+      if (a.st->done)
+        return;
+      const T   alpha = FIRST ? T(0) : (T)a.st->alpha;
+      const T   beta  = FIRST ? T(0) : (T)a.st->beta;
+      const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+      const int tile = blockIdx.x;
+      const int txi = tile % a.tiles_x, tyi = (tile / a.tiles_x) % a.tiles_y, tzi = tile / (a.tiles_x * a.tiles_y);
+      const int cx0 = TX * txi, cy0 = TY * tyi, cz0 = a.TZ * tzi;
+      const int cz1 = min(cz0 + a.TZ, a.m[2]);
+      const int n0 = a.n[0], n1 = a.n[1], n2 = a.n[2];
+      const int lz_begin = cz0 > 0 ? cz0 - 1 : 0;
+      const int XB = 2 * cx0 - XOFF, Y0 = 2 * cy0 - 2;
+      const long long plane_stride = (long long)a.P0 * n1;
+
+      // thread's cell: main rows (warp < TY), halo row (warp == TY), halo column (warp == TY + 1)
+      const int  role = warp < TY ? 0 : (warp == TY ? 1 : 2);
+      const int  cxl = role == 2 ? -1 : lane, cyl = role == 0 ? warp : (role == 1 ? -1 : lane - 1);
+      const bool active = role != 2 || lane <= TY;
+      const int  cx = cx0 + cxl, cy = cy0 + cyl;
+      const bool vxy = active && cx >= 0 && cx < a.m[0] && cy >= 0 && cy < a.m[1];
+      const int  sxi = XOFF + 2 * cxl, syi = 2 + 2 * cyl; // staged index of the cell's first point
+      const bool last_x = cx == a.m[0] - 1, last_y = cy == a.m[1] - 1;
+
+      double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0}; // S0, S6, S1, S2, S3
+
+      if (tid == 0)
+        {
+          mbar_init(&bar[0], 1);
+          mbar_init(&bar[1], 1);
+          asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+      __syncthreads();
+
+      const unsigned box_bytes = (unsigned)(sizeof(T) * S::PLANE);
+      auto issue = [&](int slot, int L) {
+        // one thread: the plane L of every staged vector into slot
+        T *base = stage + (size_t)slot * NV * (S::STAGE_B / sizeof(T));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bar[slot], (FIRST ? 2u : (unsigned)NV) * box_bytes);
+        const size_t vs = S::STAGE_B / sizeof(T);
+        tma_load_3d(base + 0 * vs, &tm_r, XB, Y0, L, &bar[slot]);
+        if constexpr (!FIRST)
+          {
+            tma_load_3d(base + 1 * vs, &tm_v, XB, Y0, L, &bar[slot]);
+            tma_load_3d(base + 2 * vs, &tm_p, XB, Y0, L, &bar[slot]);
+            tma_load_3d(base + 3 * vs, &tm_x, XB, Y0, L, &bar[slot]);
+          }
+        tma_load_3d(base + 4 * vs, &tm_d, XB, Y0, L, &bar[slot]);
+      };
+      unsigned phase[2] = {0u, 0u};
+      bool     failed   = false;
+
+      const int  Pfirst = 2 * lz_begin, Plast = 2 * cz1; // planes of the segment (with its halo)
+      if (tid == 0)
+        {
+          issue(0, Pfirst);
+          if (Pfirst + 1 <= Plast)
+            issue(1, Pfirst + 1);
+        }
+
+      auto owned_z = [&](int L) { return L >= 2 * cz0 && L < n2 && (L < 2 * cz1 || L == n2 - 1); };
+      auto constrained_xy = [&](int I, int J) {
+        const unsigned f = a.faces;
+        return ((f & 1u) && I == 0) || ((f & 2u) && I == n0 - 1) || ((f & 4u) && J == 0) ||
+               ((f & 8u) && J == n1 - 1);
+      };
+
+      // ---- U stage of plane L: vector updates on every staged point the cells read; owned points
+      // are written back and summed
+      auto update_plane = [&](int L) {
+        const int slot = (L - Pfirst) & 1;
+        if (!mbar_wait(&bar[slot], phase[slot], a.spin_limit))
+          failed = true;
+        phase[slot] ^= 1u;
+        const T *sb   = stage + (size_t)slot * NV * (S::STAGE_B / sizeof(T));
+        const size_t vs = S::STAGE_B / sizeof(T);
+        const T *sr = sb, *sv = sb + vs, *sp = sb + 2 * vs, *sxv = sb + 3 * vs, *sd = sb + 4 * vs;
+        T       *pr = pring + (size_t)(L % 3) * (S::STAGE_B / sizeof(T));
+        PV      *zr = zd + (size_t)(L % 3) * S::OPL;
+        const bool Lin = L >= 0 && L < n2, Lown = owned_z(L);
+        const bool Lcon = ((a.faces & 16u) && L == 0) || ((a.faces & 32u) && L == n2 - 1);
+        for (int q = tid; q < S::NPAIR; q += S::NT)
+          {
+            const int row = q / (SX / 2 - 2), pp = q - row * (SX / 2 - 2);
+            const int xi  = 2 + 2 * pp;           // staged x index (even)
+            const int I   = XB + xi, J = Y0 + row; // lattice coordinates of the pair's first point
+            const int si  = row * SX + xi;
+            const PV  r2  = *reinterpret_cast<const PV *>(sr + si);
+            const PV  d2  = *reinterpret_cast<const PV *>(sd + si);
+            PV        v2{}, p2{}, x2{};
+            if constexpr (!FIRST)
+              {
+                v2 = *reinterpret_cast<const PV *>(sv + si);
+                p2 = *reinterpret_cast<const PV *>(sp + si);
+                x2 = *reinterpret_cast<const PV *>(sxv + si);
+              }
+            const bool Jin = J >= 0 && J < n1;
+            const bool Jown = J >= 2 * cy0 && J < n1 && (J < 2 * cy0 + 2 * TY || J == n1 - 1);
+            T          pn[2], rn[2], zn[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+              {
+                const int  Ih  = I + h;
+                const T    rv  = h ? r2.y : r2.x, dv = h ? d2.y : d2.x;
+                const T    vv  = h ? v2.y : v2.x, pv = h ? p2.y : p2.x;
+                const bool in  = Lin && Jin && Ih >= 0 && Ih < n0;
+                const bool con = Lcon || constrained_xy(Ih, J);
+                const T    r   = FIRST ? rv : rv - alpha * vv;
+                const T    z   = dv * r;
+                rn[h]          = r;
+                zn[h]          = (in && !con) ? z : T(0);
+                pn[h]          = (in && !con) ? (FIRST ? z : z + beta * pv) : T(0);
+              }
+            *reinterpret_cast<PV *>(pr + si) = PV{pn[0], pn[1]};
+            if (Lown && Jown)
+              {
+                const long long g = (long long)L * plane_stride + (long long)J * a.P0 + I;
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                  {
+                    const int Ih = I + h;
+                    if (!(Ih >= 2 * cx0 && Ih < n0 && (Ih < 2 * cx0 + 2 * TX || Ih == n0 - 1)))
+                      continue;
+                    const T pv = h ? p2.y : p2.x, xv = h ? x2.y : x2.x, dv = h ? d2.y : d2.x;
+                    if constexpr (!FIRST)
+                      {
+                        a.x[g + h]     = xv + alpha * pv;
+                        a.r_out[g + h] = rn[h];
+                      }
+                    a.p_out[g + h] = pn[h];
+                    zr[(J - 2 * cy0) * OXW + (Ih - 2 * cx0)] = PV{zn[h], dv};
+                    const double rd = (double)rn[h];
+                    acc[0] += rd * (double)zn[h];
+                    acc[1] += rd * rd;
+                  }
+              }
+          }
+      };
+
+      auto refill = [&](int L_done) {
+        // the slot of plane L_done is free once every thread passed the barrier before this call
+        const int Ln = L_done + 2;
+        if (tid == 0 && Ln <= Plast)
+          issue((L_done - Pfirst) & 1, Ln);
+      };
+
+      update_plane(Pfirst);
+      __syncthreads();
+      refill(Pfirst);
+
+      // fast-diagonalisation tables (k = 2: even block 2 x 2, odd block 1 x 1)
+      T we[NE * NE], wo[NO * NO], lam[N];
+#pragma unroll
+      for (int i = 0; i < NE * NE; ++i)
+        we[i] = a.we[i];
+      wo[0] = a.wo[0];
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+        lam[i] = a.lam[i];
+
+      T carry[N * N];
+#pragma unroll
+      for (int q = 0; q < N * N; ++q)
+        carry[q] = T(0);
+
+      for (int lz = lz_begin; lz < cz1; ++lz)
+        {
+          const bool halo_layer = lz < cz0;
+          T          kc         = T(0);
+          if (vxy)
+            kc = a.kcell ? a.kcell[(long long)cx + (long long)a.m[0] * ((long long)cy + (long long)a.m[1] * lz)]
+                         : a.kconst;
+          update_plane(2 * lz + 1);
+          __syncthreads();
+          refill(2 * lz + 1);
+          update_plane(2 * lz + 2);
+          __syncthreads();
+          refill(2 * lz + 2);
+
+          // ---- cell stage: u = A_c p_c for the thread's cell
+          T u[N * N * N];
+#pragma unroll
+          for (int l = 0; l < N; ++l)
+            {
+              const T *pl = pring + (size_t)((2 * lz + l) % 3) * (S::STAGE_B / sizeof(T));
+#pragma unroll
+              for (int j = 0; j < N; ++j)
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                  u[(l * N + j) * N + i] = vxy ? pl[(syi + j) * SX + sxi + i] : T(0);
+            }
+          {
+            const T kcx = kc * a.cx, kcy = kc * a.cy, kcz = kc * a.cz, am = a.alpha_m;
+            xy_planes<T, N, N, true>(u, we, wo);
+#pragma unroll
+            for (int q = 0; q < N * N; ++q)
+              fwd_line<T, N, N * N>(u, q, we, wo);
+            T form = T(0);
+#pragma unroll
+            for (int c = 0; c < N; ++c)
+              {
+                const T tz = fma(kcz, lam[c], am);
+#pragma unroll
+                for (int b = 0; b < N; ++b)
+                  {
+                    const T tyz = fma(kcy, lam[b], tz);
+#pragma unroll
+                    for (int aa = 0; aa < N; ++aa)
+                      {
+                        const T d = fma(kcx, lam[aa], tyz);
+                        T      &v = u[(c * N + b) * N + aa];
+                        form      = fma(d * v, v, form);
+                        v *= d;
+                      }
+                  }
+              }
+            if (role == 0 && !halo_layer && vxy)
+              acc[2] += (double)form;
+#pragma unroll
+            for (int q = 0; q < N * N; ++q)
+              bwd_line<T, N, N * N>(u, q, we, wo);
+            xy_planes<T, N, N, false>(u, we, wo);
+          }
+          // ---- x faces: the halo column hands its x = 2 face to lane 0 of every other row
+          if (role == 2 && active)
+#pragma unroll
+            for (int q = 0; q < N * N; ++q)
+              hx[lane * 9 + q] = u[q * N + K];
+          __syncthreads();
+          if (role != 2)
+            {
+              const int hrow = role == 0 ? warp + 1 : 0; // halo column lane of this row
+#pragma unroll
+              for (int q = 0; q < N * N; ++q)
+                {
+                  const T v = __shfl_up_sync(0xffffffffu, u[q * N + K], 1);
+                  u[q * N] += lane > 0 ? v : hx[hrow * 9 + q];
+                }
+              // y faces: main rows and the halo row hand their y = 2 face to the next row
+              const int slot = role == 0 ? warp : TY;
+#pragma unroll
+              for (int l = 0; l < N; ++l)
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                  yx[((slot * N + l) * N + i) * 32 + lane] = u[(l * N + K) * N + i];
+            }
+          __syncthreads();
+          if (role == 0)
+            {
+              const int from = warp == 0 ? TY : warp - 1;
+#pragma unroll
+              for (int l = 0; l < N; ++l)
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                  u[(l * N) * N + i] += yx[((from * N + l) * N + i) * 32 + lane];
+              // z faces: add the carried face, carry this layer's z = 2 face
+#pragma unroll
+              for (int q = 0; q < N * N; ++q)
+                {
+                  u[q] += carry[q];
+                  carry[q] = u[K * N * N + q];
+                }
+              // ---- owned points of the finished planes: v_k, S2, S3
+              if (!halo_layer && vxy)
+                {
+                  const int nl = lz == a.m[2] - 1 ? 3 : 2;
+                  for (int l = 0; l < nl; ++l)
+                    {
+                      const int  L    = 2 * lz + l;
+                      const PV  *zl   = zd + (size_t)(L % 3) * S::OPL;
+                      const bool Lcon = ((a.faces & 16u) && L == 0) || ((a.faces & 32u) && L == n2 - 1);
+#pragma unroll
+                      for (int j = 0; j < N; ++j)
+                        {
+                          if (j == K && !last_y)
+                            continue;
+                          const int J = 2 * cy + j;
+                          T        *vrow = a.v_out + (long long)L * plane_stride + (long long)J * a.P0;
+                          const PV *zrow = zl + (J - 2 * cy0) * OXW;
+                          const bool Jcon = Lcon || ((a.faces & 4u) && J == 0) || ((a.faces & 8u) && J == n1 - 1);
+                          T          vv[N];
+                          double     s2 = 0.0, s3 = 0.0;
+#pragma unroll
+                          for (int i = 0; i < N; ++i)
+                            {
+                              const int  I   = 2 * cx + i;
+                              const bool con = Jcon || ((a.faces & 1u) && I == 0) || ((a.faces & 2u) && I == n0 - 1);
+                              vv[i]          = con ? T(0) : u[(l * N + j) * N + i];
+                              if (i < K || last_x)
+                                {
+                                  const PV   zz = zrow[I - 2 * cx0];
+                                  const double v = (double)vv[i];
+                                  s2 += (double)zz.x * v;
+                                  s3 += (double)zz.y * v * v;
+                                }
+                            }
+                          acc[3] += s2;
+                          acc[4] += s3;
+                          *reinterpret_cast<PV *>(vrow + 2 * cx) = PV{vv[0], vv[1]};
+                          if (last_x)
+                            vrow[2 * cx + 2] = vv[2];
+                        }
+                    }
+                }
+            }
+          __syncthreads();
+        }
+
+      // ---- CTA sums in a fixed order, then the last CTA adds the tiles in order and steps the state
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        {
+          double v = acc[k];
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1)
+            v += __shfl_down_sync(0xffffffffu, v, off);
+          if (lane == 0)
+            red[warp * 5 + k] = v;
+        }
+      __syncthreads();
+      const int ntiles = gridDim.x;
+      if (tid < 5)
+        {
+          double t = 0.0;
+          for (int w = 0; w < S::NW; ++w)
+            t += red[w * 5 + tid];
+          a.part[(size_t)tid * ntiles + tile] = t;
+        }
+      if (failed)
+        atomicExch(a.err, 3);
+      __syncthreads();
+      if (tid == 0)
+        {
+          __threadfence();
+          s_last = atomicAdd(a.counter, 1u) == (unsigned)ntiles - 1 ? 1u : 0u;
+        }
+      __syncthreads();
+      if (!s_last)
+        return;
+      __threadfence();
+      for (int k = 0; k < 5; ++k)
+        {
+          double t = 0.0;
+          for (int i = tid; i < ntiles; i += S::NT)
+            t += __ldcg(a.part + (size_t)k * ntiles + i);
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1)
+            t += __shfl_down_sync(0xffffffffu, t, off);
+          if (lane == 0)
+            red[warp * 5 + k] = t;
+        }
+      __syncthreads();
+      if (tid == 0)
+        {
+          double s[5];
+          for (int k = 0; k < 5; ++k)
+            {
+              s[k] = 0.0;
+              for (int w = 0; w < S::NW; ++w)
+                s[k] += red[w * 5 + k];
+            }
+          CGState    &st  = *a.st;
+          const double res = sqrt(s[1]);
+          int          it  = 0;
+          if (FIRST)
+            {
+              st.res0 = res;
+              st.tol  = fmax(st.abs_tol, st.rel_tol * res);
+            }
+          else
+            it = st.it + 1;
+          st.it  = it;
+          st.res = res;
+          if (a.hist)
+            a.hist[it] = res;
+          const double rho   = s[0];
+          const double alph  = rho / s[2];
+          const double rho_n = rho - 2.0 * alph * s[3] + alph * alph * s[4];
+          st.rho             = rho;
+          st.alpha           = alph;
+          st.beta            = rho_n / rho;
+          st.done            = control_check(st, it, res);
+          *a.counter         = 0u;
+          __threadfence();
+        }
+    }
+  } // namespace cgf
+
+  // ------------------------------------------------------------------------------------------
+  // host side
+
+  namespace
+  {
+    PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+    {
+      static std::once_flag                    once;
+      static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+      std::call_once(once, [] {
+        void                          *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+          fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+      });
+      return fn;
+    }
+  } // namespace
+
+  template <typename T>
+  int
+  FusedCG<T>::make_map(CUtensorMap *map, const T *base) const
+  {
+    auto fn = encode_fn();
+    if (!fn)
+      return 1;
+    const int       TY   = sizeof(T) == 8 ? FUSED_TY_F64 : FUSED_TY_F32;
+    cuuint64_t      dims[3]    = {(cuuint64_t)n[0], (cuuint64_t)n[1], (cuuint64_t)n[2]};
+    cuuint64_t      strides[2] = {(cuuint64_t)P0 * sizeof(T), (cuuint64_t)P0 * n[1] * sizeof(T)};
+    cuuint32_t      box[3]     = {(cuuint32_t)cgf::SX, (cuuint32_t)(2 * TY + 3), 1u};
+    cuuint32_t      estr[3]    = {1u, 1u, 1u};
+    const CUresult  r = fn(map, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                          const_cast<T *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : 2;
+  }
+
+  template <typename T>
+  size_t
+  FusedCG<T>::smem_bytes()
+  {
+    return sizeof(T) == 8 ? cgf::Shape<double, FUSED_TY_F64>::BYTES : cgf::Shape<float, FUSED_TY_F32>::BYTES;
+  }
+
+  template <typename T>
+  int
+  FusedCG<T>::threads()
+  {
+    return sizeof(T) == 8 ? cgf::Shape<double, FUSED_TY_F64>::NT : cgf::Shape<float, FUSED_TY_F32>::NT;
+  }
+
+  template <typename T>
+  void
+  FusedCG<T>::plan(int sm_count)
+  {
+    const int TY = sizeof(T) == 8 ? FUSED_TY_F64 : FUSED_TY_F32;
+    tiles_x      = (m[0] + cgf::TX - 1) / cgf::TX;
+    tiles_y      = (m[1] + TY - 1) / TY;
+    // CTAs resident per SM from the shared memory footprint (227 KB usable per CTA, 228 KB per SM)
+    const int per_sm = std::max(1, (int)(233472 / (smem_bytes() + 1024)));
+    const long long slots = (long long)sm_count * per_sm;
+    // segment length: the fewest waves of equal tiles, weighted by the halo layer each tile adds
+    double best = 1e300;
+    for (int tz = 2; tz <= 64; ++tz)
+      {
+        const long long segs  = (m[2] + tz - 1) / tz;
+        const long long tiles = (long long)tiles_x * tiles_y * segs;
+        const double    waves = std::ceil((double)tiles / (double)slots);
+        const double    cost  = waves * (std::min(tz, m[2]) + 1.5);
+        if (cost < best - 1e-9)
+          {
+            best = cost;
+            TZ   = tz;
+          }
+      }
+    segs   = (m[2] + TZ - 1) / TZ;
+    ntiles = tiles_x * tiles_y * segs;
+  }
+
+  template <typename T>
+  cudaError_t
+  FusedCG<T>::sweep(bool first, const CUtensorMap &r_in, const CUtensorMap &v_in, const CUtensorMap &p_in,
+                    const CUtensorMap &x, const CUtensorMap &d, T *x_ptr, T *r_out, T *p_out, T *v_out,
+                    CGState *st, double *part, unsigned *counter, double *hist, int *err, unsigned spin_limit,
+                    cudaStream_t s) const
+  {
+    constexpr int TY = sizeof(T) == 8 ? FUSED_TY_F64 : FUSED_TY_F32;
+    cgf::Sweep<T> a{};
+    for (int i = 0; i < 3; ++i)
+      {
+        a.m[i] = m[i];
+        a.n[i] = n[i];
+      }
+    a.P0      = P0;
+    a.faces   = faces;
+    a.tiles_x = tiles_x;
+    a.tiles_y = tiles_y;
+    a.TZ      = TZ;
+    a.ty      = TY;
+    a.alpha_m = (T)mass_coef;
+    a.cx      = (T)geo[0];
+    a.cy      = (T)geo[1];
+    a.cz      = (T)geo[2];
+    a.kconst  = (T)kconst;
+    a.kcell   = kcell;
+    const Tables1D &t = tables(2);
+    for (int i = 0; i < cgf::NE * cgf::NE; ++i)
+      a.we[i] = (T)t.WE[i];
+    a.wo[0] = (T)t.WO[0];
+    for (int i = 0; i < cgf::N; ++i)
+      a.lam[i] = (T)t.lam[i];
+    a.x          = x_ptr;
+    a.r_out      = r_out;
+    a.p_out      = p_out;
+    a.v_out      = v_out;
+    a.st         = st;
+    a.part       = part;
+    a.counter    = counter;
+    a.hist       = hist;
+    a.err        = err;
+    a.spin_limit = spin_limit;
+    const size_t bytes = smem_bytes();
+    if (first)
+      {
+        auto k = cgf::heat_cg_sweep_kernel<T, TY, true>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess)
+          return e;
+        k<<<ntiles, threads(), bytes, s>>>(a, r_in, v_in, p_in, x, d);
+      }
+    else
+      {
+        auto k = cgf::heat_cg_sweep_kernel<T, TY, false>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess)
+          return e;
+        k<<<ntiles, threads(), bytes, s>>>(a, r_in, v_in, p_in, x, d);
+      }
+    return cudaGetLastError();
+  }
+
+  // padded layout conversions: rows of n0 entries <-> rows of P0 entries (padding zero)
+  template <typename Td, typename Ts>
+  __global__ void
+  pad_rows_kernel(Td *dst, const Ts *src, int n0, int P0, long long rows)
+  {
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x)
+      for (int i = threadIdx.x; i < P0; i += blockDim.x)
+        dst[row * P0 + i] = i < n0 ? (Td)src[row * n0 + i] : Td(0);
+  }
+  template <typename Td, typename Ts>
+  __global__ void
+  unpad_rows_kernel(Td *dst, const Ts *src, int n0, int P0, long long rows)
+  {
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x)
+      for (int i = threadIdx.x; i < n0; i += blockDim.x)
+        dst[row * n0 + i] = (Td)src[row * P0 + i];
+  }
+
+  template <typename Td, typename Ts>
+  cudaError_t
+  pad_rows(Td *dst, const Ts *src, int n0, int P0, long long rows, cudaStream_t s)
+  {
+    pad_rows_kernel<Td, Ts><<<(int)std::min<long long>(rows, 148LL * 16), 256, 0, s>>>(dst, src, n0, P0, rows);
+    return cudaGetLastError();
+  }
+  template <typename Td, typename Ts>
+  cudaError_t
+  unpad_rows(Td *dst, const Ts *src, int n0, int P0, long long rows, cudaStream_t s)
+  {
+    unpad_rows_kernel<Td, Ts><<<(int)std::min<long long>(rows, 148LL * 16), 256, 0, s>>>(dst, src, n0, P0, rows);
+    return cudaGetLastError();
+  }
+
+  template struct FusedCG<double>;
+  template struct FusedCG<float>;
+  template cudaError_t pad_rows<double, double>(double *, const double *, int, int, long long, cudaStream_t);
+  template cudaError_t pad_rows<float, float>(float *, const float *, int, int, long long, cudaStream_t);
+  template cudaError_t unpad_rows<double, double>(double *, const double *, int, int, long long, cudaStream_t);
+  template cudaError_t unpad_rows<float, float>(float *, const float *, int, int, long long, cudaStream_t);
+} // namespace mpdg

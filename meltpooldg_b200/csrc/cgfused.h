@@ -1,0 +1,51 @@
+// Host interface of the one-launch-per-iteration Jacobi-PCG of the FE_Q(2) heat operator
+// (cgfused.cu).  Internal to the library, not part of the C ABI.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "kernels.h"
+
+namespace mpdg
+{
+#ifndef MPDG_FUSED_TY_F64
+#define MPDG_FUSED_TY_F64 8
+#endif
+#ifndef MPDG_FUSED_TY_F32
+#define MPDG_FUSED_TY_F32 8
+#endif
+  constexpr int FUSED_TY_F64 = MPDG_FUSED_TY_F64; // owned cell rows per tile (FP64)
+  constexpr int FUSED_TY_F32 = MPDG_FUSED_TY_F32; // owned cell rows per tile (FP32)
+
+  // Problem description and tiling of the fused sweep; vectors in the padded layout (x rows of P0
+  // entries, P0 = n0 rounded up to a multiple of 8 and > n0).
+  template <typename T>
+  struct FusedCG
+  {
+    int      m[3]{}, n[3]{};
+    int      P0 = 0;
+    unsigned faces = 0;
+    double   mass_coef = 0.0, geo[3]{}, kconst = 1.0;
+    const T *kcell = nullptr;
+    int      tiles_x = 0, tiles_y = 0, TZ = 0, segs = 0, ntiles = 0;
+
+    static int padded_pitch(int n0) { return (n0 + 8) / 8 * 8; }
+    long long  padded_len() const { return (long long)P0 * n[1] * n[2]; }
+    void       plan(int sm_count);
+    int        make_map(CUtensorMap *map, const T *base) const;
+    static size_t smem_bytes();
+    static int    threads();
+    cudaError_t   sweep(bool first, const CUtensorMap &r_in, const CUtensorMap &v_in, const CUtensorMap &p_in,
+                        const CUtensorMap &x, const CUtensorMap &d, T *x_ptr, T *r_out, T *p_out, T *v_out,
+                        CGState *st, double *part, unsigned *counter, double *hist, int *err, unsigned spin_limit,
+                        cudaStream_t s) const;
+  };
+
+  template <typename Td, typename Ts>
+  cudaError_t pad_rows(Td *dst, const Ts *src, int n0, int P0, long long rows, cudaStream_t s);
+  template <typename Td, typename Ts>
+  cudaError_t unpad_rows(Td *dst, const Ts *src, int n0, int P0, long long rows, cudaStream_t s);
+} // namespace mpdg

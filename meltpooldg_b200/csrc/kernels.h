@@ -277,4 +277,10 @@ namespace mpdg
   // dst = src on constrained DoFs, other entries untouched
   template <typename T>
   cudaError_t vec_distribute_constrained(T *dst, const T *src, const GridDesc &g, cudaStream_t s);
+  // dst[idx[k]] += scale src[idx[k]];  dst[idx[k]] = vals ? vals[k] : fill;  out[k] = src[idx[k]]
+  template <typename T>
+  cudaError_t idx_add_scaled(T *dst, const T *src, const long long *idx, long long n, double scale, cudaStream_t s);
+  template <typename T>
+  cudaError_t idx_set(T *dst, const long long *idx, const double *vals, long long n, T fill, cudaStream_t s);
+  cudaError_t idx_gather(double *out, const double *src, const long long *idx, long long n, cudaStream_t s);
 } // namespace mpdg

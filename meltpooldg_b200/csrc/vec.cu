@@ -743,7 +743,61 @@ namespace mpdg
     return cudaGetLastError();
   }
 
+  // ---- indexed operations over a DoF list (inflow rows of the advection operator)
+  template <typename T>
+  __global__ void
+  idx_add_scaled_kernel(T *dst, const T *src, const long long *idx, long long n, T scale)
+  {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+      {
+        const long long i = idx[k];
+        dst[i] += scale * src[i];
+      }
+  }
+  template <typename T>
+  __global__ void
+  idx_set_kernel(T *dst, const long long *idx, const double *vals, long long n, T fill)
+  {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+      dst[idx[k]] = vals ? (T)vals[k] : fill;
+  }
+  __global__ void
+  idx_gather_kernel(double *out, const double *src, const long long *idx, long long n)
+  {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+      out[k] = src[idx[k]];
+  }
+
+  template <typename T>
+  cudaError_t
+  idx_add_scaled(T *dst, const T *src, const long long *idx, long long n, double scale, cudaStream_t s)
+  {
+    if (n <= 0)
+      return cudaSuccess;
+    idx_add_scaled_kernel<T><<<stream_blocks(n), 256, 0, s>>>(dst, src, idx, n, (T)scale);
+    return cudaGetLastError();
+  }
+  template <typename T>
+  cudaError_t
+  idx_set(T *dst, const long long *idx, const double *vals, long long n, T fill, cudaStream_t s)
+  {
+    if (n <= 0)
+      return cudaSuccess;
+    idx_set_kernel<T><<<stream_blocks(n), 256, 0, s>>>(dst, idx, vals, n, fill);
+    return cudaGetLastError();
+  }
+  cudaError_t
+  idx_gather(double *out, const double *src, const long long *idx, long long n, cudaStream_t s)
+  {
+    if (n <= 0)
+      return cudaSuccess;
+    idx_gather_kernel<<<stream_blocks(n), 256, 0, s>>>(out, src, idx, n);
+    return cudaGetLastError();
+  }
+
 #define MPDG_INST(T)                                                                                         \
+  template cudaError_t idx_add_scaled<T>(T *, const T *, const long long *, long long, double, cudaStream_t); \
+  template cudaError_t idx_set<T>(T *, const long long *, const double *, long long, T, cudaStream_t);       \
   template cudaError_t cg_init<T>(const T *, const T *, T *, CGState *, double *, Reducer, long long, cudaStream_t); \
   template cudaError_t cg_update_p<T>(const T *, const T *, T *, const CGState *, long long, cudaStream_t);      \
   template cudaError_t cg_alpha<T>(const T *, const T *, CGState *, Reducer, long long, cudaStream_t);          \

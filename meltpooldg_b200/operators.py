@@ -263,6 +263,22 @@ class AdvectionDiffusionOperator(OperatorMatrixFree):
             raise ValueError("convection stabilization type must be 'none' or 'SUPG'")
         check(lib().mpdg_op_set_supg(self._h, 1 if type == "SUPG" else 0, float(coefficient)))
 
+    def set_inflow_outflow_bc(self, faces: int, values) -> int:
+        """Inflow/outflow condition on the box faces in `faces` (bit 2d low / 2d+1 high face of dim
+        d): AdvectionDiffusionOperation::create_inflow_outflow_constraints and the operator's
+        set_inflow_outflow_bc (source/level_set/advection_diffusion_operation.cpp:369-499).  values:
+        device vector with the condition's function at every DoF.  Returns the number of inflow
+        DoFs; faces == 0 removes the condition."""
+        check(lib().mpdg_op_set_inflow_outflow(self._h, int(faces), self._v(values) if faces else None))
+        return int(lib().mpdg_op_n_inflow(self._h))
+
+    def set_apply_inflow_outflow_constraints_pre_post_matrix_free(self, enabled: bool) -> None:
+        check(lib().mpdg_op_set_inflow_outflow_pre_post(self._h, 1 if enabled else 0))
+
+    def distribute_inflow(self, x) -> None:
+        """x = prescribed values on the inflow DoFs (advection_diffusion_operation.cpp:288-296)."""
+        check(lib().mpdg_op_distribute_inflow(self._h, self._v(x)))
+
 
 class OlssonOperator(OperatorMatrixFree):
     """Conservative level-set reinitialisation operator (source/level_set/olsson_CG_operator.cpp):
@@ -338,9 +354,10 @@ class LinearSolver:
     @staticmethod
     def solve_mixed(op: HeatDiffuseOperator, solution, rhs, outer_rel_tol: float = 1e-8,
                     inner_rel_tol: float = 1e-4, max_outer: int = 50, max_inner: int = 10000,
-                    solver: str = "CG", restart: int = 30) -> SolveStats:
+                    solver: str = "CG", restart: int = 30, inexact_last: bool = False) -> SolveStats:
         p = L.MixedParams()
         p.outer_rel_tol, p.inner_rel_tol = float(outer_rel_tol), float(inner_rel_tol)
+        p.inexact_last = 1 if inexact_last else 0
         p.max_outer, p.max_inner = int(max_outer), int(max_inner)
         p.solver = L.MPDG_CG if solver.upper() == "CG" else L.MPDG_GMRES
         p.restart = int(restart)

@@ -67,6 +67,7 @@ typedef struct orc_op
   double         theta;   // advection: one-step-theta weight
   double         eps;     // advection: diffusivity
   double         vel[12]; // advection: v(x) = vel[0..2] + G x, G = vel[3..11] row-major
+  const uint8_t *imask;   // advection: inflow DoFs with identity rows (NULL: none), see apply_impl
 } orc_op;
 
 } // extern "C"
@@ -421,6 +422,9 @@ namespace
       }
   }
 
+  // Inflow DoFs (imask) of the advection operator follow AdvectionDiffusionOperator::do_pre_vmult /
+  // do_post_vmult (source/level_set/advection_diffusion_operator.cpp:543-578): src reads 0 there,
+  // and the row is the identity (vmult: dst_i = src_i; the add form: dst_i += src_i).
   template <int N>
   void
   apply_impl(const orc_op &op, const double *src, double *dst, bool zero_dst)
@@ -429,18 +433,23 @@ namespace
     const Basis1D b = make_basis(op.degree);
     if (zero_dst)
       std::memset(dst, 0, sizeof(double) * L.ndofs);
+    auto skip = [&](int64_t i) { return (op.cmask && op.cmask[i]) || (op.imask && op.imask[i]); };
     colored_cell_loop(op, [&](int cx, int cy, int cz, int64_t cell) {
       int64_t idx[N * N * N];
       double  u[N * N * N], out[N * N * N];
       cell_dofs(op, L, cx, cy, cz, idx);
       for (int i = 0; i < N * N * N; ++i)
-        u[i] = (op.cmask && op.cmask[idx[i]]) ? 0.0 : src[idx[i]];
+        u[i] = skip(idx[i]) ? 0.0 : src[idx[i]];
       const CellGeom g = cell_geom(op, L, cx, cy, cz);
       local_operator<N>(op, b, g, cell_k(op, cell), 0, u, nullptr, nullptr, out);
       for (int i = 0; i < N * N * N; ++i)
-        if (!(op.cmask && op.cmask[idx[i]]))
+        if (!skip(idx[i]))
           dst[idx[i]] += out[i];
     });
+    if (op.imask)
+      for (int64_t i = 0; i < L.ndofs; ++i)
+        if (op.imask[i] && !(op.cmask && op.cmask[i]))
+          dst[i] += src[i];
   }
 
   template <int N>
@@ -680,6 +689,11 @@ orc_inverse_diagonal(const orc_op *op, double *diag)
       linf = std::max(1.0, linf);
       for (int64_t i = 0; i < L.ndofs; ++i)
         diag[i] = (std::abs(diag[i]) > 1.0e-14 * linf) ? 1.0 / diag[i] : 1.0;
+      // inflow rows are identity rows (advection_diffusion_operator.cpp:444-445)
+      if (op->imask)
+        for (int64_t i = 0; i < L.ndofs; ++i)
+          if (op->imask[i])
+            diag[i] = 1.0;
     }
   return 0;
 }

@@ -51,6 +51,7 @@ class OrcOp(C.Structure):
         ("theta", C.c_double),
         ("eps", C.c_double),
         ("vel", C.c_double * 12),
+        ("imask", C.c_void_p),
     ]
 
 
@@ -212,6 +213,7 @@ class Operator:
     theta: float = 1.0
     eps: float = 0.0
     vel: Sequence[float] = field(default_factory=lambda: [0.0] * 12)
+    imask: Optional[np.ndarray] = None  # advection inflow DoFs: identity rows (do_pre/post_vmult)
 
     def _struct(self) -> OrcOp:
         s = OrcOp()
@@ -237,6 +239,12 @@ class Operator:
         s.theta, s.eps = self.theta, self.eps
         for i in range(12):
             s.vel[i] = float(self.vel[i])
+        if self.imask is not None:
+            self._im = np.ascontiguousarray(self.imask, dtype=np.uint8)
+            assert self._im.size == self.mesh.ndofs
+            s.imask = self._im.ctypes.data
+        else:
+            s.imask = None
         return s
 
     def with_(self, **kw) -> "Operator":
@@ -288,6 +296,31 @@ class Operator:
         s = self._struct()
         u = np.ascontiguousarray(u, dtype=np.float64)
         return lib().orc_l2_norm(C.byref(s), _ptr(u))
+
+
+def inflow_dofs(mesh: Mesh, vel, faces: int = 63) -> np.ndarray:
+    """uint8 flags of the inflow DoFs of an inflow/outflow condition on the box faces in `faces`
+    (bit 2d low / 2d+1 high face of dim d): every support point of such a face where the outward
+    normal n and the velocity v (affine, vel[0..2] + G x) satisfy n . v <= 0, as
+    AdvectionDiffusionOperation::create_inflow_outflow_constraints
+    (source/level_set/advection_diffusion_operation.cpp:369-499) collects them face by face."""
+    X, Y, Z = mesh.coords()
+    P = np.stack([X, Y, Z])
+    v = np.asarray(vel[:3], dtype=np.float64)[:, None] + np.asarray(vel[3:12], dtype=np.float64).reshape(3, 3) @ P
+    nx, ny, nz = mesh.n
+    I = np.tile(np.arange(nx), ny * nz)
+    J = np.tile(np.repeat(np.arange(ny), nx), nz)
+    K = np.repeat(np.arange(nz), nx * ny)
+    lat = (I, J, K)
+    flags = np.zeros(mesh.ndofs, dtype=np.uint8)
+    for f in range(6):
+        if not (faces >> f) & 1:
+            continue
+        d, side = f // 2, f % 2
+        on = lat[d] == (mesh.n[d] - 1 if side else 0)
+        nv = v[d] if side else -v[d]
+        flags[on & (nv <= 0.0)] = 1
+    return flags
 
 
 class NoConvergence(RuntimeError):

@@ -68,3 +68,24 @@ def vortex(dim: int):
     mask = mask.ravel()
     phi[mask == 1] = -1.0
     return mesh, phi, mask, vel
+
+
+def vortex_inflow(dim: int):
+    """applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf_inflow_outflow[_3d].json:
+    the vortex case with the inflow/outflow condition (value -1) on every boundary face of the
+    domain (advection_diffusion_vortex.hpp:159-166 attaches it to both boundary ids), no Dirichlet
+    constraints, so the initial field keeps its interpolated boundary values.  Returns the mesh, the
+    initial field, the velocity and the box faces that carry the condition (the z faces of the
+    depth-1 extrusion are not boundaries of the 2-D problem)."""
+    mesh, _, _, vel = vortex(dim)
+    X, Y, Z = mesh.coords()
+    if dim == 3:
+        sd = 0.25 - np.sqrt(X ** 2 + Y ** 2 + (Z - 0.5) ** 2)
+        eps = 0.5 * (0.25 * np.sqrt(3)) / np.sqrt(3)
+        faces = 0b111111
+    else:
+        h = 2.0 / 32
+        sd = 0.25 - np.sqrt(X ** 2 + (Y - 0.5) ** 2)
+        eps = 0.5 * (h * np.sqrt(2)) / np.sqrt(2)
+        faces = 0b001111
+    return mesh, np.tanh(sd / (2 * eps)), vel, faces

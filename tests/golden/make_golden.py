@@ -8,6 +8,8 @@ Sources (paths inside the MeltPoolDG tree):
       unidirectional_heat_transfer.mpirun=4.output   (Newton "||solution||" per step)
   applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf_3d.mpirun=4.output
   applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf.mpirun=4.output
+  applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf_inflow_outflow{,_3d}.mpirun=4.output
+  applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf_supg.mpirun=4.output
       ("|| advected field ||L2" per step)
 """
 import json
@@ -28,6 +30,15 @@ CASES = {
         r"\|\| advected field \|\|L2 = ([0-9.eE+-]+)"),
     "advdiff_vortex_mf_2d_q1": (
         "applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf.mpirun=4.output",
+        r"\|\| advected field \|\|L2 = ([0-9.eE+-]+)"),
+    "advdiff_vortex_mf_inflow_outflow_3d_q1": (
+        "applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf_inflow_outflow_3d.mpirun=4.output",
+        r"\|\| advected field \|\|L2 = ([0-9.eE+-]+)"),
+    "advdiff_vortex_mf_inflow_outflow_2d_q1": (
+        "applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf_inflow_outflow.mpirun=4.output",
+        r"\|\| advected field \|\|L2 = ([0-9.eE+-]+)"),
+    "advdiff_vortex_supg_2d_q1": (
+        "applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf_supg.mpirun=4.output",
         r"\|\| advected field \|\|L2 = ([0-9.eE+-]+)"),
 }
 

@@ -4,8 +4,8 @@ import os
 
 import numpy as np
 
-from oracle.oracle import Operator, solve
-from tests.cases import heat_unidirectional, vortex
+from oracle.oracle import Operator, inflow_dofs, solve
+from tests.cases import heat_unidirectional, vortex, vortex_inflow
 
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_logs.json")))
 
@@ -49,11 +49,52 @@ def _vortex_norms(dim):
     return np.array(out)
 
 
+# The logs print 11 digits, but the reference computes the norm from per-cell values stored in
+# single precision: MeltPoolDG::VectorTools::compute_global_error_norm collects
+# dealii::VectorTools::integrate_difference into a dealii::Vector<float>
+# (source/utilities/vector_tools.cpp:151-165) and dealii::VectorTools::compute_global_error sums
+# their squares in that vector's type.  Its last printed digits therefore carry float rounding of a
+# few 1e-8 relative, in an order set by the MPI partition and the summation tree of the machine that
+# wrote the logs; the restatement computes the norm in double and agrees to that float noise.
+FLOAT_NORM_NOISE = 5e-8
+
+
 def test_vortex_logs():
-    """Reproduced to 7 significant digits (the logs print 11); the remaining 4e-8 relative gap is
-    not a solver effect: a dense direct solve of the same discrete system agrees with GMRES here
-    to 11 digits."""
+    """Reproduced to the float rounding of the reference's norm (see FLOAT_NORM_NOISE); a dense
+    direct solve of the same discrete system agrees with GMRES here to 11 digits, so the solution
+    itself is not the source of the remaining difference."""
     for dim, key in ((3, "advdiff_vortex_mf_3d_q1"), (2, "advdiff_vortex_mf_2d_q1")):
         ref = np.array([float(v) for v in GOLD[key]["values"]])
         got = _vortex_norms(dim)
-        assert np.max(np.abs(got - ref) / ref) < 5e-8, (got, ref)
+        assert np.max(np.abs(got - ref) / ref) < FLOAT_NORM_NOISE, (got, ref)
+
+
+def _vortex_inflow_norms(dim):
+    """AdvectionDiffusionOperation::solve with inflow/outflow constraints
+    (source/level_set/advection_diffusion_operation.cpp:243-296): Dirichlet lifting with the inflow
+    values as additional inhomogeneous constraints and the operator's pre/post hooks off, rhs zero
+    on the inflow rows, GMRES on the operator with identity inflow rows, then the inflow values set."""
+    mesh, phi, vel, faces = vortex_inflow(dim)
+    inflow = inflow_dofs(mesh, vel, faces)
+    op = Operator(mesh, "advdiff", dt=0.01, theta=0.5, eps=0.0, vel=vel, imask=inflow)
+    nobc = op.with_(imask=None)
+    out = []
+    for _ in range(5):
+        old = phi.copy()
+        bc = np.where(inflow == 1, -1.0, 0.0)
+        rhs = -nobc.vmult(bc)
+        nobc.create_rhs(rhs, old)
+        rhs[inflow == 1] = 0.0
+        x = old.copy()
+        solve(op, x, rhs, "gmres", inv_diag=op.inverse_diagonal(), rel_tol=1e-12)
+        x[inflow == 1] = -1.0
+        phi = x
+        out.append(op.l2_norm(phi))
+    return np.array(out)
+
+
+def test_vortex_inflow_outflow_logs():
+    for dim, key in ((3, "advdiff_vortex_mf_inflow_outflow_3d_q1"), (2, "advdiff_vortex_mf_inflow_outflow_2d_q1")):
+        ref = np.array([float(v) for v in GOLD[key]["values"]])
+        got = _vortex_inflow_norms(dim)
+        assert np.max(np.abs(got - ref) / ref) < FLOAT_NORM_NOISE, (dim, got, ref)

@@ -279,6 +279,12 @@ typedef struct mpdg_solid_liquid
   double  liquidus_temperature, solidus_temperature;
   int32_t sharp; /* SolidLiquidPropertiesTransitionType: 0 mushy_zone, 1 sharp */
   int32_t reserved;
+  /* latent heat of fusion per unit mass (MaterialData::latent_heat_of_fusion, material.hpp:654-655);
+     > 0 adds the apparent capacity of the mushy zone to the specific heat
+     (material.templates.hpp:561-614, source/heat/apparent_capacity.cpp:157-300) */
+  double  latent_heat;
+  int32_t capacity_type; /* 0 quadratic-linear-quadratic tent (the default), 1 quartic bell, 2 constant */
+  int32_t reserved2;
 } mpdg_solid_liquid;
 MPDG_API int mpdg_op_set_solidification(mpdg_op *op, const mpdg_solid_liquid *material);
 MPDG_API int mpdg_op_set_old_temperature(mpdg_op *op, const double *temperature_old);

@@ -85,6 +85,9 @@ class SolidLiquid(C.Structure):
         ("solidus_temperature", C.c_double),
         ("sharp", C.c_int32),
         ("reserved", C.c_int32),
+        ("latent_heat", C.c_double),
+        ("capacity_type", C.c_int32),
+        ("reserved2", C.c_int32),
     ]
 
 

@@ -1164,7 +1164,8 @@ mpdg_op_set_solidification(mpdg_op *op, const mpdg_solid_liquid *mat)
     return fail(MPDG_ERR_UNSUPPORTED, "temperature-dependent material supports FE_Q degree 1..2");
   if (!(mat->liquid_density > 0 && mat->liquid_specific_heat > 0 && mat->liquid_conductivity > 0 &&
         mat->solid_density > 0 && mat->solid_specific_heat > 0 && mat->solid_conductivity > 0) ||
-      (!mat->sharp && !(mat->liquidus_temperature > mat->solidus_temperature)))
+      (!mat->sharp && !(mat->liquidus_temperature > mat->solidus_temperature)) || !(mat->latent_heat >= 0.0) ||
+      mat->capacity_type < 0 || mat->capacity_type > 2)
     return fail(MPDG_ERR_ARG, "material parameters must be positive and the liquidus above the solidus");
   // the solid-phase kernel's bricks may outnumber the flags allocated for the constant-material ones
   int shape[3];
@@ -1194,6 +1195,8 @@ mpdg_op_set_solidification(mpdg_op *op, const mpdg_solid_liquid *mat)
   m.t_liquidus = mat->liquidus_temperature;
   m.t_solidus  = mat->solidus_temperature;
   m.sharp      = mat->sharp ? 1 : 0;
+  m.latent_heat   = mat->latent_heat;
+  m.capacity_type = mat->capacity_type;
   op->smat     = m;
   op->solid    = true;
   return MPDG_OK;

@@ -42,7 +42,66 @@ namespace mpdg
     {
       T   rho_l, cp_l, k_l, rho_s, cp_s, k_s, t_liquidus, t_solidus, inv_mushy;
       int sharp;
+      T   latent;   // latent heat of fusion (0: none)
+      int cap_type; // apparent capacity: 0 quadratic-linear-quadratic, 1 quartic bell, 2 constant
     };
+
+    // Ramp from (x1, y1) to (x2, y2) with zero slope at both ends: quadratic on [x1, x1 + delta],
+    // linear in between, quadratic on [x2 - delta, x2] (value and slope continuous).
+    template <typename T>
+    __device__ __forceinline__ void
+    zero_slope_ramp(T x, T x1, T x2, T y1, T y2, T delta, T &val, T &der)
+    {
+      const T s = (y2 - y1) / (x2 - x1 - delta);
+      if (x < x1 + delta)
+        {
+          val = y1 + T(0.5) * s * (x - x1) * (x - x1) / delta;
+          der = s * (x - x1) / delta;
+        }
+      else if (x > x2 - delta)
+        {
+          val = y2 - T(0.5) * s * (x2 - x) * (x2 - x) / delta;
+          der = s * (x2 - x) / delta;
+        }
+      else
+        {
+          val = y1 + s * (x - x1 - T(0.5) * delta);
+          der = s;
+        }
+    }
+
+    // Apparent specific heat of the latent heat and its temperature derivative at solid fraction fs
+    // (include/meltpooldg/core/material.templates.hpp:561-614, source/heat/apparent_capacity.cpp:
+    // 157-300): zero outside the mushy zone, each shape integrating to L over [T_solidus, T_liquidus]:
+    // constant L / dT; quartic bell L (2 / dT) 15/16 (1 - x^2)^2 with x = 1 - 2 fs; the default tent of
+    // peak 2 L / dT at the mid temperature with flat-ended flanks of width dT / 6, evaluated at
+    // T = T_liquidus - fs dT.
+    template <typename T>
+    __device__ __forceinline__ void
+    apparent_capacity(const SolidMat<T> &m, T fs, T &c, T &dc)
+    {
+      c = dc = T(0);
+      if (!(m.latent > T(0)) || !(fs > T(0)) || !(fs < T(1)))
+        return;
+      const T L = m.latent, dT = m.t_liquidus - m.t_solidus;
+      if (m.cap_type == 2)
+        c = L / dT;
+      else if (m.cap_type == 1)
+        {
+          const T r = T(2) / dT, x = T(1) - T(2) * fs;
+          c         = L * r * T(15.0 / 16.0) * (T(1) - x * x) * (T(1) - x * x);
+          dc        = L * r * r * T(15.0 / 4.0) * (x * x - T(1)) * x;
+        }
+      else
+        {
+          const T t = m.t_liquidus - fs * dT, tp = T(0.5) * (m.t_solidus + m.t_liquidus);
+          const T peak = T(2) * L / dT, delta = dT / T(6);
+          if (t <= tp)
+            zero_slope_ramp(t, m.t_solidus, tp, T(0), peak, delta, c, dc);
+          else
+            zero_slope_ramp(t, tp, m.t_liquidus, peak, T(0), delta, c, dc);
+        }
+    }
 
     // solid fraction, cubic blend weight and its temperature derivative at temperature t
     template <typename T>
@@ -87,11 +146,13 @@ namespace mpdg
       const T    w   = (T(3) - T(2) * fs) * fs * fs, dw = -m.inv_mushy * (T(6) * fs - T(6) * fs * fs);
       auto       pr  = [&](T vl, T vs) { return fs == T(0) ? vl : (fs == T(1) ? vs : vl + (vs - vl) * w); };
       auto       dpr = [&](T vl, T vs) { return end ? T(0) : (vs - vl) * dw; };
-      const T    rho = pr(m.rho_l, m.rho_s), cp = pr(m.cp_l, m.cp_s);
-      rc             = rho * cp;
-      k              = pr(m.k_l, m.k_s);
-      drc            = dpr(m.rho_l, m.rho_s) * cp + rho * dpr(m.cp_l, m.cp_s);
-      dk             = dpr(m.k_l, m.k_s);
+      T          ca, dca;
+      apparent_capacity(m, fs, ca, dca);
+      const T rho = pr(m.rho_l, m.rho_s), cp = pr(m.cp_l, m.cp_s) + ca;
+      rc          = rho * cp;
+      k           = pr(m.k_l, m.k_s);
+      drc         = dpr(m.rho_l, m.rho_s) * cp + rho * (dpr(m.cp_l, m.cp_s) + dca);
+      dk          = dpr(m.k_l, m.k_s);
     }
 
     template <typename T, int N>
@@ -374,6 +435,8 @@ namespace mpdg
       s.t_liquidus = (T)m.t_liquidus, s.t_solidus = (T)m.t_solidus;
       s.inv_mushy  = m.t_liquidus > m.t_solidus ? (T)(1.0 / (m.t_liquidus - m.t_solidus)) : T(0);
       s.sharp      = m.sharp;
+      s.latent     = (T)m.latent_heat;
+      s.cap_type   = m.capacity_type;
       return s;
     }
 

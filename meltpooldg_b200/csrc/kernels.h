@@ -82,6 +82,8 @@ namespace mpdg
     double rho_s = 1.0, cp_s = 1.0, k_s = 1.0; // solid
     double t_liquidus = 1.0, t_solidus = 0.0;
     int    sharp = 0;                          // 0 mushy zone, 1 sharp transition at t_solidus
+    double latent_heat   = 0.0;                // > 0: apparent capacity over the mushy zone
+    int    capacity_type = 0;                  // 0 quadratic-linear-quadratic, 1 quartic bell, 2 constant
   };
 
   template <typename T>

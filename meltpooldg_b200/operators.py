@@ -218,10 +218,15 @@ class HeatDiffuseOperator(OperatorMatrixFree):
             bc.neumann_flux[i] = float(neumann_flux[i])
         check(lib().mpdg_op_set_heat_bc(self._h, C.byref(bc)))
 
+    CAPACITY_TYPES = {"qlq": 0, "quadratic_linear_quadratic": 0, "poly4_bell": 1, "constant": 2}
+
     def set_solidification(self, liquid=(1.0, 1.0, 1.0), solid=(1.0, 1.0, 1.0), liquidus_temperature: float = 1.0,
-                           solidus_temperature: float = 0.0, sharp: bool = False, enabled: bool = True) -> None:
-        """Temperature-dependent material (MaterialTypes::liquid_solid, no latent heat); liquid and
-        solid are (density, specific heat capacity, thermal conductivity)."""
+                           solidus_temperature: float = 0.0, sharp: bool = False, enabled: bool = True,
+                           latent_heat: float = 0.0, capacity_type: str = "qlq") -> None:
+        """Temperature-dependent material (MaterialTypes::liquid_solid); liquid and solid are
+        (density, specific heat capacity, thermal conductivity); latent_heat > 0 adds the apparent
+        capacity of the mushy zone of shape capacity_type ("qlq", the reference's default,
+        "poly4_bell" or "constant")."""
         if not enabled:
             check(lib().mpdg_op_set_solidification(self._h, None))
             return
@@ -230,6 +235,10 @@ class HeatDiffuseOperator(OperatorMatrixFree):
         m.solid_density, m.solid_specific_heat, m.solid_conductivity = (float(v) for v in solid)
         m.liquidus_temperature, m.solidus_temperature = float(liquidus_temperature), float(solidus_temperature)
         m.sharp = 1 if sharp else 0
+        m.latent_heat = float(latent_heat)
+        if capacity_type not in self.CAPACITY_TYPES:
+            raise ValueError(f"unknown apparent capacity type {capacity_type}")
+        m.capacity_type = self.CAPACITY_TYPES[capacity_type]
         check(lib().mpdg_op_set_solidification(self._h, C.byref(m)))
 
     def set_old_temperature(self, temperature_old_device) -> None:

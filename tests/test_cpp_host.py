@@ -202,3 +202,78 @@ def test_cpp_newton_with_solidification_matches_oracle(tmp_path):
         assert np.max(np.abs(got[s] - ref[s])) <= 1e-9 * np.max(np.abs(ref[s]))
     # part of the block crosses the mushy zone
     assert np.any((ref[-1] > 1600.0) & (ref[-1] < 1700.0))
+
+
+def oracle_level_set_step():
+    """The chain of tests/cpp/level_set_step.cpp restated with the oracle: SUPG advection (GMRES to
+    1e-13 on the oracle operator plus oracle/supg.py), the normal and curvature projections
+    (M + h^2 K, oracle CG) and three Olsson steps (oracle/reinit.py, CG to 1e-13)."""
+    import scipy.sparse.linalg as spla
+
+    from oracle import reinit as R
+    from oracle import supg as S
+    from oracle.oracle import Mesh as OMesh
+    from oracle.oracle import Operator as OOp
+    from oracle.oracle import solve as osolve
+
+    m, k = 12, 2
+    h = 1.0 / m
+    mesh = OMesh(k, (m, m, m))
+    X, Y, Z = mesh.coords()
+    r = np.sqrt((X - 0.5) ** 2 + (Y - 0.6) ** 2 + (Z - 0.5) ** 2)
+    psi0 = 0.5 * (1.0 - np.tanh((r - 0.25) / 0.04))
+    vel = [0.5, -0.5, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0]
+    dt, theta, eps, tau = 5e-3, 1.0, 1e-3, 0.1
+    adv = OOp(mesh, "advdiff", dt=dt, theta=theta, eps=eps, vel=vel)
+    n = mesh.ndofs
+
+    def A(u):
+        return adv.vmult(u) + S.supg_apply(mesh, None, vel, tau, 1.0 / dt, theta, theta * eps, u)
+
+    rhs = np.zeros(n)
+    adv.create_rhs(rhs, psi0)
+    rhs += S.supg_apply(mesh, None, vel, tau, 1.0 / dt, theta - 1.0, (theta - 1.0) * eps, psi0, plain=True)
+    d = adv.diagonal() + S.supg_diagonal(mesh, None, vel, tau, 1.0 / dt, theta, theta * eps)
+    Aop = spla.LinearOperator((n, n), matvec=A)
+    Pop = spla.LinearOperator((n, n), matvec=lambda v: v / d)
+    psi, info = spla.gmres(Aop, rhs, x0=psi0.copy(), M=Pop, rtol=1e-13, atol=0.0, restart=60, maxiter=2000)
+    assert info == 0
+    proj = OOp(mesh, "heat", rho_cp=1.0, dt=1.0, k=h * h)
+    inv = proj.inverse_diagonal()
+    normal = []
+    for c in R.normal_rhs(mesh, None, psi):
+        x = np.zeros(n)
+        osolve(proj, x, c, "cg", inv, rel_tol=1e-13)
+        normal.append(x)
+    tol = 1e-10
+    kappa = np.zeros(n)
+    osolve(proj, kappa, R.curvature_rhs(mesh, None, normal, tol), "cg", inv, rel_tol=1e-13)
+    rdt, eps_n, eps_t = 0.25 * h, 0.5 * h, 0.0
+    dr = R.diagonal(mesh, None, rdt, eps_n, eps_t, normal, tol)
+    Rop = spla.LinearOperator((n, n), matvec=lambda u: R.tangent_apply(mesh, None, rdt, eps_n, eps_t, normal, tol, u))
+    Dop = spla.LinearOperator((n, n), matvec=lambda v: v / dr)
+    psi_r = psi.copy()
+    for _ in range(3):
+        b = R.create_rhs(mesh, None, eps_n, eps_t, normal, tol, psi_r)
+        dpsi, info = spla.cg(Rop, b, M=Dop, rtol=1e-13, atol=0.0, maxiter=5000)
+        assert info == 0
+        psi_r = psi_r + dpsi
+    return np.array([psi, normal[0], normal[1], normal[2], kappa, psi_r])
+
+
+@pytest.mark.gpu
+def test_cpp_level_set_step_matches_oracle_chain(tmp_path):
+    """tests/cpp/level_set_step.cpp (LevelSetOperation::solve's order, source/level_set/
+    level_set_operation.cpp:364-387) on the GPU through the C++ host layer, field by field against
+    the oracle's chain: each output within 1e-8 of the oracle's (relative to its largest entry)."""
+    exe = build_program(tmp_path, "level_set_step")
+    out = str(tmp_path / "ls.bin")
+    r = subprocess.run([exe, out], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    its = json.loads(r.stdout.strip().splitlines()[-1])
+    assert its["advection_iterations"] > 0 and its["reinit_iterations"] > 0
+    ref = oracle_level_set_step()
+    got = np.fromfile(out, dtype=np.float64).reshape(ref.shape)
+    for f, name in enumerate(["psi (advected)", "n_x", "n_y", "n_z", "curvature", "psi (reinitialised)"]):
+        err = np.max(np.abs(got[f] - ref[f])) / np.max(np.abs(ref[f]))
+        assert err <= 1e-8, (name, err)

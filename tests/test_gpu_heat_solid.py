@@ -123,3 +123,40 @@ def test_solid_argument_checks():
     g.vmult(y, x)
     g.set_solidification(enabled=False)
     g.vmult(y, x)
+
+
+@pytest.mark.parametrize("degree,capacity", [(1, "qlq"), (2, "qlq"), (2, "poly4_bell"), (2, "constant")])
+def test_solid_latent_heat_matches_oracle(degree, capacity):
+    """Latent heat of fusion as the reference's apparent capacity (material.templates.hpp:561-614):
+    vmult, the residual part of create_rhs and the inverse diagonal against the oracle, with the
+    temperatures spread over the mushy zone and both pure phases."""
+    import torch
+
+    from meltpooldg_b200.operators import HeatDiffuseOperator
+
+    dt, L = 1e-3, 2.7e5
+    om, gm, cm = meshes(degree, (9, 8, 6), faces=0b000011, length=(0.7, 0.9, 0.5))
+    g = HeatDiffuseOperator(gm, rho_cp=1.0, dt=dt, conductivity=1.0)
+    g.set_solidification(LIQ, SOL, TL, TS, latent_heat=L, capacity_type=capacity)
+    mat = SolidLiquid(LIQ, SOL, TL, TS, False, latent_heat=L, capacity_type=capacity)
+    T = 1650.0 + 90.0 * uniform_dofs(om, seed=5)
+    Told = T - 4.0 * (uniform_dofs(om, seed=6) + 1.0)
+    Td, Tod = to_gpu(T), to_gpu(Told)
+    g.set_temperature(Td)
+    g.set_old_temperature(Tod)
+    x = uniform_dofs(om, seed=1)
+    ref = tangent_apply(om, cm, mat, dt, T, Told, x)
+    yd = torch.full((om.ndofs,), np.nan, dtype=torch.float64, device="cuda")
+    g.vmult(yd, to_gpu(x))
+    assert rel_err(yd.cpu().numpy(), ref) <= 1e-12
+    rhs = torch.zeros(om.ndofs, dtype=torch.float64, device="cuda")
+    g.create_rhs(rhs, Td, Tod)
+    assert rel_err(rhs.cpu().numpy(), residual(om, cm, mat, dt, T, Told)) <= 1e-12
+    d = torch.empty_like(rhs)
+    g.compute_inverse_diagonal_from_matrixfree(d)
+    dref = diagonal(om, cm, mat, dt, T, Told)
+    inv = np.where(np.abs(dref) > 1e-10, 1.0 / np.where(dref != 0, dref, 1.0), 1.0)
+    if cm is not None:
+        inv[cm == 1] = 1.0
+    assert rel_err(d.cpu().numpy(), inv) <= 1e-12
+    assert g.device_errors() == 0

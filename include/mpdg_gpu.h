@@ -235,6 +235,17 @@ MPDG_API int mpdg_level_set_normal_rhs(mpdg_op *op, const double *psi, int norma
                                        double *nz);
 MPDG_API int mpdg_level_set_curvature_rhs(mpdg_op *op, const double *nx, const double *ny, const double *nz,
                                           double normal_tolerance, double *dst);
+/* Narrow band of the normal-vector and curvature projections (NormalVectorData / CurvatureData
+   ::narrow_band, include/meltpooldg/level_set/level_set_tools.hpp:357-368): on a heat handle used as
+   the projection operator (rho_c_p = dt = 1, conductivity = the damping), every integrand is
+   multiplied at each Gauss point by 1 where |level_set(x_q)| < threshold and 0 elsewhere -- the
+   operator's mass and stiffness terms (vmult, inverse diagonal, normal_vector_operator.cpp:326-358,
+   inverted with the relative rule of :318-321), the gradient in mpdg_level_set_normal_rhs (masked
+   by |psi|, :184-191) and the divergence in mpdg_level_set_curvature_rhs (masked by |level_set|,
+   curvature_operator.cpp:209-214).  level_set: DEVICE array of n_dofs the caller keeps alive
+   (read plainly); NULL or threshold <= 0 removes the band.  Constant conductivity, Dirichlet faces
+   only. */
+MPDG_API int mpdg_op_set_narrow_band(mpdg_op *op, const double *level_set, double threshold);
 /* Inflow/outflow condition of the advection-diffusion operator
    (AdvectionDiffusionOperation::create_inflow_outflow_constraints,
    source/level_set/advection_diffusion_operation.cpp:369-499, with the operator's set_inflow_outflow_bc

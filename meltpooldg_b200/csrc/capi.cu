@@ -98,6 +98,14 @@ struct mpdg_op
   double       *d_in_val   = nullptr; // their prescribed values
   long long     n_inflow   = 0;
   bool          inflow_prepost = true; // set_apply_inflow_outflow_constraints_pre_post_matrix_free
+  // narrow band of the normal-vector / curvature projections (heat handles): level set (not owned)
+  const double *d_band_ls = nullptr;
+  double        band      = 0.0;
+  bool
+  banded() const
+  {
+    return kind == MPDG_HEAT && d_band_ls != nullptr && band > 0.0;
+  }
   double        eps_n = 0.0, eps_t = 0.0, ntol = 1e-16; // reinitialisation
   const double *d_normal[3]{};                           // reinitialisation normal field (not owned)
   double        supg_coef = 0.0;
@@ -254,6 +262,33 @@ namespace
     return r;
   }
 
+  // The heat operator rho c_p / dt M + k K as the isotropic point-wise kernel with the narrow band
+  // of the handle ('which' as in apply: 1 mass only, 2 stiffness only)
+  template <typename T>
+  ReinitLaunch<T>
+  band_launch(const mpdg_op *op, int which, double scale, const T *src, T *dst, int mask_src)
+  {
+    ReinitLaunch<T> r;
+    r.degree           = op->degree;
+    r.scale            = scale;
+    r.dt               = which == 2 ? 1e300 : op->dt / op->rho_cp;
+    r.eps_normal       = which == 1 ? 0.0 : op->k;
+    r.eps_tangential   = r.eps_normal;
+    r.normal_tolerance = 1.0;
+    for (int d = 0; d < 3; ++d)
+      {
+        r.hlen[d]   = op->h[d];
+        r.normal[d] = nullptr;
+      }
+    r.grid     = op->grid<T>();
+    r.src      = src;
+    r.dst      = dst;
+    r.mask_src = mask_src;
+    r.band_ls  = op->d_band_ls;
+    r.band     = op->band;
+    return r;
+  }
+
   // Temperature-dependent material: the tangent (rhs = false) or the residual part of create_rhs
   // (rhs = true, dst +=, src unused) with the operator's temperature and old temperature.  FP32
   // applies read FP32 copies of both.
@@ -313,6 +348,17 @@ namespace
   apply(mpdg_op *op, int mode, double scale, T *dst, const T *src, const T *b, int mask_src, int which = 0,
         const int *skip = nullptr, const DotSink *dot = nullptr)
   {
+    if (op->banded())
+      {
+        // the projection operator M + damping K with a narrow band (normal_vector_operator.cpp:
+        // 326-358, curvature_operator.cpp:337-369): the isotropic form of the point-wise kernel
+        if (mode == (int)OutMode::Set)
+          MPDG_CUDA(vec_fill<T>(dst, T(0), op->ndofs, op->stream));
+        else if (mode == (int)OutMode::BPlus && dst != b)
+          MPDG_CUDA(cudaMemcpyAsync(dst, b, sizeof(T) * op->ndofs, cudaMemcpyDeviceToDevice, op->stream));
+        MPDG_CUDA(reinit_integrate<T>(band_launch<T>(op, which, scale, src, dst, mask_src), 0, op->stream));
+        return MPDG_OK;
+      }
     if (op->kind == MPDG_HEAT)
       {
         HeatLaunch<T> h;
@@ -423,6 +469,24 @@ namespace
   inverse_diagonal_cells(mpdg_op *op, T *diag)
   {
     const GridDesc g = op->grid();
+    if (op->banded())
+      {
+        // diagonal of the banded projection, inverted with NormalVectorOperator's relative rule
+        // (normal_vector_operator.cpp:318-321): |d| > 1e-14 max(1, |d|_inf) ? 1/d : 1
+        double *d64 = std::is_same<T, double>::value ? reinterpret_cast<double *>(diag) : op->vec<double>("band_diag");
+        if (!d64)
+          return fail(MPDG_ERR_NOMEM, "diagonal work vector");
+        MPDG_CUDA(vec_fill<double>(d64, 0.0, op->ndofs, op->stream));
+        ReinitLaunch<double> r = band_launch<double>(op, 0, 1.0, nullptr, nullptr, 0);
+        r.diag                 = d64;
+        MPDG_CUDA(reinit_integrate<double>(r, 2, op->stream));
+        MPDG_CUDA(vec_set_constrained<double>(d64, 1.0, g, op->stream));
+        MPDG_CUDA(vec_absmax<double>(d64, op->ndofs, op->d_scal, op->reducer(), op->stream));
+        MPDG_CUDA(vec_invert_rel<double>(d64, op->d_scal, op->ndofs, op->stream));
+        if (!std::is_same<T, double>::value)
+          MPDG_CUDA(vec_convert<T, double>(diag, d64, op->ndofs, op->stream));
+        return MPDG_OK;
+      }
     if (op->kind == MPDG_HEAT && (op->tangent_faces() || op->solid))
       {
         // cell and face parts summed in FP64, then inverted (|d| > 1e-10 ? 1/d : 1)
@@ -1241,8 +1305,9 @@ mpdg_level_set_normal_rhs(mpdg_op *op, const double *psi, int normalized, double
     return fail(MPDG_ERR_ARG, "null argument to mpdg_level_set_normal_rhs");
   if (op->degree > 2)
     return fail(MPDG_ERR_UNSUPPORTED, "the level-set right-hand sides support FE_Q degree 1..2");
+  // the normal's narrow band masks with the level set psi itself (normal_vector_operator.cpp:184-189)
   MPDG_CUDA(level_set_rhs(op->grid(), op->degree, op->h, 0, normalized ? 1 : 0, 0.0, psi, nullptr, nullptr, nx, ny,
-                          nz, op->stream));
+                          nz, op->stream, op->banded() ? psi : nullptr, op->band));
   return MPDG_OK;
 }
 
@@ -1258,7 +1323,30 @@ mpdg_level_set_curvature_rhs(mpdg_op *op, const double *nx, const double *ny, co
     return fail(MPDG_ERR_UNSUPPORTED, "the level-set right-hand sides support FE_Q degree 1..2");
   MPDG_CUDA(vec_fill<double>(dst, 0.0, op->ndofs, op->stream));
   MPDG_CUDA(level_set_rhs(op->grid(), op->degree, op->h, 1, 0, normal_tolerance, nx, ny, nz, dst, nullptr, nullptr,
-                          op->stream));
+                          op->stream, op->banded() ? op->d_band_ls : nullptr, op->band));
+  return MPDG_OK;
+}
+
+int
+mpdg_op_set_narrow_band(mpdg_op *op, const double *level_set, double threshold)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_HEAT)
+    return fail(MPDG_ERR_ARG, "the narrow band belongs to the projection (heat-form) operators");
+  if (!level_set || !(threshold > 0.0))
+    {
+      op->d_band_ls = nullptr;
+      op->band      = 0.0;
+      return MPDG_OK;
+    }
+  if (op->degree > 2)
+    return fail(MPDG_ERR_UNSUPPORTED, "the narrow band supports FE_Q degree 1..2");
+  if (op->d_k64 || op->d_mask || op->solid || heat_faces_active(op->fbc, 0) || heat_faces_active(op->fbc, 1))
+    return fail(MPDG_ERR_UNSUPPORTED, "the narrow band takes a constant damping, Dirichlet faces only and no "
+                                      "boundary-face terms or temperature-dependent material");
+  op->d_band_ls = level_set;
+  op->band      = threshold;
   return MPDG_OK;
 }
 

@@ -128,6 +128,8 @@ namespace mpdg
     T            *dst  = nullptr;
     double       *diag = nullptr;
     int           mask_src = 1;
+    const double *band_ls = nullptr; // narrow band: integrands masked where |level set| >= band
+    double        band    = 0.0;
   };
   // mode 0: dst += scale * A src on free rows; 1: dst += the rhs integrand of psi_old = src (plain);
   // 2: diag += the tangent's diagonal on free rows
@@ -135,9 +137,10 @@ namespace mpdg
   cudaError_t reinit_integrate(const ReinitLaunch<T> &h, int mode, cudaStream_t s);
   // normal-vector (mode 0: out_d += int grad_d psi phi, normalised on request) and curvature (mode 1:
   // out0 += -int div(normalize(n_i, tol)) phi) right-hand sides, FE_Q(1, 2), free rows only
+  // band_ls / band: optional narrow band (integrand masked where |band_ls(x_q)| >= band)
   cudaError_t level_set_rhs(const GridDesc &g, int K, const double hlen[3], int mode, int normalized, double tol,
                             const double *in0, const double *in1, const double *in2, double *out0, double *out1,
-                            double *out2, cudaStream_t s);
+                            double *out2, cudaStream_t s, const double *band_ls = nullptr, double band = 0.0);
 
   // whether mode (0 tangent / 2 diagonal, 1 rhs) has any face to integrate
   bool heat_faces_active(const HeatFaceBC &bc, int mode);

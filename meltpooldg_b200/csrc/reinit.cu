@@ -40,6 +40,8 @@ namespace mpdg
       double       *diag;
       int           mode; // 0 tangent apply, 1 rhs (src = psi_old, plain), 2 diagonal
       int           mask_src;
+      const double *band_ls; // narrow band (include/meltpooldg/level_set/level_set_tools.hpp:357-368)
+      T             band;
     };
 
     template <int K, typename T>
@@ -54,7 +56,7 @@ namespace mpdg
           const int cx = (int)(c % m0), cy = (int)((c / m0) % m1), cz = (int)(c / ((long long)m0 * m1));
           long long idx[N3];
           bool      con[N3];
-          T         u[N3], R[N3];
+          T         u[N3], R[N3], ls[N3];
 #pragma unroll
           for (int l = 0; l < N; ++l)
 #pragma unroll
@@ -69,13 +71,16 @@ namespace mpdg
                   con[q]             = is_constrained(a.g, I, J, L, id);
                   u[q]               = (a.mode == 2 || (a.mask_src && con[q])) ? T(0) : a.src[id];
                   R[q]               = T(0);
+                  ls[q]              = a.band_ls ? (T)a.band_ls[id] : T(0); // read plainly
                 }
           for (int qz = 0; qz < N; ++qz)
             for (int qy = 0; qy < N; ++qy)
               for (int qx = 0; qx < N; ++qx)
                 {
                   // value and gradient of u and the normal field at the Gauss point
-                  T uv = T(0), g[3] = {T(0), T(0), T(0)}, nv[3] = {T(0), T(0), T(0)};
+                  // (the isotropic form, eps_n == eps_t, has no normal field: n == nullptr)
+                  T uv = T(0), g[3] = {T(0), T(0), T(0)}, nv[3] = {T(0), T(0), T(0)}, lq = T(0);
+                  const bool has_n = a.n[0] != nullptr;
 #pragma unroll
                   for (int l = 0; l < N; ++l)
 #pragma unroll
@@ -87,22 +92,28 @@ namespace mpdg
                           const T   bx = a.B[qx * N + i], by = a.B[qy * N + j], bz = a.B[qz * N + l];
                           const T   phi = bx * by * bz;
                           uv += phi * u[q];
+                          lq += phi * ls[q];
                           g[0] += a.G[qx * N + i] * by * bz * u[q];
                           g[1] += bx * a.G[qy * N + j] * bz * u[q];
                           g[2] += bx * by * a.G[qz * N + l] * u[q];
+                          if (has_n)
 #pragma unroll
-                          for (int d = 0; d < 3; ++d)
-                            nv[d] += phi * (T)a.n[d][idx[q]];
+                            for (int d = 0; d < 3; ++d)
+                              nv[d] += phi * (T)a.n[d][idx[q]];
                         }
 #pragma unroll
                   for (int d = 0; d < 3; ++d)
                     g[d] *= a.ih[d];
-                  const T nn  = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
-                  const T inv = nn > a.tol ? T(1) / nn : T(1) / a.tol;
+                  if (has_n)
+                    {
+                      const T nn  = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+                      const T inv = nn > a.tol ? T(1) / nn : T(1) / a.tol;
 #pragma unroll
-                  for (int d = 0; d < 3; ++d)
-                    nv[d] *= inv;
-                  const T jw = a.det * a.w[qx] * a.w[qy] * a.w[qz];
+                      for (int d = 0; d < 3; ++d)
+                        nv[d] *= inv;
+                    }
+                  // narrow band: the point contributes only where |level set| < band
+                  const T jw = (a.band_ls && !(fabs(lq) < a.band)) ? T(0) : a.det * a.w[qx] * a.w[qy] * a.w[qz];
                   if (a.mode == 2)
                     {
                       // diagonal: int phi_i^2 / dt + grad phi_i . D grad phi_i
@@ -197,6 +208,8 @@ namespace mpdg
       a.diag     = h.diag;
       a.mode     = mode;
       a.mask_src = h.mask_src;
+      a.band_ls  = h.band > 0.0 ? h.band_ls : nullptr;
+      a.band     = (T)h.band;
       const long long ncell  = (long long)h.grid.m[0] * h.grid.m[1] * h.grid.m[2];
       const int       blocks = (int)std::max<long long>(1, std::min<long long>((ncell + 127) / 128, 148LL * 16));
       reinit_kernel<K, T><<<blocks, 128, 0, s>>>(a);
@@ -215,7 +228,8 @@ namespace mpdg
     __global__ void __launch_bounds__(128)
     level_set_rhs_kernel(const GridDesc g, const double *B, const double *G, const double *w, double det, double ihx,
                          double ihy, double ihz, int mode, int normalized, double tol, const double *in0,
-                         const double *in1, const double *in2, double *out0, double *out1, double *out2)
+                         const double *in1, const double *in2, double *out0, double *out1, double *out2,
+                         const double *band_ls, double band)
     {
       constexpr int   N = K + 1, N3 = N * N * N;
       const double    ih[3] = {ihx, ihy, ihz};
@@ -226,7 +240,7 @@ namespace mpdg
           const int cx = (int)(c % m0), cy = (int)((c / m0) % m1), cz = (int)(c / ((long long)m0 * m1));
           long long idx[N3];
           bool      con[N3];
-          double    v[3][N3], R[3][N3];
+          double    v[3][N3], R[3][N3], ls[N3];
 #pragma unroll
           for (int l = 0; l < N; ++l)
 #pragma unroll
@@ -239,6 +253,7 @@ namespace mpdg
                   const long long id = (long long)I + (long long)g.n[0] * ((long long)J + (long long)g.n[1] * L);
                   idx[q]            = id;
                   con[q]            = is_constrained(g, I, J, L, id);
+                  ls[q]             = band_ls ? band_ls[id] : 0.0;
                   if (mode == 0)
                     v[0][q] = in0[id];
                   else
@@ -255,7 +270,7 @@ namespace mpdg
             for (int qy = 0; qy < N; ++qy)
               for (int qx = 0; qx < N; ++qx)
                 {
-                  double gv[3] = {0.0, 0.0, 0.0}, div = 0.0;
+                  double gv[3] = {0.0, 0.0, 0.0}, div = 0.0, lq = 0.0;
 #pragma unroll
                   for (int l = 0; l < N; ++l)
 #pragma unroll
@@ -267,6 +282,7 @@ namespace mpdg
                           const double bx = B[qx * N + i], by = B[qy * N + j], bz = B[qz * N + l];
                           const double p[3] = {G[qx * N + i] * ih[0] * by * bz, bx * G[qy * N + j] * ih[1] * bz,
                                                bx * by * G[qz * N + l] * ih[2]};
+                          lq += bx * by * bz * ls[q];
                           if (mode == 0)
                             {
 #pragma unroll
@@ -276,6 +292,14 @@ namespace mpdg
                           else
                             div += p[0] * v[0][q] + p[1] * v[1][q] + p[2] * v[2][q];
                         }
+                  // narrow band (normal_vector_operator.cpp:184-191, curvature_operator.cpp:209-214):
+                  // the gradient (before its normalisation) or the divergence is masked by
+                  // |level set| < band at the point
+                  if (band_ls && !(fabs(lq) < band))
+                    {
+                      gv[0] = gv[1] = gv[2] = 0.0;
+                      div                   = 0.0;
+                    }
                   if (mode == 0 && normalized)
                     {
                       const double nn = sqrt(gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2]);
@@ -351,8 +375,10 @@ namespace mpdg
   cudaError_t
   level_set_rhs(const GridDesc &g, int K, const double hlen[3], int mode, int normalized, double tol,
                 const double *in0, const double *in1, const double *in2, double *out0, double *out1, double *out2,
-                cudaStream_t s)
+                cudaStream_t s, const double *band_ls, double band)
   {
+    if (!(band > 0.0))
+      band_ls = nullptr;
     if (K < 1 || K > 2)
       return cudaErrorInvalidValue;
     const double *tab = level_set_tables(K);
@@ -365,11 +391,11 @@ namespace mpdg
     if (K == 1)
       level_set_rhs_kernel<1><<<blocks, 128, 0, s>>>(g, tab, tab + n * n, tab + 2 * n * n, det, 1.0 / hlen[0],
                                                       1.0 / hlen[1], 1.0 / hlen[2], mode, normalized, tol, in0, in1,
-                                                      in2, out0, out1, out2);
+                                                      in2, out0, out1, out2, band_ls, band);
     else
       level_set_rhs_kernel<2><<<blocks, 128, 0, s>>>(g, tab, tab + n * n, tab + 2 * n * n, det, 1.0 / hlen[0],
                                                       1.0 / hlen[1], 1.0 / hlen[2], mode, normalized, tol, in0, in1,
-                                                      in2, out0, out1, out2);
+                                                      in2, out0, out1, out2, band_ls, band);
     return cudaGetLastError();
   }
 

@@ -218,6 +218,14 @@ class HeatDiffuseOperator(OperatorMatrixFree):
             bc.neumann_flux[i] = float(neumann_flux[i])
         check(lib().mpdg_op_set_heat_bc(self._h, C.byref(bc)))
 
+    def set_narrow_band(self, level_set, threshold: float) -> None:
+        """Narrow band of the projection operators (NormalVectorData / CurvatureData::narrow_band):
+        integrands masked where |level_set| >= threshold at the Gauss points; level_set is kept by
+        reference; threshold <= 0 or level_set None removes the band."""
+        self._band_ls = level_set
+        ptr = None if level_set is None or threshold <= 0 else self._v(level_set)
+        check(lib().mpdg_op_set_narrow_band(self._h, ptr, float(threshold)))
+
     CAPACITY_TYPES = {"qlq": 0, "quadratic_linear_quadratic": 0, "poly4_bell": 1, "constant": 2}
 
     def set_solidification(self, liquid=(1.0, 1.0, 1.0), solid=(1.0, 1.0, 1.0), liquidus_temperature: float = 1.0,

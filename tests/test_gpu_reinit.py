@@ -139,3 +139,59 @@ def test_level_set_rhs_and_normal_projection(degree, m, faces):
     c = to_gpu(np.full(om.ndofs, 7.0))  # overwritten
     g.level_set_curvature_rhs(c, *[to_gpu(v) for v in normal], normal_tolerance=1e-6)
     assert rel_err(c.cpu().numpy(), c_ref) <= 1e-12
+
+
+@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0), (2, (8, 7, 6), 0b000011)])
+def test_narrow_band_projection_and_rhs(degree, m, faces):
+    """Narrow band of the normal-vector / curvature projections (level_set_tools.hpp:357-368) on a
+    heat handle used as the projection operator: vmult (FP64, FP32), the inverse diagonal with the
+    relative rule, the normal and curvature right-hand sides and a CG solve, against the oracle."""
+    import torch
+
+    from meltpooldg_b200.operators import HeatDiffuseOperator, LinearSolver, LinearSolverData
+    from oracle.reinit import curvature_rhs, normal_rhs, projection_apply
+
+    om, gm, cm = meshes(degree, m, faces=faces, length=(1.0, 0.9, 1.1))
+    X, Y, Z = om.coords()
+    psi = np.tanh((np.sqrt((X - 0.5) ** 2 + (Y - 0.45) ** 2 + (Z - 0.55) ** 2) - 0.3) / 0.1)
+    band, damping = 0.8, 0.02
+    g = HeatDiffuseOperator(gm, rho_cp=1.0, dt=1.0, conductivity=damping)
+    psid = to_gpu(psi)
+    g.set_narrow_band(psid, band)
+    x = uniform_dofs(om, seed=1)
+    ref = projection_apply(om, cm, damping, x, level_set=psi, narrow_band=band)
+    y = torch.full((om.ndofs,), np.nan, dtype=torch.float64, device="cuda")
+    g.vmult(y, to_gpu(x))
+    assert rel_err(y.cpu().numpy(), ref) <= 1e-12
+    y32 = torch.empty(om.ndofs, dtype=torch.float32, device="cuda")
+    g.vmult(y32, to_gpu(x, torch.float32))
+    assert rel_err(y32.cpu().numpy(), ref) <= 2e-6
+    # diagonal by unit vectors of the oracle, relative inversion rule, constrained rows 1
+    n = om.ndofs
+    dref = np.array([projection_apply(om, cm, damping, np.eye(1, n, i).ravel(), level_set=psi, narrow_band=band)[i]
+                     for i in range(n)])
+    if cm is not None:
+        dref[cm == 1] = 1.0
+    thr = 1e-14 * max(1.0, np.max(np.abs(dref)))
+    inv = np.where(np.abs(dref) > thr, 1.0 / np.where(dref != 0, dref, 1.0), 1.0)
+    d = torch.empty_like(y)
+    g.compute_inverse_diagonal_from_matrixfree(d)
+    assert rel_err(d.cpu().numpy(), inv) <= 1e-12
+    # right-hand sides
+    nx, ny, nz = (torch.zeros_like(y) for _ in range(3))
+    g.level_set_normal_rhs(psid, nx, ny, nz)
+    for got, want in zip((nx, ny, nz), normal_rhs(om, cm, psi, narrow_band=band)):
+        assert rel_err(got.cpu().numpy(), want) <= 1e-12
+    normal = [X - 0.5, Y - 0.45, Z - 0.55]
+    kap = torch.empty_like(y)
+    g.level_set_curvature_rhs(kap, *(to_gpu(c) for c in normal), 1e-10)
+    assert rel_err(kap.cpu().numpy(), curvature_rhs(om, cm, normal, 1e-10, level_set=psi, narrow_band=band)) <= 1e-12
+    # projection solve: the band's rows only (outside the band the rows are identity-preconditioned zeros)
+    rhs = nx.clone()
+    sol = torch.zeros_like(rhs)
+    LinearSolver.solve(g, sol, rhs, LinearSolverData("CG", "Diagonal", rel_tolerance=1e-11))
+    r = rhs.cpu().numpy() - projection_apply(om, cm, damping, sol.cpu().numpy(), level_set=psi, narrow_band=band)
+    assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(rhs.cpu().numpy())
+    g.set_narrow_band(None, 0.0)
+    g.vmult(y, to_gpu(x))
+    assert rel_err(y.cpu().numpy(), projection_apply(om, cm, damping, x)) <= 1e-12

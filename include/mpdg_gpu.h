@@ -246,6 +246,14 @@ MPDG_API int mpdg_level_set_curvature_rhs(mpdg_op *op, const double *nx, const d
    (read plainly); NULL or threshold <= 0 removes the band.  Constant conductivity, Dirichlet faces
    only. */
 MPDG_API int mpdg_op_set_narrow_band(mpdg_op *op, const double *level_set, double threshold);
+/* Wetting boundary faces of the reinitialisation operator (OlssonOperator's boundary loops with
+   wetting_bc_ids, source/level_set/olsson_CG_operator.cpp:550-716): on the box faces in `faces`
+   (bit 2d low / 2d+1 high face of dim d) vmult adds int (D grad u . n_f) phi and create_rhs adds
+   -int (-c(psi) n + D grad psi) . n_f phi, D = eps_n n n^T + eps_t (I - n n^T), c(psi) = (1 - psi^2)/2,
+   n the unit interface normal, n_f the outward face normal; the inverse diagonal includes the
+   faces' terms of the wetting faces (the reference's diagonal adds those of every boundary face
+   when its face integrals are on, :377-405).  0 removes them. */
+MPDG_API int mpdg_op_set_wetting(mpdg_op *op, uint32_t faces);
 /* Inflow/outflow condition of the advection-diffusion operator
    (AdvectionDiffusionOperation::create_inflow_outflow_constraints,
    source/level_set/advection_diffusion_operation.cpp:369-499, with the operator's set_inflow_outflow_bc

@@ -107,6 +107,7 @@ struct mpdg_op
     return kind == MPDG_HEAT && d_band_ls != nullptr && band > 0.0;
   }
   double        eps_n = 0.0, eps_t = 0.0, ntol = 1e-16; // reinitialisation
+  unsigned      wetting = 0;                           // reinitialisation: wetting boundary faces
   const double *d_normal[3]{};                           // reinitialisation normal field (not owned)
   double        supg_coef = 0.0;
   const double *d_temp = nullptr; // linearisation temperature of the radiation tangent (not owned)
@@ -259,6 +260,7 @@ namespace
     r.src      = src;
     r.dst      = dst;
     r.mask_src = mask_src;
+    r.wetting  = op->wetting;
     return r;
   }
 
@@ -1324,6 +1326,19 @@ mpdg_level_set_curvature_rhs(mpdg_op *op, const double *nx, const double *ny, co
   MPDG_CUDA(vec_fill<double>(dst, 0.0, op->ndofs, op->stream));
   MPDG_CUDA(level_set_rhs(op->grid(), op->degree, op->h, 1, 0, normal_tolerance, nx, ny, nz, dst, nullptr, nullptr,
                           op->stream, op->banded() ? op->d_band_ls : nullptr, op->band));
+  return MPDG_OK;
+}
+
+int
+mpdg_op_set_wetting(mpdg_op *op, uint32_t faces)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_REINIT)
+    return fail(MPDG_ERR_ARG, "wetting boundary faces belong to the reinitialisation operator");
+  if (faces & ~63u)
+    return fail(MPDG_ERR_ARG, "wetting faces: a 6-bit mask of box faces");
+  op->wetting = faces;
   return MPDG_OK;
 }
 

@@ -130,6 +130,8 @@ namespace mpdg
     int           mask_src = 1;
     const double *band_ls = nullptr; // narrow band: integrands masked where |level set| >= band
     double        band    = 0.0;
+    unsigned      wetting = 0;       // wetting boundary faces (reinitialisation operator)
+    bool          faces_only = false;
   };
   // mode 0: dst += scale * A src on free rows; 1: dst += the rhs integrand of psi_old = src (plain);
   // 2: diag += the tangent's diagonal on free rows

@@ -42,6 +42,8 @@ namespace mpdg
       int           mask_src;
       const double *band_ls; // narrow band (include/meltpooldg/level_set/level_set_tools.hpp:357-368)
       T             band;
+      unsigned      wetting; // wetting boundary faces (bit 2d low / 2d+1 high face of dim d)
+      T             Vend[2 * N], Dend[2 * N]; // basis values / derivatives at x = 0 and x = 1
     };
 
     template <int K, typename T>
@@ -177,6 +179,148 @@ namespace mpdg
         }
     }
 
+    // Wetting boundary faces of the reinitialisation operator (olsson_CG_operator.cpp:550-716), one
+    // thread per boundary cell face: at the face's Gauss points the flux D grad u . n_f with
+    // D = eps_n n n^T + eps_t (I - n n^T) (tangent, src read with constraints; diagonal: per basis
+    // function), or -(-c(psi) n + D grad psi) . n_f with c(psi) = (1 - psi^2) / 2 (rhs, plain reads),
+    // tested with the basis values on the face.
+    template <int K, typename T>
+    __global__ void __launch_bounds__(128)
+    wetting_kernel(const __grid_constant__ ReinitArgs<T, K + 1> a)
+    {
+      constexpr int N = K + 1, N3 = N * N * N;
+      const int     m[3] = {a.g.m[0], a.g.m[1], a.g.m[2]};
+      long long     count[6], total = 0;
+      for (int f = 0; f < 6; ++f)
+        {
+          const int d = f >> 1;
+          count[f]    = ((a.wetting >> f) & 1u) ? (long long)m[(d + 1) % 3] * m[(d + 2) % 3] : 0;
+          total += count[f];
+        }
+      const T hl[3] = {T(1) / a.ih[0], T(1) / a.ih[1], T(1) / a.ih[2]};
+      for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x)
+        {
+          int       f = 0;
+          long long r = t;
+          while (r >= count[f])
+            r -= count[f++];
+          const int d = f >> 1, side = f & 1, ea = (d + 1) % 3, eb = (d + 2) % 3;
+          int       c[3];
+          c[d]  = side ? m[d] - 1 : 0;
+          c[ea] = (int)(r % m[ea]);
+          c[eb] = (int)(r / m[ea]);
+          long long idx[N3];
+          bool      con[N3];
+          T         u[N3], R[N3], nn[3][N3];
+#pragma unroll
+          for (int l = 0; l < N; ++l)
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+#pragma unroll
+              for (int i = 0; i < N; ++i)
+                {
+                  const int       q = (l * N + j) * N + i;
+                  const int       I = K * c[0] + i, J = K * c[1] + j, L = K * c[2] + l;
+                  const long long id = (long long)I + (long long)a.g.n[0] * ((long long)J + (long long)a.g.n[1] * L);
+                  idx[q]            = id;
+                  con[q]            = is_constrained(a.g, I, J, L, id);
+                  u[q]              = (a.mode == 2 || (a.mode == 0 && a.mask_src && con[q])) ? T(0) : a.src[id];
+                  R[q]              = T(0);
+#pragma unroll
+                  for (int e = 0; e < 3; ++e)
+                    nn[e][q] = (T)a.n[e][id];
+                }
+          const T *Vd = a.Vend + side * N, *Dd = a.Dend + side * N;
+          const T  W0 = hl[0] * hl[1] * hl[2] / hl[d], sgn = side ? T(1) : T(-1);
+          for (int qb = 0; qb < N; ++qb)
+            for (int qa = 0; qa < N; ++qa)
+              {
+                // per node: value and the three derivative factors at this face point
+                auto factors = [&](int i, int j, int l, T &val, T gr[3]) {
+                  const int ii[3] = {i, j, l};
+                  T         v[3], dv[3];
+#pragma unroll
+                  for (int e = 0; e < 3; ++e)
+                    {
+                      if (e == d)
+                        {
+                          v[e]  = Vd[ii[e]];
+                          dv[e] = Dd[ii[e]] * a.ih[e];
+                        }
+                      else
+                        {
+                          const int qe = e == ea ? qa : qb;
+                          v[e]         = a.B[qe * N + ii[e]];
+                          dv[e]        = a.G[qe * N + ii[e]] * a.ih[e];
+                        }
+                    }
+                  val   = v[0] * v[1] * v[2];
+                  gr[0] = dv[0] * v[1] * v[2];
+                  gr[1] = v[0] * dv[1] * v[2];
+                  gr[2] = v[0] * v[1] * dv[2];
+                };
+                T uv = T(0), g[3] = {T(0), T(0), T(0)}, nv[3] = {T(0), T(0), T(0)};
+#pragma unroll
+                for (int l = 0; l < N; ++l)
+#pragma unroll
+                  for (int j = 0; j < N; ++j)
+#pragma unroll
+                    for (int i = 0; i < N; ++i)
+                      {
+                        const int q = (l * N + j) * N + i;
+                        T         val, gr[3];
+                        factors(i, j, l, val, gr);
+                        uv += val * u[q];
+#pragma unroll
+                        for (int e = 0; e < 3; ++e)
+                          {
+                            g[e] += gr[e] * u[q];
+                            nv[e] += val * nn[e][q];
+                          }
+                      }
+                const T nrm = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+                const T inv = nrm > a.tol ? T(1) / nrm : T(1) / a.tol;
+#pragma unroll
+                for (int e = 0; e < 3; ++e)
+                  nv[e] *= inv;
+                const T W  = W0 * a.w[qa] * a.w[qb];
+                const T gn = g[0] * nv[0] + g[1] * nv[1] + g[2] * nv[2];
+                T       integrand;
+                if (a.mode == 1)
+                  integrand = -sgn * (-T(0.5) * (T(1) - uv * uv) * nv[d] + a.eps_t * g[d] + (a.eps_n - a.eps_t) * gn * nv[d]);
+                else
+                  integrand = sgn * (a.eps_t * g[d] + (a.eps_n - a.eps_t) * gn * nv[d]);
+#pragma unroll
+                for (int l = 0; l < N; ++l)
+#pragma unroll
+                  for (int j = 0; j < N; ++j)
+#pragma unroll
+                    for (int i = 0; i < N; ++i)
+                      {
+                        const int q = (l * N + j) * N + i;
+                        T         val, gr[3];
+                        factors(i, j, l, val, gr);
+                        if (a.mode == 2)
+                          {
+                            const T pn = gr[0] * nv[0] + gr[1] * nv[1] + gr[2] * nv[2];
+                            R[q] += W * sgn * (a.eps_t * gr[d] + (a.eps_n - a.eps_t) * pn * nv[d]) * val;
+                          }
+                        else
+                          R[q] += W * integrand * val;
+                      }
+              }
+#pragma unroll
+          for (int q = 0; q < N3; ++q)
+            if (!con[q])
+              {
+                if (a.mode == 2)
+                  atomicAdd(a.diag + idx[q], (double)R[q]);
+                else
+                  atomicAdd(a.dst + idx[q], (a.mode == 0 ? a.scale : T(1)) * R[q]);
+              }
+        }
+    }
+
     template <int K, typename T>
     cudaError_t
     launch_reinit(const ReinitLaunch<T> &h, int mode, cudaStream_t s)
@@ -210,9 +354,51 @@ namespace mpdg
       a.mask_src = h.mask_src;
       a.band_ls  = h.band > 0.0 ? h.band_ls : nullptr;
       a.band     = (T)h.band;
+      a.wetting  = h.wetting;
+      // basis values and derivatives at the end points of [0, 1] (Lagrange on the Gauss-Lobatto
+      // nodes: the values are the unit rows of the first and last node; the derivatives are the rows
+      // of the nodal differentiation matrix there, from the barycentric weights)
+      for (int side = 0; side < 2; ++side)
+        {
+          const int jn = side ? N - 1 : 0;
+          for (int i = 0; i < N; ++i)
+            {
+              a.Vend[side * N + i] = i == jn ? T(1) : T(0);
+              double wi = 1.0, wj = 1.0;
+              for (int k = 0; k < N; ++k)
+                {
+                  if (k != i)
+                    wi /= (t.nodes[i] - t.nodes[k]);
+                  if (k != jn)
+                    wj /= (t.nodes[jn] - t.nodes[k]);
+                }
+              double dji = 0.0;
+              if (i != jn)
+                dji = wi / wj / (t.nodes[jn] - t.nodes[i]);
+              else
+                for (int k = 0; k < N; ++k)
+                  if (k != jn)
+                    {
+                      double wk = 1.0;
+                      for (int kk = 0; kk < N; ++kk)
+                        if (kk != k)
+                          wk /= (t.nodes[k] - t.nodes[kk]);
+                      dji -= wk / wj / (t.nodes[jn] - t.nodes[k]);
+                    }
+              a.Dend[side * N + i] = (T)dji;
+            }
+        }
       const long long ncell  = (long long)h.grid.m[0] * h.grid.m[1] * h.grid.m[2];
       const int       blocks = (int)std::max<long long>(1, std::min<long long>((ncell + 127) / 128, 148LL * 16));
-      reinit_kernel<K, T><<<blocks, 128, 0, s>>>(a);
+      if (!h.faces_only)
+        reinit_kernel<K, T><<<blocks, 128, 0, s>>>(a);
+      if (h.wetting && a.n[0] != nullptr)
+        {
+          cudaError_t e = cudaGetLastError();
+          if (e != cudaSuccess)
+            return e;
+          wetting_kernel<K, T><<<148, 128, 0, s>>>(a);
+        }
       return cudaGetLastError();
     }
   } // namespace

@@ -315,6 +315,11 @@ class OlssonOperator(OperatorMatrixFree):
         check(lib().mpdg_op_set_reinit(self._h, float(self.eps_normal), float(self.eps_tangential),
                                        float(self.normal_tolerance), self._v(nx), self._v(ny), self._v(nz)))
 
+    def set_wetting(self, faces: int) -> None:
+        """Wetting boundary faces (OlssonOperator's boundary loops, olsson_CG_operator.cpp:550-716):
+        box faces by bit, 2d low / 2d+1 high face of dimension d; 0 removes them."""
+        check(lib().mpdg_op_set_wetting(self._h, int(faces)))
+
 
 @dataclass
 class LinearSolverData:

@@ -195,3 +195,41 @@ def test_narrow_band_projection_and_rhs(degree, m, faces):
     g.set_narrow_band(None, 0.0)
     g.vmult(y, to_gpu(x))
     assert rel_err(y.cpu().numpy(), projection_apply(om, cm, damping, x)) <= 1e-12
+
+
+@pytest.mark.parametrize("degree,m,faces,wet", [(1, (6, 5, 4), 0, 0b000101), (2, (5, 4, 6), 0b100000, 0b011010),
+                                                (2, (7, 6, 5), 0, 0b111111)])
+def test_wetting_faces_match_oracle(degree, m, faces, wet):
+    """Wetting boundary faces of the reinitialisation operator (olsson_CG_operator.cpp:550-716):
+    vmult, create_rhs and the inverse diagonal with the face terms, against oracle/reinit.py."""
+    import torch
+
+    from oracle.reinit import wetting_rhs, wetting_tangent_apply
+
+    g, om, cm, normal, keep = setup(degree, m, faces)
+    g.set_wetting(wet)
+    x = uniform_dofs(om, seed=1)
+    ref = tangent_apply(om, cm, DT, EPS_N, EPS_T, normal, TOL, x) + \
+        wetting_tangent_apply(om, cm, wet, EPS_N, EPS_T, normal, TOL, x)
+    y = torch.full((om.ndofs,), np.nan, dtype=torch.float64, device="cuda")
+    g.vmult(y, to_gpu(x))
+    assert rel_err(y.cpu().numpy(), ref) <= 1e-12
+    psi = np.tanh(uniform_dofs(om, seed=3))
+    r = torch.full_like(y, np.nan)
+    g.create_rhs(r, to_gpu(psi))
+    rref = create_rhs(om, cm, EPS_N, EPS_T, normal, TOL, psi) + wetting_rhs(om, cm, wet, EPS_N, EPS_T, normal, TOL, psi)
+    assert rel_err(r.cpu().numpy(), rref) <= 1e-12
+    n = om.ndofs
+    dw = np.array([wetting_tangent_apply(om, cm, wet, EPS_N, EPS_T, normal, TOL, np.eye(1, n, i).ravel())[i]
+                   for i in range(n)])
+    dref = diagonal(om, cm, DT, EPS_N, EPS_T, normal, TOL) + dw
+    if cm is not None:
+        dref[cm == 1] = 1.0
+    thr = 1e-14 * max(1.0, np.max(np.abs(dref)))
+    inv = np.where(np.abs(dref) > thr, 1.0 / np.where(dref != 0, dref, 1.0), 1.0)
+    d = torch.empty_like(y)
+    g.compute_inverse_diagonal_from_matrixfree(d)
+    assert rel_err(d.cpu().numpy(), inv) <= 1e-12
+    g.set_wetting(0)
+    g.vmult(y, to_gpu(x))
+    assert rel_err(y.cpu().numpy(), tangent_apply(om, cm, DT, EPS_N, EPS_T, normal, TOL, x)) <= 1e-12

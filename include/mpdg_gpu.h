@@ -254,6 +254,14 @@ MPDG_API int mpdg_op_set_narrow_band(mpdg_op *op, const double *level_set, doubl
    faces' terms of the wetting faces (the reference's diagonal adds those of every boundary face
    when its face integrals are on, :377-405).  0 removes them. */
 MPDG_API int mpdg_op_set_wetting(mpdg_op *op, uint32_t faces);
+/* Advection velocity as a finite-element DoF vector (AdvectionDiffusionOperator with
+   advection_velocity, source/level_set/advection_diffusion_operator.cpp:461-466, 475-479): three
+   DEVICE arrays of n_dofs, the components of an FE_Q(k) field on the operator's lattice, kept by
+   reference (the caller keeps them alive and current) and read plainly per cell; they replace the
+   affine velocity of mpdg_op_params in vmult, create_rhs, the inverse diagonal and the inflow
+   detection of mpdg_op_set_inflow_outflow.  All NULL returns to the affine velocity.  Not with
+   SUPG. */
+MPDG_API int mpdg_op_set_velocity_field(mpdg_op *op, const double *vx, const double *vy, const double *vz);
 /* Inflow/outflow condition of the advection-diffusion operator
    (AdvectionDiffusionOperation::create_inflow_outflow_constraints,
    source/level_set/advection_diffusion_operation.cpp:369-499, with the operator's set_inflow_outflow_bc

@@ -166,6 +166,7 @@ SIGNATURES = [
     ("mpdg_level_set_curvature_rhs", [P, P, P, P, D, P], C.c_int),
     ("mpdg_op_set_narrow_band", [P, P, D], C.c_int),
     ("mpdg_op_set_wetting", [P, C.c_uint32], C.c_int),
+    ("mpdg_op_set_velocity_field", [P, P, P, P], C.c_int),
     ("mpdg_op_distribute_constraints", [P, P, P], C.c_int),
     ("mpdg_vec_alloc", [P, C.POINTER(C.c_void_p)], C.c_int),
     ("mpdg_vec_free", [P], C.c_int),

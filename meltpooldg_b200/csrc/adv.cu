@@ -63,6 +63,7 @@ namespace mpdg
     const T     *b;
     int          mask_src;
     const int   *skip;
+    const double *vfield[3]; // velocity as a DoF vector (three FE_Q(k) components), else affine
   };
 
   // out = M in along a line (in place), M[a*N+b], TR: transpose
@@ -138,7 +139,7 @@ namespace mpdg
   template <typename T, int N, int D>
   __device__ __forceinline__ void
   adv_direction(const T *uq, T *R, const T *tD, const T *tqp, const T *tw3, T c_g, T inv_h, T vd0, T gx, T gy,
-                T gz, T th_adv, T th_dif)
+                T gz, T th_adv, T th_dif, const T *vq = nullptr)
   {
     constexpr int S = D == 0 ? 1 : (D == 1 ? N : N * N);
 #pragma unroll
@@ -162,7 +163,7 @@ namespace mpdg
             {
               const int q  = base + r * S;
               const int qx = q % N, qy = (q / N) % N, qz = q / (N * N);
-              const T   vd = vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
+              const T   vd = vq ? vq[q] : vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
               const T   gw = g[r] * (c_g * tw3[q]);
               R[q]         = fma(th_adv * vd, gw, R[q]);
               g[r]         = th_dif * gw * inv_h;
@@ -310,8 +311,30 @@ namespace mpdg
       (SUPG && K == 2) ? (AdvLayout<K, T>::MINB > 1 ? AdvLayout<K, T>::MINB / 2 : 1) : AdvLayout<K, T>::MINB;
   };
 
-  template <int K, typename T, OutMode MODE, bool SUPG>
-  __global__ void __launch_bounds__(AdvLayout<K, T>::BR::NT, AdvMinBlocks<K, T, SUPG>::value)
+  // Velocity component d of a DoF-vector field at the cell's Gauss points: the cell's nodal values
+  // read plainly (advection_diffusion_operator.cpp:461-466), interpolated by three sweeps of B.
+  template <typename T, int N>
+  __device__ __forceinline__ void
+  field_at_points(const double *f, const GridDesc &g, int cx, int cy, int cz, const T *tB, T *vq)
+  {
+    constexpr int K = N - 1;
+#pragma unroll
+    for (int l = 0; l < N; ++l)
+#pragma unroll
+      for (int j = 0; j < N; ++j)
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+          vq[(l * N + j) * N + i] =
+            (T)f[(long long)(K * cx + i) + (long long)g.n[0] * ((long long)(K * cy + j) + (long long)g.n[1] * (K * cz + l))];
+    sweep<T, N, 0, false>(vq, tB);
+    sweep<T, N, 1, false>(vq, tB);
+    sweep<T, N, 2, false>(vq, tB);
+  }
+
+  // SUPG = true: the stabilised form; VDOF = true: the velocity is a DoF vector (three cell arrays
+  // live in both cases, so both run at the reduced occupancy)
+  template <int K, typename T, OutMode MODE, bool SUPG, bool VDOF = false>
+  __global__ void __launch_bounds__(AdvLayout<K, T>::BR::NT, AdvMinBlocks<K, T, SUPG || VDOF>::value)
   adv_apply_kernel(const __grid_constant__ AdvArgs<T, K + 1> a)
   {
     using LAY             = AdvLayout<K, T>;
@@ -365,8 +388,15 @@ namespace mpdg
     const T inv_h = T(1) / a.h[d];                                                                              \
     const T c_g   = a.det * inv_h;                                                                              \
     const T vd0   = a.vel[d] + a.vel[3 + 3 * d] * x0 + a.vel[4 + 3 * d] * y0 + a.vel[5 + 3 * d] * z0;          \
-    adv_direction<T, N, d>(uq, R, tD, tqp, tw3, c_g, inv_h, vd0, a.vel[3 + 3 * d] * a.h[0],                   \
-                           a.vel[4 + 3 * d] * a.h[1], a.vel[5 + 3 * d] * a.h[2], th_adv, th_dif);              \
+    if constexpr (VDOF)                                                                                         \
+      {                                                                                                         \
+        T vq[N * N * N];                                                                                        \
+        field_at_points<T, N>(a.vfield[d], a.g, cx, cy, cz, tB, vq);                                            \
+        adv_direction<T, N, d>(uq, R, tD, tqp, tw3, c_g, inv_h, vd0, T(0), T(0), T(0), th_adv, th_dif, vq);     \
+      }                                                                                                         \
+    else                                                                                                        \
+      adv_direction<T, N, d>(uq, R, tD, tqp, tw3, c_g, inv_h, vd0, a.vel[3 + 3 * d] * a.h[0],                 \
+                             a.vel[4 + 3 * d] * a.h[1], a.vel[5 + 3 * d] * a.h[2], th_adv, th_dif);            \
   }
           MPDG_ADV_DIR(0)
           MPDG_ADV_DIR(1)
@@ -485,9 +515,16 @@ namespace mpdg
     a.skip     = h.skip;
     a.supg_coef = (T)h.p.supg_coef;
     a.cell_size = (T)(std::sqrt(h.p.h[0] * h.p.h[0] + h.p.h[1] * h.p.h[1] + h.p.h[2] * h.p.h[2]) / std::sqrt(3.0));
-    auto                                   kern = h.p.supg ? adv_apply_kernel<K, T, MODE, true> : adv_apply_kernel<K, T, MODE, false>;
-    static std::atomic<unsigned long long> devices{0}, devices_supg{0};
-    if (cudaError_t e = ensure_smem(kern, LAY::bytes, h.p.supg ? devices_supg : devices); e != cudaSuccess)
+    for (int d = 0; d < 3; ++d)
+      a.vfield[d] = h.p.vfield[d];
+    const bool vdof = h.p.vfield[0] != nullptr;
+    if (vdof && h.p.supg)
+      return cudaErrorInvalidValue; // SUPG with a DoF-vector velocity is not built
+    auto kern = h.p.supg ? adv_apply_kernel<K, T, MODE, true>
+                         : (vdof ? adv_apply_kernel<K, T, MODE, false, true> : adv_apply_kernel<K, T, MODE, false>);
+    static std::atomic<unsigned long long> devices{0}, devices_supg{0}, devices_vdof{0};
+    if (cudaError_t e = ensure_smem(kern, LAY::bytes, h.p.supg ? devices_supg : (vdof ? devices_vdof : devices));
+        e != cudaSuccess)
       return e;
     const unsigned nbricks = (unsigned)h.grid.nbr[0] * h.grid.nbr[1] * h.grid.nbr[2];
     kern<<<nbricks, LAY::BR::NT, LAY::bytes, stream>>>(a);
@@ -772,6 +809,99 @@ namespace mpdg
       adv_supg_diag_kernel<1, T><<<blocks, 128, 0, s>>>(a);
     else
       adv_supg_diag_kernel<2, T><<<blocks, 128, 0, s>>>(a);
+    return cudaGetLastError();
+  }
+
+  // ---- diagonal with a DoF-vector velocity: one thread per cell; the velocity at the Gauss points
+  // from the cell's nodal values, then for each free local DoF i
+  //   sum_q JxW (phi_i^2 / dt + theta_adv (v.grad phi_i) phi_i + theta_dif |grad phi_i|^2)
+  // (MatrixFreeTools::compute_diagonal of the tangent, advection_diffusion_operator.cpp:399-446)
+  struct AdvFieldDiagArgs
+  {
+    GridDesc      g;
+    double        B[MAX_N * MAX_N], G[MAX_N * MAX_N], qw[MAX_N];
+    double        inv_dt, th_adv, th_dif, det, h[3];
+    const double *f[3];
+    double       *diag;
+  };
+
+  template <int K>
+  __global__ void
+  adv_field_diag_kernel(const __grid_constant__ AdvFieldDiagArgs a)
+  {
+    constexpr int   N = K + 1, N3 = N * N * N;
+    const int       m0 = a.g.m[0], m1 = a.g.m[1];
+    const long long ncell = (long long)m0 * m1 * a.g.m[2];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
+      {
+        const int cx = (int)(c % m0), cy = (int)((c / m0) % m1), cz = (int)(c / ((long long)m0 * m1));
+        double    vq[3][N3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          field_at_points<double, N>(a.f[d], a.g, cx, cy, cz, a.B, vq[d]);
+        const double ih[3] = {1.0 / a.h[0], 1.0 / a.h[1], 1.0 / a.h[2]};
+        for (int l = 0; l < N; ++l)
+          for (int j = 0; j < N; ++j)
+            for (int i = 0; i < N; ++i)
+              {
+                const int       I = K * cx + i, J = K * cy + j, L = K * cz + l;
+                const long long idx = (long long)I + (long long)a.g.n[0] * ((long long)J + (long long)a.g.n[1] * L);
+                if (is_constrained(a.g, I, J, L, idx))
+                  continue;
+                double sum = 0.0;
+                for (int qz = 0; qz < N; ++qz)
+                  for (int qy = 0; qy < N; ++qy)
+#pragma unroll
+                    for (int qx = 0; qx < N; ++qx)
+                      {
+                        const int    q  = (qz * N + qy) * N + qx;
+                        const double bx = a.B[qx * N + i], by = a.B[qy * N + j], bz = a.B[qz * N + l];
+                        const double dp[3] = {a.G[qx * N + i] * ih[0] * by * bz, bx * a.G[qy * N + j] * ih[1] * bz,
+                                              bx * by * a.G[qz * N + l] * ih[2]};
+                        const double phi = bx * by * bz;
+                        const double vg  = vq[0][q] * dp[0] + vq[1][q] * dp[1] + vq[2][q] * dp[2];
+                        const double pp  = dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2];
+                        sum += a.qw[qx] * a.qw[qy] * a.qw[qz] * (a.inv_dt * phi * phi + a.th_adv * vg * phi + a.th_dif * pp);
+                      }
+                atomicAdd(a.diag + idx, a.det * sum);
+              }
+      }
+  }
+
+  cudaError_t
+  adv_field_diagonal(const GridDesc &g, int K, const AdvParams &p, double *diag, cudaStream_t s)
+  {
+    if (K < 1 || K > 2 || !p.vfield[0] || !p.vfield[1] || !p.vfield[2])
+      return cudaErrorInvalidValue;
+    AdvFieldDiagArgs a{};
+    const Tables1D  &t = tables(K);
+    const int        n = t.n;
+    for (int q = 0; q < n; ++q)
+      {
+        a.qw[q] = t.qw[q];
+        for (int i = 0; i < n; ++i)
+          {
+            a.B[q * n + i] = t.B[q * n + i];
+            a.G[q * n + i] = t.G[q * n + i];
+          }
+      }
+    a.g      = g;
+    a.inv_dt = p.inv_dt;
+    a.th_adv = p.theta_adv;
+    a.th_dif = p.theta_dif;
+    a.det    = p.h[0] * p.h[1] * p.h[2];
+    for (int d = 0; d < 3; ++d)
+      {
+        a.h[d] = p.h[d];
+        a.f[d] = p.vfield[d];
+      }
+    a.diag                 = diag;
+    const long long ncell  = (long long)g.m[0] * g.m[1] * g.m[2];
+    const int       blocks = (int)std::max<long long>(1, std::min<long long>((ncell + 127) / 128, 148LL * 16));
+    if (K == 1)
+      adv_field_diag_kernel<1><<<blocks, 128, 0, s>>>(a);
+    else
+      adv_field_diag_kernel<2><<<blocks, 128, 0, s>>>(a);
     return cudaGetLastError();
   }
 

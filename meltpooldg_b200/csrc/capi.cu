@@ -109,6 +109,7 @@ struct mpdg_op
   double        eps_n = 0.0, eps_t = 0.0, ntol = 1e-16; // reinitialisation
   unsigned      wetting = 0;                           // reinitialisation: wetting boundary faces
   const double *d_normal[3]{};                           // reinitialisation normal field (not owned)
+  const double *d_vfield[3]{};                           // advection velocity as a DoF vector (not owned)
   double        supg_coef = 0.0;
   const double *d_temp = nullptr; // linearisation temperature of the radiation tangent (not owned)
   int       brick[3]{}, nbr[3]{};
@@ -237,6 +238,8 @@ namespace
       }
     p.supg      = op->supg;
     p.supg_coef = op->supg_coef;
+    for (int d = 0; d < 3; ++d)
+      p.vfield[d] = op->d_vfield[d];
     return p;
   }
 
@@ -546,6 +549,21 @@ namespace
             MPDG_CUDA(vec_invert_rel<double>(r64, op->d_scal, op->ndofs, op->stream));
             if (!std::is_same<T, double>::value)
               MPDG_CUDA(vec_convert<T, double>(diag, r64, op->ndofs, op->stream));
+            return MPDG_OK;
+          }
+        if (op->d_vfield[0])
+          {
+            // DoF-vector velocity: the per-cell diagonal in FP64, inverted with the advection rule
+            double *f64 = std::is_same<T, double>::value ? reinterpret_cast<double *>(diag) : op->vec<double>("vf_diag");
+            if (!f64)
+              return fail(MPDG_ERR_NOMEM, "diagonal work vector");
+            MPDG_CUDA(vec_fill<double>(f64, 0.0, op->ndofs, op->stream));
+            MPDG_CUDA(adv_field_diagonal(g, op->degree, adv_params(op, 0, false), f64, op->stream));
+            MPDG_CUDA(vec_set_constrained<double>(f64, 1.0, g, op->stream));
+            MPDG_CUDA(vec_absmax<double>(f64, op->ndofs, op->d_scal, op->reducer(), op->stream));
+            MPDG_CUDA(vec_invert_rel<double>(f64, op->d_scal, op->ndofs, op->stream));
+            if (!std::is_same<T, double>::value)
+              MPDG_CUDA(vec_convert<T, double>(diag, f64, op->ndofs, op->stream));
             return MPDG_OK;
           }
         // the SUPG part sums terms of both signs: an FP32 diagonal is computed in FP64 and rounded once
@@ -1330,6 +1348,23 @@ mpdg_level_set_curvature_rhs(mpdg_op *op, const double *nx, const double *ny, co
 }
 
 int
+mpdg_op_set_velocity_field(mpdg_op *op, const double *vx, const double *vy, const double *vz)
+{
+  if (int e = check_op(op))
+    return e;
+  if (op->kind != MPDG_ADVDIFF)
+    return fail(MPDG_ERR_ARG, "a velocity field belongs to the advection-diffusion operator");
+  if ((vx || vy || vz) && !(vx && vy && vz))
+    return fail(MPDG_ERR_ARG, "a velocity field needs all three components");
+  if (vx && op->supg)
+    return fail(MPDG_ERR_UNSUPPORTED, "SUPG with a DoF-vector velocity is not supported");
+  op->d_vfield[0] = vx;
+  op->d_vfield[1] = vy;
+  op->d_vfield[2] = vz;
+  return MPDG_OK;
+}
+
+int
 mpdg_op_set_wetting(mpdg_op *op, uint32_t faces)
 {
   if (int e = check_op(op))
@@ -1372,6 +1407,8 @@ mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient)
     return e;
   if (op->kind != MPDG_ADVDIFF)
     return fail(MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator");
+  if (enabled && op->d_vfield[0])
+    return fail(MPDG_ERR_UNSUPPORTED, "SUPG with a DoF-vector velocity is not supported");
   op->supg      = enabled ? 1 : 0;
   op->supg_coef = coefficient;
   return MPDG_OK;
@@ -1418,6 +1455,14 @@ mpdg_op_set_inflow_outflow(mpdg_op *op, uint32_t faces, const double *values)
       dmask.resize(op->ndofs);
       MPDG_CUDA(cudaMemcpy(dmask.data(), op->d_mask, op->ndofs, cudaMemcpyDeviceToHost));
     }
+  // a DoF-vector velocity is evaluated at the support points: its nodal values there
+  std::vector<double> vf[3];
+  if (op->d_vfield[0])
+    for (int d = 0; d < 3; ++d)
+      {
+        vf[d].resize(op->ndofs);
+        MPDG_CUDA(cudaMemcpy(vf[d].data(), op->d_vfield[d], sizeof(double) * op->ndofs, cudaMemcpyDeviceToHost));
+      }
   std::vector<uint8_t>   flag(op->ndofs, 0);
   std::vector<long long> idx;
   for (int L = 0; L < n[2]; ++L)
@@ -1433,7 +1478,9 @@ mpdg_op_set_inflow_outflow(mpdg_op *op, uint32_t faces, const double *values)
               if (!((faces >> f) & 1u) || lat[d] != (side ? n[d] - 1 : 0))
                 continue;
               const double x = xs[0][I], y = xs[1][J], z = xs[2][L];
-              const double v = op->vel[d] + op->vel[3 + 3 * d] * x + op->vel[4 + 3 * d] * y + op->vel[5 + 3 * d] * z;
+              const double v = vf[0].empty() ? op->vel[d] + op->vel[3 + 3 * d] * x + op->vel[4 + 3 * d] * y +
+                                                 op->vel[5 + 3 * d] * z
+                                             : vf[d][q];
               in             = (side ? v : -v) <= 0.0;
             }
           bool con = false;

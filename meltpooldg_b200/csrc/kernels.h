@@ -161,6 +161,7 @@ namespace mpdg
     double h[3];
     int    supg      = 0;   // SUPG streamline stabilisation (ConvectionStabilizationType::SUPG)
     double supg_coef = 0.0; // < 0: tau_c = h_c / max_q |v|, else tau_c = supg_coef h_c
+    const double *vfield[3] = {nullptr, nullptr, nullptr}; // velocity as a DoF vector (else affine)
   };
 
   template <typename T>
@@ -188,6 +189,8 @@ namespace mpdg
   // adds the SUPG part of the diagonal (p.supg) on the free rows
   template <typename T>
   cudaError_t adv_supg_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, cudaStream_t s);
+  // diagonal of the tangent with a DoF-vector velocity (p.vfield), added on the free rows (FP64)
+  cudaError_t adv_field_diagonal(const GridDesc &g, int K, const AdvParams &p, double *diag, cudaStream_t s);
 
   template <typename T>
   void adv_brick_shape(int K, int shape[3]);

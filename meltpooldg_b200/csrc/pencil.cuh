@@ -37,6 +37,9 @@
 #ifndef MPDG_PENCIL_MINB4
 #define MPDG_PENCIL_MINB4 4
 #endif
+#ifndef MPDG_PENCIL_XPAIR
+#define MPDG_PENCIL_XPAIR 0
+#endif
 
 namespace mpdg
 {
@@ -204,7 +207,74 @@ namespace mpdg
                   tb[(c * N + b) * TP + K * BX] = v[b];
               }
             __syncthreads();
-            // ---- 2. x lines: one (cell, mode) line per thread and round
+            // ---- 2. x lines: (cell, mode) lines per thread and round
+#if MPDG_PENCIL_XPAIR
+            // two lines per round, interleaved: twice the independent work per round
+            {
+              auto next = [&](int &c, int &mm) {
+                c += DCX;
+                mm += DM;
+                if (mm >= M)
+                  {
+                    mm -= M;
+                    ++c;
+                  }
+              };
+              int cx = cx_first, m = m_first;
+              while (cx < ncx)
+                {
+                  int cb = cx, mb = m;
+                  next(cb, mb);
+                  const bool hb  = cb < ncx;
+                  const int  cy2 = hb ? cb : cx, my2 = hb ? mb : m; // the second line, or the first again
+                  T          x[N], y[N];
+#pragma unroll
+                  for (int i = 0; i < N; ++i)
+                    {
+                      x[i] = tb[m * TP + K * cx + i];
+                      y[i] = tb[my2 * TP + K * cy2 + i];
+                    }
+                  fwd_line<T, N, 1>(x, 0, we, wo);
+                  fwd_line<T, N, 1>(y, 0, we, wo);
+                  const T kca = kcs[cx], kcb = kcs[cy2];
+                  const T ba = fma(kca, mus[m], alpha), bb = fma(kcb, mus[my2], alpha);
+                  const T kxa = kca * cxg, kxb = kcb * cxg;
+                  T       fa = T(0), fb = T(0);
+#pragma unroll
+                  for (int i = 0; i < N; ++i)
+                    {
+                      const T da = fma(kxa, lam[i], ba), db = fma(kxb, lam[i], bb);
+                      if constexpr (DOT)
+                        {
+                          fa = fma(da * x[i], x[i], fa);
+                          fb = fma(db * y[i], y[i], fb);
+                        }
+                      x[i] *= da;
+                      y[i] *= db;
+                    }
+                  if constexpr (DOT)
+                    dsum += hb ? (double)fa + (double)fb : (double)fa;
+                  bwd_line<T, N, 1>(x, 0, we, wo);
+                  bwd_line<T, N, 1>(y, 0, we, wo);
+#pragma unroll
+                  for (int i = 1; i < K; ++i)
+                    tb[m * TP + K * cx + i] = x[i];
+                  e0[cx * MP + m] = x[0];
+                  e4[cx * MP + m] = x[K];
+                  if (hb)
+                    {
+#pragma unroll
+                      for (int i = 1; i < K; ++i)
+                        tb[mb * TP + K * cb + i] = y[i];
+                      e0[cb * MP + mb] = y[0];
+                      e4[cb * MP + mb] = y[K];
+                    }
+                  cx = cb;
+                  m  = mb;
+                  next(cx, m);
+                }
+            }
+#else
             {
               int cx = cx_first, m = m_first;
               while (cx < ncx)
@@ -243,6 +313,7 @@ namespace mpdg
                     }
                 }
             }
+#endif
             __syncthreads();
             // ---- 3. read back (face points: both adjacent cells), backward y and z transforms
 #pragma unroll

@@ -280,6 +280,15 @@ class AdvectionDiffusionOperator(OperatorMatrixFree):
             raise ValueError("convection stabilization type must be 'none' or 'SUPG'")
         check(lib().mpdg_op_set_supg(self._h, 1 if type == "SUPG" else 0, float(coefficient)))
 
+    def set_velocity_field(self, vx, vy, vz) -> None:
+        """Velocity as a DoF vector (three device vectors on the lattice, kept by reference), as the
+        reference's advection_velocity; None returns to the affine velocity."""
+        self._vfield = (vx, vy, vz)
+        if vx is None:
+            check(lib().mpdg_op_set_velocity_field(self._h, None, None, None))
+        else:
+            check(lib().mpdg_op_set_velocity_field(self._h, self._v(vx), self._v(vy), self._v(vz)))
+
     def set_inflow_outflow_bc(self, faces: int, values) -> int:
         """Inflow/outflow condition on the box faces in `faces` (bit 2d low / 2d+1 high face of dim
         d): AdvectionDiffusionOperation::create_inflow_outflow_constraints and the operator's

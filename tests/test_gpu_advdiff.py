@@ -93,3 +93,55 @@ def test_gmres_solve():
     st = LinearSolver.solve(g, xd, to_gpu(b), LinearSolverData("GMRES", "Diagonal", rel_tolerance=1e-10))
     assert abs(st.iterations - it_ref) <= 1
     assert rel_err(xd.cpu().numpy(), x_ref) <= 1e-8
+
+
+@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0), (2, (8, 9, 6), 0b010011), (2, (33, 5, 4), 0)])
+def test_velocity_field_matches_oracle(degree, m, faces):
+    """Advection velocity as a DoF vector (advection_diffusion_operator.cpp:461-466, 475-479): vmult
+    (FP64, FP32), create_rhs, the inverse diagonal and a GMRES solve against oracle/advection_field.py,
+    and a field sampled from the affine velocity reproduces the affine operator."""
+    import torch
+
+    from meltpooldg_b200.operators import AdvectionDiffusionOperator, LinearSolver, LinearSolverData
+    from oracle import advection_field as AF
+    from tests.gpu_util import meshes, rel_err, to_gpu
+
+    om, gm, cm = meshes(degree, m, faces=faces, length=(1.0, 0.8, 1.1))
+    X, Y, Z = om.coords()
+    field = [np.sin(3.0 * Y) * (Z + 0.2), np.cos(2.0 * X) - Z * Z, 0.5 * X * Y - 0.1]
+    dt, theta, eps = 5e-3, 0.5, 2e-3
+    g = AdvectionDiffusionOperator(gm, dt=dt, theta=theta, diffusivity=eps)
+    fd = [to_gpu(c) for c in field]
+    g.set_velocity_field(*fd)
+    u = uniform_dofs(om, seed=1)
+    ref = AF.tangent_apply(om, cm, field, dt, theta, eps, u)
+    y = torch.full((om.ndofs,), np.nan, dtype=torch.float64, device="cuda")
+    g.vmult(y, to_gpu(u))
+    assert rel_err(y.cpu().numpy(), ref) <= 1e-12
+    y32 = torch.empty(om.ndofs, dtype=torch.float32, device="cuda")
+    g.vmult(y32, to_gpu(u, torch.float32))
+    assert rel_err(y32.cpu().numpy(), ref) <= 2e-6
+    r = torch.zeros_like(y)
+    g.create_rhs(r, to_gpu(u))
+    assert rel_err(r.cpu().numpy(), AF.create_rhs(om, cm, field, dt, theta, eps, u)) <= 1e-12
+    d = torch.empty_like(y)
+    g.compute_inverse_diagonal_from_matrixfree(d)
+    assert rel_err(d.cpu().numpy(), AF.inverse_diagonal(om, cm, field, dt, theta, eps)) <= 1e-12
+    b = uniform_dofs(om, seed=2, cmask=cm)
+    x = torch.zeros_like(y)
+    LinearSolver.solve(g, x, to_gpu(b), LinearSolverData("GMRES", "Diagonal", rel_tolerance=1e-10))
+    res = b - AF.tangent_apply(om, cm, field, dt, theta, eps, x.cpu().numpy())
+    assert np.linalg.norm(res) <= 1.01e-10 * np.linalg.norm(b)
+    # an affine field sampled at the support points is the affine operator
+    vel = [0.2, -0.1, 0.05, 0.0, -1.0, 0.3, 1.0, 0.0, -0.2, 0.1, 0.2, 0.0]
+    aff = [vel[k] + vel[3 + 3 * k] * X + vel[4 + 3 * k] * Y + vel[5 + 3 * k] * Z for k in range(3)]
+    om0 = om
+    ga = AdvectionDiffusionOperator(gm, dt=dt, theta=theta, diffusivity=eps, velocity=vel)
+    gf = AdvectionDiffusionOperator(gm, dt=dt, theta=theta, diffusivity=eps)
+    af = [to_gpu(c) for c in aff]
+    gf.set_velocity_field(*af)
+    ya, yf = torch.empty_like(y), torch.empty_like(y)
+    ga.vmult(ya, to_gpu(u))
+    gf.vmult(yf, to_gpu(u))
+    assert rel_err(yf.cpu().numpy(), ya.cpu().numpy()) <= 1e-12
+    assert om0.ndofs == om.ndofs and g.device_errors() == 0

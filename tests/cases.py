@@ -89,3 +89,18 @@ def vortex_inflow(dim: int):
         eps = 0.5 * (h * np.sqrt(2)) / np.sqrt(2)
         faces = 0b001111
     return mesh, np.tanh(sd / (2 * eps)), vel, faces
+
+
+def vortex_supg():
+    """applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf_supg.json: the 2-D vortex
+    case (matrix-free by default) with SUPG, coefficient -1 (tau_c = h_c / max |v|).  The SUPG cell
+    size is the cell diameter / sqrt(dim) (source/core/scratch_data.cpp:262-277), h for the 2-D
+    squares; the extrusion here is one cube cell deep (depth h), whose diameter / sqrt(3) is the same
+    h.  Every term then scales with the depth, so the solution is the 2-D one and the 2-D L2 norm is
+    the 3-D norm divided by sqrt(h).  Returns the mesh, the initial field, the Dirichlet mask, the
+    velocity and h."""
+    m, h = 32, 2.0 / 32
+    mesh0, phi0, mask0, vel = vortex(2)
+    mesh = Mesh(1, (m, m, 1), origin=(-1, -1, 0), length=(2, 2, h))
+    assert mesh.ndofs == mesh0.ndofs  # the same lattice, only the depth differs
+    return mesh, phi0, mask0, vel, h

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from oracle.oracle import Operator as OOp
-from tests.cases import heat_unidirectional, vortex, vortex_inflow
+from tests.cases import heat_unidirectional, vortex, vortex_inflow, vortex_supg
 from tests.gpu_util import to_gpu
 
 pytestmark = pytest.mark.gpu
@@ -123,5 +123,36 @@ def test_vortex_inflow_outflow_log_gpu(dim, key):
         x_o[inflow == 1] = -1.0
         phi_o = x_o
         assert np.max(np.abs(phi.cpu().numpy() - phi_o)) <= 1e-10
+    assert np.max(np.abs(np.array(out) - ref) / ref) < 5e-8
+    assert g.device_errors() == 0
+
+
+def test_vortex_supg_log_gpu():
+    """advection_diffusion_vortex_mf_supg.mpirun=4.output through the GPU operator with SUPG
+    (coefficient -1): Dirichlet lifting, GMRES(30) with the Jacobi preconditioner, 5 steps."""
+    import torch
+
+    from meltpooldg_b200.operators import AdvectionDiffusionOperator, LinearSolver, LinearSolverData, Mesh
+
+    om, phi0, mask, vel, h = vortex_supg()
+    gm = Mesh(1, om.m, om.origin, om.length, dirichlet_mask=mask)
+    g = AdvectionDiffusionOperator(gm, dt=0.01, theta=0.5, diffusivity=0.0, velocity=vel)
+    g.set_convection_stabilization("SUPG", -1.0)
+    norm = OOp(om, "heat")
+    ref = np.array([float(v) for v in GOLD["advdiff_vortex_supg_2d_q1"]["values"]])
+    phi = to_gpu(phi0)
+    mask_t = torch.tensor(mask, device="cuda").bool()
+    minus_one = torch.full_like(phi, -1.0)
+    data = LinearSolverData("GMRES", "Diagonal", rel_tolerance=1e-12)
+    out = []
+    for _ in range(5):
+        old = phi.clone()
+        rhs = torch.empty_like(phi)
+        g.create_rhs_and_apply_dirichlet(rhs, old, minus_one)
+        x = old.clone()
+        LinearSolver.solve(g, x, rhs, data)
+        x[mask_t] = -1.0
+        phi = x
+        out.append(norm.l2_norm(phi.cpu().numpy()) / np.sqrt(h))
     assert np.max(np.abs(np.array(out) - ref) / ref) < 5e-8
     assert g.device_errors() == 0

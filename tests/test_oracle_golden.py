@@ -5,7 +5,7 @@ import os
 import numpy as np
 
 from oracle.oracle import Operator, inflow_dofs, solve
-from tests.cases import heat_unidirectional, vortex, vortex_inflow
+from tests.cases import heat_unidirectional, vortex, vortex_inflow, vortex_supg
 
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_logs.json")))
 
@@ -98,3 +98,49 @@ def test_vortex_inflow_outflow_logs():
         ref = np.array([float(v) for v in GOLD[key]["values"]])
         got = _vortex_inflow_norms(dim)
         assert np.max(np.abs(got - ref) / ref) < FLOAT_NORM_NOISE, (dim, got, ref)
+
+
+def supg_vortex_norms(steps=5):
+    """The SUPG vortex case restated: the oracle's affine advection operator plus oracle/supg.py, the
+    Dirichlet lifting (utilities_matrixfree.hpp:39-100) and right-preconditioned GMRES(30) to 1e-12
+    (scipy, the same Krylov space); norms of the 2-D field."""
+    import scipy.sparse.linalg as spla
+
+    from oracle import supg as S
+
+    mesh, phi, mask, vel, h = vortex_supg()
+    dt, theta, coef = 0.01, 0.5, -1.0
+    op = Operator(mesh, "advdiff", cmask=mask, dt=dt, theta=theta, eps=0.0, vel=vel)
+    nobc = op.with_(cmask=None)
+    n = mesh.ndofs
+
+    def A(u):
+        return op.vmult(u) + S.supg_apply(mesh, mask, vel, coef, 1.0 / dt, theta, 0.0, u)
+
+    d = op.diagonal() + S.supg_diagonal(mesh, mask, vel, coef, 1.0 / dt, theta, 0.0)
+    d[mask == 1] = 1.0
+    thr = 1e-14 * max(1.0, np.max(np.abs(d)))
+    inv = np.where(np.abs(d) > thr, 1.0 / d, 1.0)
+    out = []
+    for _ in range(steps):
+        old = phi.copy()
+        bc = np.where(mask == 1, -1.0, 0.0)
+        rhs = -(nobc.vmult(bc) + S.supg_apply(mesh, None, vel, coef, 1.0 / dt, theta, 0.0, bc))
+        nobc.create_rhs(rhs, old)
+        rhs += S.supg_apply(mesh, None, vel, coef, 1.0 / dt, theta - 1.0, 0.0, old, plain=True)
+        rhs[mask == 1] = 0.0
+        Aop = spla.LinearOperator((n, n), matvec=lambda v: A(inv * v))  # right preconditioning
+        y, info = spla.gmres(Aop, rhs - A(old), rtol=1e-13, atol=0.0, restart=30, maxiter=1000)
+        assert info == 0
+        x = old + inv * y
+        x[mask == 1] = -1.0
+        phi = x
+        out.append(op.l2_norm(phi) / np.sqrt(h))
+    return np.array(out)
+
+
+def test_vortex_supg_log():
+    """advection_diffusion_vortex_mf_supg.mpirun=4.output: SUPG pinned on the reference's log."""
+    ref = np.array([float(v) for v in GOLD["advdiff_vortex_supg_2d_q1"]["values"]])
+    got = supg_vortex_norms()
+    assert np.max(np.abs(got - ref) / ref) < FLOAT_NORM_NOISE, (got, ref)

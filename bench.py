@@ -462,12 +462,12 @@ def run_advection(torch, stream, steps=10):
     return out
 
 
-def run_adjoint(torch, stream, fd_dirs=3):
+def run_adjoint(torch, stream, fd_dirs=20):
     """Adjoint of the transient heat problem: 48^3 FE_Q(2) cells, 20 implicit-Euler steps (dt 1e-3,
     T0 = 0, homogeneous Dirichlet), moving Gaussian source A exp(-2|x - x0(t)|^2 / 0.05^2), A = 100,
     x0(t) = (0.2 + 30 t, 0.5, 0.95); log k ~ N(0, 0.3^2) (seed 5), target from seed 6; checkpoints
     every 5 steps.  Times J + dJ/dz (110,592 cells) + dJ/dA, and checks the gradient against central
-    differences (h = 1e-6) on a few random directions (seed 7)."""
+    differences (h = 1e-6) on 20 random directions (seed 7)."""
     from meltpooldg_b200.adjoint import TransientHeatAdjoint
     from meltpooldg_b200.inputs import moving_gaussian, normal_cells, unit_directions
     from meltpooldg_b200.operators import HeatDiffuseOperator, Mesh

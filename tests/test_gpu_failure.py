@@ -54,7 +54,8 @@ def test_stale_ticket_makes_the_wait_give_up(degree, cells):
     op.vmult(y, x)
     torch.cuda.synchronize()
     assert op.device_errors() == 0
-    assert torch.equal(y, ref)
+    # brick faces are summed with atomics, so repeated applies agree to rounding, not bit for bit
+    assert torch.max(torch.abs(y - ref)).item() <= 1e-13 * torch.max(torch.abs(ref)).item()
 
 
 @pytest.mark.gpu

@@ -99,3 +99,19 @@ def test_rhs_is_minus_residual():
     ref[cm == 1] = 0.0
     assert np.allclose(rhs, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
     assert nb is not None
+
+
+@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0b101101), (2, (17, 9, 6), 63), (3, (8, 7, 9), 0),
+                                            (4, (10, 6, 5), 0b010010)])
+def test_batched_cpu_apply_matches_the_quadrature_form(degree, m, faces):
+    """The cell-batched SIMD heat apply (the timed CPU baseline) equals the oracle's apply."""
+    from meltpooldg_b200.inputs import normal_cells, uniform_dofs
+    from oracle.oracle import Mesh, Operator
+
+    om = Mesh(degree, m, length=(1.0, 0.8, 1.2))
+    cm = om.face_mask(faces) if faces else None
+    kc = np.exp(normal_cells(om, seed=2, sigma=0.5))
+    op = Operator(om, "heat", cmask=cm, rho_cp=1.3, dt=1e-2, k_cell=kc)
+    x = uniform_dofs(om, seed=1)
+    a = op.vmult(x)
+    assert np.max(np.abs(op.vmult_batched(x) - a)) <= 1e-13 * np.max(np.abs(a))

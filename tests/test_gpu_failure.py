@@ -67,7 +67,10 @@ def test_solver_reports_timeout_after_a_wait_gave_up():
 
     mesh, op = _op(2, (64, 4, 8))
     lib = L.lib()
-    b = torch.tensor(uniform_dofs(mesh, seed=3, cmask=None), device="cuda")
+    from oracle.oracle import Mesh as OMesh
+
+    cm = OMesh(2, (64, 4, 8)).face_mask(63)  # right-hand side zero on the Dirichlet rows
+    b = torch.tensor(uniform_dofs(mesh, seed=3, cmask=cm), device="cuda")
     x = torch.zeros_like(b)
     assert lib.mpdg_op_test_set_wait_limit(op._h, SHORT) == L.MPDG_OK
     assert lib.mpdg_op_test_set_ticket(op._h, 1) == L.MPDG_OK

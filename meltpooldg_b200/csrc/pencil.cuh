@@ -208,7 +208,67 @@ namespace mpdg
               }
             __syncthreads();
             // ---- 2. x lines: (cell, mode) lines per thread and round
-#if MPDG_PENCIL_XPAIR
+#if MPDG_PENCIL_XPAIR == 2
+            // K consecutive threads share a cell and take its modes g, g + K, ... (g = thread % K),
+            // two lines per round: the cell's conductivity is read once, the line offsets advance by
+            // a constant, and a warp's 8 cells x K mode groups hit distinct banks
+            {
+              constexpr int G = NT / BX; // threads per cell (= K)
+              const int     cxg_ = p / G, g = p % G;
+              if (cxg_ < ncx)
+                {
+                  const T kc  = kcs[cxg_];
+                  const T kcx = kc * cxg;
+                  T      *tl  = tb + K * cxg_;
+                  for (int m = g; m < M; m += 2 * G)
+                    {
+                      const int  mb = m + G;
+                      const bool hb = mb < M;
+                      const int  m2 = hb ? mb : m;
+                      T          x[N], y[N];
+#pragma unroll
+                      for (int i = 0; i < N; ++i)
+                        {
+                          x[i] = tl[m * TP + i];
+                          y[i] = tl[m2 * TP + i];
+                        }
+                      fwd_line<T, N, 1>(x, 0, we, wo);
+                      fwd_line<T, N, 1>(y, 0, we, wo);
+                      const T ba = fma(kc, mus[m], alpha), bb = fma(kc, mus[m2], alpha);
+                      T       fa = T(0), fb = T(0);
+#pragma unroll
+                      for (int i = 0; i < N; ++i)
+                        {
+                          const T da = fma(kcx, lam[i], ba), db = fma(kcx, lam[i], bb);
+                          if constexpr (DOT)
+                            {
+                              fa = fma(da * x[i], x[i], fa);
+                              fb = fma(db * y[i], y[i], fb);
+                            }
+                          x[i] *= da;
+                          y[i] *= db;
+                        }
+                      if constexpr (DOT)
+                        dsum += hb ? (double)fa + (double)fb : (double)fa;
+                      bwd_line<T, N, 1>(x, 0, we, wo);
+                      bwd_line<T, N, 1>(y, 0, we, wo);
+#pragma unroll
+                      for (int i = 1; i < K; ++i)
+                        tl[m * TP + i] = x[i];
+                      e0[cxg_ * MP + m] = x[0];
+                      e4[cxg_ * MP + m] = x[K];
+                      if (hb)
+                        {
+#pragma unroll
+                          for (int i = 1; i < K; ++i)
+                            tl[mb * TP + i] = y[i];
+                          e0[cxg_ * MP + mb] = y[0];
+                          e4[cxg_ * MP + mb] = y[K];
+                        }
+                    }
+                }
+            }
+#elif MPDG_PENCIL_XPAIR
             // two lines per round, interleaved: twice the independent work per round
             {
               auto next = [&](int &c, int &mm) {

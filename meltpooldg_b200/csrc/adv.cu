@@ -64,6 +64,10 @@ namespace mpdg
     int          mask_src;
     const int   *skip;
     const double *vfield[3]; // velocity as a DoF vector (three FE_Q(k) components), else affine
+    // cell-independent factors per direction d and Gauss point q (N^3 <= 27 used):
+    //   pa = th_adv det / h_d w_q,  pb = pa (G_d. (h (x) qp_q)),  pd = th_dif det / h_d^2 w_q;
+    // pm = det inv_dt w_q.  The velocity term of a cell is (vd0 pa + pb) g, vd0 = v_d(cell origin).
+    T pa[3][27], pb[3][27], pd[3][27], pm[27];
   };
 
   // out = M in along a line (in place), M[a*N+b], TR: transpose
@@ -134,12 +138,13 @@ namespace mpdg
 
   // One direction d of the advection and diffusion terms, line by line (a line along d at a time):
   //   g = D_d uq along the line;  R += theta_adv v_d JxW g / h_d;  R += D_d^T (theta_dif JxW g / h_d^2)
-  // Only the k+1 values of one line are live besides uq and R (the whole-array form needs a third
-  // cell array); the arithmetic and its order per entry are those of the whole-array sweeps.
+  // with the cell-independent factors of each point precomputed (AdvArgs::pa, pb, pd): the velocity
+  // weight is vd0 pa_q + pb_q (affine field) or vq_q pa_q (DoF-vector field).  Only the k+1 values of
+  // one line are live besides uq and R.
   template <typename T, int N, int D>
   __device__ __forceinline__ void
-  adv_direction(const T *uq, T *R, const T *tD, const T *tqp, const T *tw3, T c_g, T inv_h, T vd0, T gx, T gy,
-                T gz, T th_adv, T th_dif, const T *vq = nullptr)
+  adv_direction(const T *uq, T *R, const T *tD, const T *pa, const T *pb, const T *pd, T vd0, bool dif,
+                const T *vq = nullptr)
   {
     constexpr int S = D == 0 ? 1 : (D == 1 ? N : N * N);
 #pragma unroll
@@ -161,14 +166,12 @@ namespace mpdg
 #pragma unroll
           for (int r = 0; r < N; ++r)
             {
-              const int q  = base + r * S;
-              const int qx = q % N, qy = (q / N) % N, qz = q / (N * N);
-              const T   vd = vq ? vq[q] : vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
-              const T   gw = g[r] * (c_g * tw3[q]);
-              R[q]         = fma(th_adv * vd, gw, R[q]);
-              g[r]         = th_dif * gw * inv_h;
+              const int q = base + r * S;
+              const T   w = vq ? vq[q] * pa[q] : fma(vd0, pa[q], pb[q]);
+              R[q]        = fma(w, g[r], R[q]);
+              g[r] *= pd[q];
             }
-          if (th_dif != T(0))
+          if (dif)
 #pragma unroll
             for (int r = 0; r < N; ++r)
               {
@@ -377,26 +380,22 @@ namespace mpdg
         sweep<T, N, 2, false>(uq, tB);
         // cell origin and the velocity there
         const T x0 = a.origin[0] + a.h[0] * cx, y0 = a.origin[1] + a.h[1] * cy, z0 = a.origin[2] + a.h[2] * cz;
-        const T c_mass = a.det * a.inv_dt;
 #pragma unroll
         for (int q = 0; q < N * N * N; ++q)
-          R[q] = (tw3[q] * c_mass) * uq[q];
+          R[q] = a.pm[q] * uq[q];
         {
           const T th_adv = a.th_adv, th_dif = a.th_dif;
 #define MPDG_ADV_DIR(d)                                                                                         \
   {                                                                                                             \
-    const T inv_h = T(1) / a.h[d];                                                                              \
-    const T c_g   = a.det * inv_h;                                                                              \
-    const T vd0   = a.vel[d] + a.vel[3 + 3 * d] * x0 + a.vel[4 + 3 * d] * y0 + a.vel[5 + 3 * d] * z0;          \
+    const T vd0 = a.vel[d] + a.vel[3 + 3 * d] * x0 + a.vel[4 + 3 * d] * y0 + a.vel[5 + 3 * d] * z0;            \
     if constexpr (VDOF)                                                                                         \
       {                                                                                                         \
         T vq[N * N * N];                                                                                        \
         field_at_points<T, N>(a.vfield[d], a.g, cx, cy, cz, tB, vq);                                            \
-        adv_direction<T, N, d>(uq, R, tD, tqp, tw3, c_g, inv_h, vd0, T(0), T(0), T(0), th_adv, th_dif, vq);     \
+        adv_direction<T, N, d>(uq, R, tD, a.pa[d], a.pb[d], a.pd[d], vd0, th_dif != T(0), vq);                  \
       }                                                                                                         \
     else                                                                                                        \
-      adv_direction<T, N, d>(uq, R, tD, tqp, tw3, c_g, inv_h, vd0, a.vel[3 + 3 * d] * a.h[0],                 \
-                             a.vel[4 + 3 * d] * a.h[1], a.vel[5 + 3 * d] * a.h[2], th_adv, th_dif);            \
+      adv_direction<T, N, d>(uq, R, tD, a.pa[d], a.pb[d], a.pd[d], vd0, th_dif != T(0));                       \
   }
           MPDG_ADV_DIR(0)
           MPDG_ADV_DIR(1)
@@ -517,6 +516,29 @@ namespace mpdg
     a.cell_size = (T)(std::sqrt(h.p.h[0] * h.p.h[0] + h.p.h[1] * h.p.h[1] + h.p.h[2] * h.p.h[2]) / std::sqrt(3.0));
     for (int d = 0; d < 3; ++d)
       a.vfield[d] = h.p.vfield[d];
+    {
+      // cell-independent point factors (see AdvArgs), in double, rounded once
+      const Tables1D &t   = tables(K);
+      const double    det = h.p.h[0] * h.p.h[1] * h.p.h[2];
+      const double    ta = h.scale * h.p.theta_adv, td = h.scale * h.p.theta_dif, ti = h.scale * h.p.inv_dt;
+      for (int qz = 0; qz < N; ++qz)
+        for (int qy = 0; qy < N; ++qy)
+          for (int qx = 0; qx < N; ++qx)
+            {
+              const int    q  = (qz * N + qy) * N + qx;
+              const double w3 = t.qw[qx] * t.qw[qy] * t.qw[qz];
+              a.pm[q]         = (T)(det * ti * w3);
+              for (int d = 0; d < 3; ++d)
+                {
+                  const double pa = ta * det / h.p.h[d] * w3;
+                  const double gv = h.p.vel[3 + 3 * d] * h.p.h[0] * t.qp[qx] + h.p.vel[4 + 3 * d] * h.p.h[1] * t.qp[qy] +
+                                    h.p.vel[5 + 3 * d] * h.p.h[2] * t.qp[qz];
+                  a.pa[d][q] = (T)pa;
+                  a.pb[d][q] = (T)(pa * gv);
+                  a.pd[d][q] = (T)(td * det / (h.p.h[d] * h.p.h[d]) * w3);
+                }
+            }
+    }
     const bool vdof = h.p.vfield[0] != nullptr;
     if (vdof && h.p.supg)
       return cudaErrorInvalidValue; // SUPG with a DoF-vector velocity is not built

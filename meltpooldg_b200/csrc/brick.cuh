@@ -337,40 +337,54 @@ namespace mpdg
   brick_init_publish(const BR &br, const SyncDesc &s, T *dst, const T *bvec, unsigned acc_lo_z = 0)
   {
     static_assert(MODE != OutMode::Add, "Add mode needs no initialisation");
-    constexpr int F0 = BR::PY * BR::PZ, F1 = BR::PX * BR::PZ, F2 = BR::PX * BR::PY;
-    for (int f = threadIdx.x; f < 2 * (F0 + F1 + F2); f += BR::NT)
+    auto put = [&](int px, int py, int pz) {
+      if (br.low_shared(px, py, pz))
+        return;
+      if (acc_lo_z && pz == 0 && br.g0[2] == 0)
+        return; // accumulated onto the previous slab's values, never reset
+      const int idx = br.index(px, py, pz);
+      dst[idx]      = (MODE == OutMode::BPlus) ? bvec[idx] : T(0);
+    };
+    // face by face (side 0: low face, only at the domain boundary; side 1: high face), the faces
+    // normal to y and z in rows along x so that consecutive threads store consecutive points
+#pragma unroll
+    for (int side = 0; side < 2; ++side)
       {
-        const int  side = f / (F0 + F1 + F2); // 0: low faces, 1: high faces
-        const int  q    = f % (F0 + F1 + F2);
-        int        px, py, pz;
-        bool       use;
-        if (q < F0)
-          {
-            py  = q % BR::PY;
-            pz  = q / BR::PY;
-            px  = side ? br.nv[0] - 1 : 0;
-            use = side ? true : !br.lo_sh[0];
-          }
-        else if (q < F0 + F1)
-          {
-            px  = (q - F0) % BR::PX;
-            pz  = (q - F0) / BR::PX;
-            py  = side ? br.nv[1] - 1 : 0;
-            use = side ? true : !br.lo_sh[1];
-          }
-        else
-          {
-            px  = (q - F0 - F1) % BR::PX;
-            py  = (q - F0 - F1) / BR::PX;
-            pz  = side ? br.nv[2] - 1 : 0;
-            use = side ? true : !br.lo_sh[2];
-          }
-        if (!use || !br.inside(px, py, pz) || br.low_shared(px, py, pz))
+        if (side == 0 && br.lo_sh[0])
           continue;
-        if (acc_lo_z && pz == 0 && br.g0[2] == 0)
-          continue; // accumulated onto the previous slab's values, never reset
-        const int idx = br.index(px, py, pz);
-        dst[idx]      = (MODE == OutMode::BPlus) ? bvec[idx] : T(0);
+        const int px = side ? br.nv[0] - 1 : 0;
+        for (int e = threadIdx.x; e < BR::PY * BR::PZ; e += BR::NT)
+          {
+            const int py = e % BR::PY, pz = e / BR::PY;
+            if (py < br.nv[1] && pz < br.nv[2])
+              put(px, py, pz);
+          }
+      }
+#pragma unroll
+    for (int side = 0; side < 2; ++side)
+      {
+        if (side == 0 && br.lo_sh[1])
+          continue;
+        const int py = side ? br.nv[1] - 1 : 0;
+        for (int e = threadIdx.x; e < BR::PX * BR::PZ; e += BR::NT)
+          {
+            const int px = e % BR::PX, pz = e / BR::PX;
+            if (px < br.nv[0] && pz < br.nv[2])
+              put(px, py, pz);
+          }
+      }
+#pragma unroll
+    for (int side = 0; side < 2; ++side)
+      {
+        if (side == 0 && br.lo_sh[2])
+          continue;
+        const int pz = side ? br.nv[2] - 1 : 0;
+        for (int e = threadIdx.x; e < BR::PX * BR::PY; e += BR::NT)
+          {
+            const int px = e % BR::PX, py = e / BR::PX;
+            if (px < br.nv[0] && py < br.nv[1])
+              put(px, py, pz);
+          }
       }
     __syncthreads();
     if (threadIdx.x == 0)

@@ -621,7 +621,7 @@ namespace
   fused_cg_applies(const mpdg_op *op)
   {
     return op->fused_cg && op->kind == MPDG_HEAT && op->degree == 2 && op->d_mask == nullptr && op->with_bc &&
-           !op->tangent_faces() && !op->solid;
+           !op->tangent_faces() && !op->solid && !op->banded();
   }
 
   // Preconditioned CG with one launch per iteration (cgfused.cu): the same iterates as cg_solve in
@@ -778,8 +778,9 @@ namespace
       return e;
     MPDG_CUDA(cg_init<T>(r, invd, p, op->d_cg, hist, op->reducer(), n, op->stream));
     // heat operators without a per-DoF mask fuse p^T A p into the apply and set alpha on the device
+    // (not the narrow-band projection, whose apply is the point-wise kernel)
     const bool fused = op->kind == MPDG_HEAT && op->d_part != nullptr && !op->tangent_faces() && !op->solid &&
-                       heat_apply_fuses_dot(op->degree, op->d_mask != nullptr, true);
+                       !op->banded() && heat_apply_fuses_dot(op->degree, op->d_mask != nullptr, true);
     DotSink    sink;
     sink.part  = op->d_part;
     sink.alpha = &op->d_cg->alpha;

@@ -16,8 +16,11 @@
 // forms z_0, p_0 = z_0 and v_0 only.  Per iteration the sweep reads x, r, p, v, d and writes x, r,
 // p, v: s (9 N + N_c) bytes, against s (13 N + N_c) for separate update / apply / update passes.
 //
-// Tiles.  A CTA owns the lattice points of 32 x TY cells in x, y and a segment of TZ cell layers in
-// z, and marches through the segment layer by layer.  It also computes the cells of one halo layer
+// Tiles.  The lattice is cut into columns of 32 x TY cells in x, y; the columns' cell layers, taken
+// column after column, are dealt out in equal contiguous ranges to a grid of one CTA per resident
+// slot, so every SM gets the same number of layers.  A CTA's range is one or a few pieces (a segment
+// of z layers of one column); it owns the lattice points of each piece and marches through it
+// layer by layer.  It also computes the cells of one halo layer
 // on its low side in x, y and z (a halo column warp, a halo row warp, a halo cell layer), so every
 // owned point receives all of its cell contributions inside the CTA: no atomics, no inter-CTA
 // waits, and each owned point's update and dot products are done by one thread.  The vectors use a
@@ -67,8 +70,9 @@ namespace mpdg
       static constexpr size_t STAGE_B = align(sizeof(T) * PLANE);      // one vector, one plane
       static constexpr size_t O_STAGE = 0;                              // [2 slots][NV] planes
       static constexpr size_t O_PRING = O_STAGE + 2 * NV * STAGE_B;     // [3] planes of p_k
-      static constexpr size_t O_ZD    = O_PRING + 3 * STAGE_B;          // [3] owned planes of (z, d)
-      static constexpr size_t O_YX    = O_ZD + align(3 * sizeof(T) * 2 * OPL);
+      static constexpr size_t O_ZS    = O_PRING + 3 * STAGE_B;          // [3] owned planes of z
+      static constexpr size_t O_DS    = O_ZS + align(3 * sizeof(T) * OPL); // [3] owned planes of d
+      static constexpr size_t O_YX    = O_DS + align(3 * sizeof(T) * OPL);
       static constexpr size_t O_HX    = O_YX + align(sizeof(T) * (TY + 1) * 9 * 32);
       static constexpr size_t O_RED   = O_HX + align(sizeof(T) * (TY + 1) * 9);
       static constexpr size_t O_BAR   = O_RED + align(sizeof(double) * NW * 5);
@@ -81,7 +85,8 @@ namespace mpdg
       int           m[3], n[3];
       int           P0;          // padded x pitch (elements)
       unsigned      faces;       // Dirichlet faces (bit 2d low, 2d+1 high of dim d)
-      int           tiles_x, tiles_y, TZ, ty;
+      int           tiles_x, tiles_y, ty;
+      long long     layers;      // columns x cell layers, dealt out in equal ranges to the CTAs
       T             alpha_m, cx, cy, cz; // mass coefficient, stiffness geometry factors
       T             kconst;
       const T      *kcell;
@@ -89,7 +94,7 @@ namespace mpdg
       T            *x;           // in place (owned points)
       T            *r_out, *p_out, *v_out;
       CGState      *st;
-      double       *part;        // 5 partial sums per tile
+      double       *part;        // 5 partial sums per CTA
       unsigned     *counter;     // last-CTA ticket (0 between launches)
       double       *hist;
       int          *err;
@@ -177,7 +182,8 @@ namespace mpdg
       extern __shared__ __align__(128) unsigned char smem[];
       T                  *stage = reinterpret_cast<T *>(smem + S::O_STAGE);
       T                  *pring = reinterpret_cast<T *>(smem + S::O_PRING);
-      PV                 *zd    = reinterpret_cast<PV *>(smem + S::O_ZD);
+      T                  *zs    = reinterpret_cast<T *>(smem + S::O_ZS);
+      T                  *ds    = reinterpret_cast<T *>(smem + S::O_DS);
       T                  *yx    = reinterpret_cast<T *>(smem + S::O_YX);
       T                  *hx    = reinterpret_cast<T *>(smem + S::O_HX);
       double             *red   = reinterpret_cast<double *>(smem + S::O_RED);
@@ -190,24 +196,18 @@ namespace mpdg
       const T   beta  = FIRST ? T(0) : (T)a.st->beta;
       const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
       const int tile = blockIdx.x;
-      const int txi = tile % a.tiles_x, tyi = (tile / a.tiles_x) % a.tiles_y, tzi = tile / (a.tiles_x * a.tiles_y);
-      const int cx0 = TX * txi, cy0 = TY * tyi, cz0 = a.TZ * tzi;
-      const int cz1 = min(cz0 + a.TZ, a.m[2]);
       const int n0 = a.n[0], n1 = a.n[1], n2 = a.n[2];
-      const int lz_begin = cz0 > 0 ? cz0 - 1 : 0;
-      const int XB = 2 * cx0 - XOFF, Y0 = 2 * cy0 - 2;
       const long long plane_stride = (long long)a.P0 * n1;
 
       // thread's cell: main rows (warp < TY), halo row (warp == TY), halo column (warp == TY + 1)
       const int  role = warp < TY ? 0 : (warp == TY ? 1 : 2);
       const int  cxl = role == 2 ? -1 : lane, cyl = role == 0 ? warp : (role == 1 ? -1 : lane - 1);
       const bool active = role != 2 || lane <= TY;
-      const int  cx = cx0 + cxl, cy = cy0 + cyl;
-      const bool vxy = active && cx >= 0 && cx < a.m[0] && cy >= 0 && cy < a.m[1];
       const int  sxi = XOFF + 2 * cxl, syi = 2 + 2 * cyl; // staged index of the cell's first point
-      const bool last_x = cx == a.m[0] - 1, last_y = cy == a.m[1] - 1;
 
-      double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0}; // S0, S6, S1, S2, S3
+      // the thread's sums S0, S6, S1, S2, S3 in the working precision (a few hundred terms per thread
+      // in FP32); the CTA and grid sums are in double
+      T acc[5] = {T(0), T(0), T(0), T(0), T(0)};
 
       if (tid == 0)
         {
@@ -218,121 +218,8 @@ namespace mpdg
       __syncthreads();
 
       const unsigned box_bytes = (unsigned)(sizeof(T) * S::PLANE);
-      auto issue = [&](int slot, int L) {
-        // one thread: the plane L of every staged vector into slot
-        T *base = stage + (size_t)slot * NV * (S::STAGE_B / sizeof(T));
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(&bar[slot], (FIRST ? 2u : (unsigned)NV) * box_bytes);
-        const size_t vs = S::STAGE_B / sizeof(T);
-        tma_load_3d(base + 0 * vs, &tm_r, XB, Y0, L, &bar[slot]);
-        if constexpr (!FIRST)
-          {
-            tma_load_3d(base + 1 * vs, &tm_v, XB, Y0, L, &bar[slot]);
-            tma_load_3d(base + 2 * vs, &tm_p, XB, Y0, L, &bar[slot]);
-            tma_load_3d(base + 3 * vs, &tm_x, XB, Y0, L, &bar[slot]);
-          }
-        tma_load_3d(base + 4 * vs, &tm_d, XB, Y0, L, &bar[slot]);
-      };
-      unsigned phase[2] = {0u, 0u};
-      bool     failed   = false;
-
-      const int  Pfirst = 2 * lz_begin, Plast = 2 * cz1; // planes of the segment (with its halo)
-      if (tid == 0)
-        {
-          issue(0, Pfirst);
-          if (Pfirst + 1 <= Plast)
-            issue(1, Pfirst + 1);
-        }
-
-      auto owned_z = [&](int L) { return L >= 2 * cz0 && L < n2 && (L < 2 * cz1 || L == n2 - 1); };
-      auto constrained_xy = [&](int I, int J) {
-        const unsigned f = a.faces;
-        return ((f & 1u) && I == 0) || ((f & 2u) && I == n0 - 1) || ((f & 4u) && J == 0) ||
-               ((f & 8u) && J == n1 - 1);
-      };
-
-      // ---- U stage of plane L: vector updates on every staged point the cells read; owned points
-      // are written back and summed
-      auto update_plane = [&](int L) {
-        const int slot = (L - Pfirst) & 1;
-        if (!mbar_wait(&bar[slot], phase[slot], a.spin_limit))
-          failed = true;
-        phase[slot] ^= 1u;
-        const T *sb   = stage + (size_t)slot * NV * (S::STAGE_B / sizeof(T));
-        const size_t vs = S::STAGE_B / sizeof(T);
-        const T *sr = sb, *sv = sb + vs, *sp = sb + 2 * vs, *sxv = sb + 3 * vs, *sd = sb + 4 * vs;
-        T       *pr = pring + (size_t)(L % 3) * (S::STAGE_B / sizeof(T));
-        PV      *zr = zd + (size_t)(L % 3) * S::OPL;
-        const bool Lin = L >= 0 && L < n2, Lown = owned_z(L);
-        const bool Lcon = ((a.faces & 16u) && L == 0) || ((a.faces & 32u) && L == n2 - 1);
-        for (int q = tid; q < S::NPAIR; q += S::NT)
-          {
-            const int row = q / (SX / 2 - 2), pp = q - row * (SX / 2 - 2);
-            const int xi  = 2 + 2 * pp;           // staged x index (even)
-            const int I   = XB + xi, J = Y0 + row; // lattice coordinates of the pair's first point
-            const int si  = row * SX + xi;
-            const PV  r2  = *reinterpret_cast<const PV *>(sr + si);
-            const PV  d2  = *reinterpret_cast<const PV *>(sd + si);
-            PV        v2{}, p2{}, x2{};
-            if constexpr (!FIRST)
-              {
-                v2 = *reinterpret_cast<const PV *>(sv + si);
-                p2 = *reinterpret_cast<const PV *>(sp + si);
-                x2 = *reinterpret_cast<const PV *>(sxv + si);
-              }
-            const bool Jin = J >= 0 && J < n1;
-            const bool Jown = J >= 2 * cy0 && J < n1 && (J < 2 * cy0 + 2 * TY || J == n1 - 1);
-            T          pn[2], rn[2], zn[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-              {
-                const int  Ih  = I + h;
-                const T    rv  = h ? r2.y : r2.x, dv = h ? d2.y : d2.x;
-                const T    vv  = h ? v2.y : v2.x, pv = h ? p2.y : p2.x;
-                const bool in  = Lin && Jin && Ih >= 0 && Ih < n0;
-                const bool con = Lcon || constrained_xy(Ih, J);
-                const T    r   = FIRST ? rv : rv - alpha * vv;
-                const T    z   = dv * r;
-                rn[h]          = r;
-                zn[h]          = (in && !con) ? z : T(0);
-                pn[h]          = (in && !con) ? (FIRST ? z : z + beta * pv) : T(0);
-              }
-            *reinterpret_cast<PV *>(pr + si) = PV{pn[0], pn[1]};
-            if (Lown && Jown)
-              {
-                const long long g = (long long)L * plane_stride + (long long)J * a.P0 + I;
-#pragma unroll
-                for (int h = 0; h < 2; ++h)
-                  {
-                    const int Ih = I + h;
-                    if (!(Ih >= 2 * cx0 && Ih < n0 && (Ih < 2 * cx0 + 2 * TX || Ih == n0 - 1)))
-                      continue;
-                    const T pv = h ? p2.y : p2.x, xv = h ? x2.y : x2.x, dv = h ? d2.y : d2.x;
-                    if constexpr (!FIRST)
-                      {
-                        a.x[g + h]     = xv + alpha * pv;
-                        a.r_out[g + h] = rn[h];
-                      }
-                    a.p_out[g + h] = pn[h];
-                    zr[(J - 2 * cy0) * OXW + (Ih - 2 * cx0)] = PV{zn[h], dv};
-                    const double rd = (double)rn[h];
-                    acc[0] += rd * (double)zn[h];
-                    acc[1] += rd * rd;
-                  }
-              }
-          }
-      };
-
-      auto refill = [&](int L_done) {
-        // the slot of plane L_done is free once every thread passed the barrier before this call
-        const int Ln = L_done + 2;
-        if (tid == 0 && Ln <= Plast)
-          issue((L_done - Pfirst) & 1, Ln);
-      };
-
-      update_plane(Pfirst);
-      __syncthreads();
-      refill(Pfirst);
+      unsigned       phase[2]  = {0u, 0u}; // mbarrier parities, carried across the pieces
+      bool           failed    = false;
 
       // fast-diagonalisation tables (k = 2: even block 2 x 2, odd block 1 x 1)
       T we[NE * NE], wo[NO * NO], lam[N];
@@ -344,159 +231,351 @@ namespace mpdg
       for (int i = 0; i < N; ++i)
         lam[i] = a.lam[i];
 
-      T carry[N * N];
-#pragma unroll
-      for (int q = 0; q < N * N; ++q)
-        carry[q] = T(0);
-
-      for (int lz = lz_begin; lz < cz1; ++lz)
+      // this CTA's equal share of the (column, cell layer) sequence, as pieces of single columns
+      const long long g_end = a.layers * (tile + 1) / gridDim.x;
+      for (long long gcur = a.layers * tile / gridDim.x; gcur < g_end;)
         {
-          const bool halo_layer = lz < cz0;
-          T          kc         = T(0);
-          if (vxy)
-            kc = a.kcell ? a.kcell[(long long)cx + (long long)a.m[0] * ((long long)cy + (long long)a.m[1] * lz)]
-                         : a.kconst;
-          update_plane(2 * lz + 1);
-          __syncthreads();
-          refill(2 * lz + 1);
-          update_plane(2 * lz + 2);
-          __syncthreads();
-          refill(2 * lz + 2);
+          const long long col = gcur / a.m[2];
+          const int       cz0 = (int)(gcur - col * a.m[2]);
+          const int       cz1 = (int)min((long long)a.m[2], (long long)cz0 + (g_end - gcur));
+          gcur += cz1 - cz0;
+          const int  txi = (int)(col % a.tiles_x), tyi = (int)(col / a.tiles_x);
+          const int  cx0 = TX * txi, cy0 = TY * tyi;
+          const int  lz_begin = cz0 > 0 ? cz0 - 1 : 0;
+          const int  XB = 2 * cx0 - XOFF, Y0 = 2 * cy0 - 2;
+          const int  cx = cx0 + cxl, cy = cy0 + cyl;
+          const bool vxy    = active && cx >= 0 && cx < a.m[0] && cy >= 0 && cy < a.m[1];
+          const bool last_x = cx == a.m[0] - 1, last_y = cy == a.m[1] - 1;
 
-          // ---- cell stage: u = A_c p_c for the thread's cell
-          T u[N * N * N];
-#pragma unroll
-          for (int l = 0; l < N; ++l)
-            {
-              const T *pl = pring + (size_t)((2 * lz + l) % 3) * (S::STAGE_B / sizeof(T));
-#pragma unroll
-              for (int j = 0; j < N; ++j)
-#pragma unroll
-                for (int i = 0; i < N; ++i)
-                  u[(l * N + j) * N + i] = vxy ? pl[(syi + j) * SX + sxi + i] : T(0);
-            }
-          {
-            const T kcx = kc * a.cx, kcy = kc * a.cy, kcz = kc * a.cz, am = a.alpha_m;
-            xy_planes<T, N, N, true>(u, we, wo);
-#pragma unroll
-            for (int q = 0; q < N * N; ++q)
-              fwd_line<T, N, N * N>(u, q, we, wo);
-            T form = T(0);
-#pragma unroll
-            for (int c = 0; c < N; ++c)
+          auto issue = [&](int slot, int L) {
+            // one thread: the plane L of every staged vector into slot
+            T *base = stage + (size_t)slot * NV * (S::STAGE_B / sizeof(T));
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(&bar[slot], (FIRST ? 2u : (unsigned)NV) * box_bytes);
+            const size_t vs = S::STAGE_B / sizeof(T);
+            tma_load_3d(base + 0 * vs, &tm_r, XB, Y0, L, &bar[slot]);
+            if constexpr (!FIRST)
               {
-                const T tz = fma(kcz, lam[c], am);
+                tma_load_3d(base + 1 * vs, &tm_v, XB, Y0, L, &bar[slot]);
+                tma_load_3d(base + 2 * vs, &tm_p, XB, Y0, L, &bar[slot]);
+                tma_load_3d(base + 3 * vs, &tm_x, XB, Y0, L, &bar[slot]);
+              }
+            tma_load_3d(base + 4 * vs, &tm_d, XB, Y0, L, &bar[slot]);
+          };
+
+          const int  Pfirst = 2 * lz_begin, Plast = 2 * cz1; // planes of the segment (with its halo)
+          if (tid == 0)
+            {
+              issue(0, Pfirst);
+              if (Pfirst + 1 <= Plast)
+                issue(1, Pfirst + 1);
+            }
+
+          auto owned_z = [&](int L) { return L >= 2 * cz0 && L < n2 && (L < 2 * cz1 || L == n2 - 1); };
+          auto constrained_xy = [&](int I, int J) {
+            const unsigned f = a.faces;
+            return ((f & 1u) && I == 0) || ((f & 2u) && I == n0 - 1) || ((f & 4u) && J == 0) ||
+                   ((f & 8u) && J == n1 - 1);
+          };
+
+          // the thread's pairs of a staged plane, plane-independent parts (at most PR pairs): the
+          // in-plane global offset, and packed into one word the staged index (11 bits), the window
+          // index of z / d (11 bits) and the flags (10 bits)
+          constexpr int PR = (S::NPAIR + S::NT - 1) / S::NT;
+          constexpr unsigned F_VALID = 1u, F_JOWN = 2u, F_IN = 4u, F_CON = 16u, F_OWN = 64u, F_WIN = 256u;
+          static_assert(S::PLANE < 2048 && S::OPL < 2048, "staged and window indices must fit 11 bits");
+          int      pr_g[PR];
+          unsigned pr_w[PR];
 #pragma unroll
-                for (int b = 0; b < N; ++b)
+          for (int k = 0; k < PR; ++k)
+            {
+              const int q   = tid + k * S::NT;
+              const int row = q / (SX / 2 - 2), pp = q - row * (SX / 2 - 2);
+              const int xi  = 2 + 2 * pp;            // staged x index (even)
+              const int I   = XB + xi, J = Y0 + row; // lattice coordinates of the pair's first point
+              pr_g[k]  = J * a.P0 + I;
+              unsigned   f   = q < S::NPAIR ? F_VALID : 0u;
+              const bool Jin = J >= 0 && J < n1;
+              if (J >= 2 * cy0 && J < n1 && (J < 2 * cy0 + 2 * TY || J == n1 - 1))
+                f |= F_JOWN;
+#pragma unroll
+              for (int h = 0; h < 2; ++h)
+                {
+                  const int Ih = I + h;
+                  if (Jin && Ih >= 0 && Ih < n0)
+                    f |= F_IN << h;
+                  if (constrained_xy(Ih, J))
+                    f |= F_CON << h;
+                  if (Ih >= 2 * cx0 && Ih < n0 && (Ih < 2 * cx0 + 2 * TX || Ih == n0 - 1))
+                    f |= F_OWN << h;
+                }
+              const bool win = I - 2 * cx0 >= 0 && I - 2 * cx0 <= OXW - 2 && (f & F_JOWN);
+              if (win)
+                f |= F_WIN;
+              const unsigned zi = win ? (unsigned)((J - 2 * cy0) * OXW + (I - 2 * cx0)) : 0u;
+              pr_w[k]           = (f & F_VALID) ? (unsigned)(row * SX + xi) | (zi << 11) | (f << 22) : 0u;
+            }
+
+          // ---- U stage of plane L: vector updates on every staged point the cells read; owned points
+          // are written back and summed
+          auto update_plane = [&](int L) {
+            const int slot = (L - Pfirst) & 1;
+            if (!mbar_wait(&bar[slot], phase[slot], a.spin_limit))
+              failed = true;
+            phase[slot] ^= 1u;
+            const T *sb   = stage + (size_t)slot * NV * (S::STAGE_B / sizeof(T));
+            const size_t vs = S::STAGE_B / sizeof(T);
+            const T *sr = sb, *sv = sb + vs, *sp = sb + 2 * vs, *sxv = sb + 3 * vs, *sd = sb + 4 * vs;
+            T       *pr = pring + (size_t)(L % 3) * (S::STAGE_B / sizeof(T));
+            T       *zr = zs + (size_t)(L % 3) * S::OPL, *dr = ds + (size_t)(L % 3) * S::OPL;
+            const bool Lin = L >= 0 && L < n2, Lown = owned_z(L);
+            const bool Lcon = ((a.faces & 16u) && L == 0) || ((a.faces & 32u) && L == n2 - 1);
+            const long long gL = (long long)L * plane_stride;
+#pragma unroll
+            for (int k = 0; k < PR; ++k)
+              {
+                const unsigned w = pr_w[k], f = w >> 22;
+                if (!(f & F_VALID))
+                  continue;
+                const int si = (int)(w & 2047u), zi = (int)((w >> 11) & 2047u);
+                const PV  r2 = *reinterpret_cast<const PV *>(sr + si);
+                const PV  d2 = *reinterpret_cast<const PV *>(sd + si);
+                PV        v2{}, p2{}, x2{};
+                if constexpr (!FIRST)
                   {
-                    const T tyz = fma(kcy, lam[b], tz);
+                    v2 = *reinterpret_cast<const PV *>(sv + si);
+                    p2 = *reinterpret_cast<const PV *>(sp + si);
+                    x2 = *reinterpret_cast<const PV *>(sxv + si);
+                  }
+                T pn[2], rn[2], zn[2];
 #pragma unroll
-                    for (int aa = 0; aa < N; ++aa)
+                for (int h = 0; h < 2; ++h)
+                  {
+                    const T    rv   = h ? r2.y : r2.x, dv = h ? d2.y : d2.x;
+                    const T    vv   = h ? v2.y : v2.x, pv = h ? p2.y : p2.x;
+                    const bool free = Lin && (f & (F_IN << h)) && !Lcon && !(f & (F_CON << h));
+                    const T    r    = FIRST ? rv : rv - alpha * vv;
+                    const T    z    = dv * r;
+                    rn[h]           = r;
+                    zn[h]           = free ? z : T(0);
+                    pn[h]           = free ? (FIRST ? z : z + beta * pv) : T(0);
+                  }
+                *reinterpret_cast<PV *>(pr + si) = PV{pn[0], pn[1]};
+                if (Lown && (f & F_JOWN))
+                  {
+                    // I and P0 are even: the pair is one aligned vector in global and shared memory
+                    const long long g = gL + pr_g[k];
+                    const PV        xn{x2.x + alpha * p2.x, x2.y + alpha * p2.y};
+                    if ((f & (F_OWN | (F_OWN << 1))) == (F_OWN | (F_OWN << 1)))
                       {
-                        const T d = fma(kcx, lam[aa], tyz);
-                        T      &v = u[(c * N + b) * N + aa];
-                        form      = fma(d * v, v, form);
-                        v *= d;
+                        if constexpr (!FIRST)
+                          {
+                            *reinterpret_cast<PV *>(a.x + g)     = xn;
+                            *reinterpret_cast<PV *>(a.r_out + g) = PV{rn[0], rn[1]};
+                          }
+                        *reinterpret_cast<PV *>(a.p_out + g) = PV{pn[0], pn[1]};
                       }
+                    else
+#pragma unroll
+                      for (int h = 0; h < 2; ++h)
+                        if (f & (F_OWN << h))
+                          {
+                            if constexpr (!FIRST)
+                              {
+                                a.x[g + h]     = h ? xn.y : xn.x;
+                                a.r_out[g + h] = rn[h];
+                              }
+                            a.p_out[g + h] = pn[h];
+                          }
+                    // z and d of the owned window (points outside it are never read)
+                    if (f & F_WIN)
+                      {
+                        *reinterpret_cast<PV *>(zr + zi) = PV{zn[0], zn[1]};
+                        *reinterpret_cast<PV *>(dr + zi) = d2;
+                      }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                      if (f & (F_OWN << h))
+                        {
+                          acc[0] = fma(rn[h], zn[h], acc[0]);
+                          acc[1] = fma(rn[h], rn[h], acc[1]);
+                        }
                   }
               }
-            if (role == 0 && !halo_layer && vxy)
-              acc[2] += (double)form;
-#pragma unroll
-            for (int q = 0; q < N * N; ++q)
-              bwd_line<T, N, N * N>(u, q, we, wo);
-            xy_planes<T, N, N, false>(u, we, wo);
-          }
-          // ---- x faces: the halo column hands its x = 2 face to lane 0 of every other row
-          if (role == 2 && active)
-#pragma unroll
-            for (int q = 0; q < N * N; ++q)
-              hx[lane * 9 + q] = u[q * N + K];
+          };
+
+          auto refill = [&](int L_done) {
+            // the slot of plane L_done is free once every thread passed the barrier before this call
+            const int Ln = L_done + 2;
+            if (tid == 0 && Ln <= Plast)
+              issue((L_done - Pfirst) & 1, Ln);
+          };
+
+          update_plane(Pfirst);
           __syncthreads();
-          if (role != 2)
-            {
-              const int hrow = role == 0 ? warp + 1 : 0; // halo column lane of this row
+          refill(Pfirst);
+
+          T carry[N * N];
 #pragma unroll
-              for (int q = 0; q < N * N; ++q)
-                {
-                  const T v = __shfl_up_sync(0xffffffffu, u[q * N + K], 1);
-                  u[q * N] += lane > 0 ? v : hx[hrow * 9 + q];
-                }
-              // y faces: main rows and the halo row hand their y = 2 face to the next row
-              const int slot = role == 0 ? warp : TY;
+          for (int q = 0; q < N * N; ++q)
+            carry[q] = T(0);
+
+          for (int lz = lz_begin; lz < cz1; ++lz)
+            {
+              const bool halo_layer = lz < cz0;
+              T          kc         = T(0);
+              if (vxy)
+                kc = a.kcell ? a.kcell[(long long)cx + (long long)a.m[0] * ((long long)cy + (long long)a.m[1] * lz)]
+                             : a.kconst;
+              update_plane(2 * lz + 1);
+              __syncthreads();
+              refill(2 * lz + 1);
+              update_plane(2 * lz + 2);
+              __syncthreads();
+              refill(2 * lz + 2);
+
+              // ---- cell stage: u = A_c p_c for the thread's cell
+              T u[N * N * N];
 #pragma unroll
               for (int l = 0; l < N; ++l)
-#pragma unroll
-                for (int i = 0; i < N; ++i)
-                  yx[((slot * N + l) * N + i) * 32 + lane] = u[(l * N + K) * N + i];
-            }
-          __syncthreads();
-          if (role == 0)
-            {
-              const int from = warp == 0 ? TY : warp - 1;
-#pragma unroll
-              for (int l = 0; l < N; ++l)
-#pragma unroll
-                for (int i = 0; i < N; ++i)
-                  u[(l * N) * N + i] += yx[((from * N + l) * N + i) * 32 + lane];
-              // z faces: add the carried face, carry this layer's z = 2 face
-#pragma unroll
-              for (int q = 0; q < N * N; ++q)
                 {
-                  u[q] += carry[q];
-                  carry[q] = u[K * N * N + q];
-                }
-              // ---- owned points of the finished planes: v_k, S2, S3
-              if (!halo_layer && vxy)
-                {
-                  const int nl = lz == a.m[2] - 1 ? 3 : 2;
-                  for (int l = 0; l < nl; ++l)
+                  const T *pl = pring + (size_t)((2 * lz + l) % 3) * (S::STAGE_B / sizeof(T));
+#pragma unroll
+                  for (int j = 0; j < N; ++j)
                     {
-                      const int  L    = 2 * lz + l;
-                      const PV  *zl   = zd + (size_t)(L % 3) * S::OPL;
-                      const bool Lcon = ((a.faces & 16u) && L == 0) || ((a.faces & 32u) && L == n2 - 1);
+                      // sxi and SX are even: points 0, 1 of the row are one aligned pair
+                      const T *row = pl + (syi + j) * SX + sxi;
+                      const PV p01 = vxy ? *reinterpret_cast<const PV *>(row) : PV{T(0), T(0)};
+                      u[(l * N + j) * N + 0] = p01.x;
+                      u[(l * N + j) * N + 1] = p01.y;
+                      u[(l * N + j) * N + 2] = vxy ? row[2] : T(0);
+                    }
+                }
+              {
+                const T kcx = kc * a.cx, kcy = kc * a.cy, kcz = kc * a.cz, am = a.alpha_m;
+                xy_planes<T, N, N, true>(u, we, wo);
 #pragma unroll
-                      for (int j = 0; j < N; ++j)
+                for (int q = 0; q < N * N; ++q)
+                  fwd_line<T, N, N * N>(u, q, we, wo);
+                T form = T(0);
+#pragma unroll
+                for (int c = 0; c < N; ++c)
+                  {
+                    const T tz = fma(kcz, lam[c], am);
+#pragma unroll
+                    for (int b = 0; b < N; ++b)
+                      {
+                        const T tyz = fma(kcy, lam[b], tz);
+#pragma unroll
+                        for (int aa = 0; aa < N; ++aa)
+                          {
+                            const T d = fma(kcx, lam[aa], tyz);
+                            T      &v = u[(c * N + b) * N + aa];
+                            form      = fma(d * v, v, form);
+                            v *= d;
+                          }
+                      }
+                  }
+                if (role == 0 && !halo_layer && vxy)
+                  acc[2] += form;
+#pragma unroll
+                for (int q = 0; q < N * N; ++q)
+                  bwd_line<T, N, N * N>(u, q, we, wo);
+                xy_planes<T, N, N, false>(u, we, wo);
+              }
+              // ---- x faces: the halo column hands its x = 2 face to lane 0 of every other row
+              if (role == 2 && active)
+#pragma unroll
+                for (int q = 0; q < N * N; ++q)
+                  hx[lane * 9 + q] = u[q * N + K];
+              __syncthreads();
+              if (role != 2)
+                {
+                  const int hrow = role == 0 ? warp + 1 : 0; // halo column lane of this row
+#pragma unroll
+                  for (int q = 0; q < N * N; ++q)
+                    {
+                      const T v = __shfl_up_sync(0xffffffffu, u[q * N + K], 1);
+                      u[q * N] += lane > 0 ? v : hx[hrow * 9 + q];
+                    }
+                  // y faces: main rows and the halo row hand their y = 2 face to the next row
+                  const int slot = role == 0 ? warp : TY;
+#pragma unroll
+                  for (int l = 0; l < N; ++l)
+#pragma unroll
+                    for (int i = 0; i < N; ++i)
+                      yx[((slot * N + l) * N + i) * 32 + lane] = u[(l * N + K) * N + i];
+                }
+              __syncthreads();
+              if (role == 0)
+                {
+                  const int from = warp == 0 ? TY : warp - 1;
+#pragma unroll
+                  for (int l = 0; l < N; ++l)
+#pragma unroll
+                    for (int i = 0; i < N; ++i)
+                      u[(l * N) * N + i] += yx[((from * N + l) * N + i) * 32 + lane];
+                  // z faces: add the carried face, carry this layer's z = 2 face
+#pragma unroll
+                  for (int q = 0; q < N * N; ++q)
+                    {
+                      u[q] += carry[q];
+                      carry[q] = u[K * N * N + q];
+                    }
+                  // ---- owned points of the finished planes: v_k, S2, S3
+                  if (!halo_layer && vxy)
+                    {
+                      const int nl = lz == a.m[2] - 1 ? 3 : 2;
+                      for (int l = 0; l < nl; ++l)
                         {
-                          if (j == K && !last_y)
-                            continue;
-                          const int J = 2 * cy + j;
-                          T        *vrow = a.v_out + (long long)L * plane_stride + (long long)J * a.P0;
-                          const PV *zrow = zl + (J - 2 * cy0) * OXW;
-                          const bool Jcon = Lcon || ((a.faces & 4u) && J == 0) || ((a.faces & 8u) && J == n1 - 1);
-                          T          vv[N];
-                          double     s2 = 0.0, s3 = 0.0;
+                          const int  L    = 2 * lz + l;
+                          const T   *zl   = zs + (size_t)(L % 3) * S::OPL, *dl = ds + (size_t)(L % 3) * S::OPL;
+                          const bool Lcon = ((a.faces & 16u) && L == 0) || ((a.faces & 32u) && L == n2 - 1);
 #pragma unroll
-                          for (int i = 0; i < N; ++i)
+                          for (int j = 0; j < N; ++j)
                             {
-                              const int  I   = 2 * cx + i;
-                              const bool con = Jcon || ((a.faces & 1u) && I == 0) || ((a.faces & 2u) && I == n0 - 1);
-                              vv[i]          = con ? T(0) : u[(l * N + j) * N + i];
-                              if (i < K || last_x)
+                              if (j == K && !last_y)
+                                continue;
+                              const int J = 2 * cy + j;
+                              T        *vrow = a.v_out + (long long)L * plane_stride + (long long)J * a.P0;
+                              const int o0 = (J - 2 * cy0) * OXW + 2 * (cx - cx0); // even: aligned pairs
+                              const PV  z01 = *reinterpret_cast<const PV *>(zl + o0);
+                              const PV  d01 = *reinterpret_cast<const PV *>(dl + o0);
+                              const T   zz[N] = {z01.x, z01.y, last_x ? zl[o0 + 2] : T(0)};
+                              const T   dd[N] = {d01.x, d01.y, last_x ? dl[o0 + 2] : T(0)};
+                              const bool Jcon = Lcon || ((a.faces & 4u) && J == 0) || ((a.faces & 8u) && J == n1 - 1);
+                              T          vv[N];
+                              T          s2 = T(0), s3 = T(0);
+#pragma unroll
+                              for (int i = 0; i < N; ++i)
                                 {
-                                  const PV   zz = zrow[I - 2 * cx0];
-                                  const double v = (double)vv[i];
-                                  s2 += (double)zz.x * v;
-                                  s3 += (double)zz.y * v * v;
+                                  const int  I   = 2 * cx + i;
+                                  const bool con = Jcon || ((a.faces & 1u) && I == 0) || ((a.faces & 2u) && I == n0 - 1);
+                                  vv[i]          = con ? T(0) : u[(l * N + j) * N + i];
+                                  if (i < K || last_x)
+                                    {
+                                      s2 = fma(zz[i], vv[i], s2);
+                                      s3 = fma(dd[i] * vv[i], vv[i], s3);
+                                    }
                                 }
+                              acc[3] += s2;
+                              acc[4] += s3;
+                              *reinterpret_cast<PV *>(vrow + 2 * cx) = PV{vv[0], vv[1]};
+                              if (last_x)
+                                vrow[2 * cx + 2] = vv[2];
                             }
-                          acc[3] += s2;
-                          acc[4] += s3;
-                          *reinterpret_cast<PV *>(vrow + 2 * cx) = PV{vv[0], vv[1]};
-                          if (last_x)
-                            vrow[2 * cx + 2] = vv[2];
                         }
                     }
                 }
+              __syncthreads();
             }
-          __syncthreads();
         }
 
       // ---- CTA sums in a fixed order, then the last CTA adds the tiles in order and steps the state
 #pragma unroll
       for (int k = 0; k < 5; ++k)
         {
-          double v = acc[k];
+          double v = (double)acc[k];
 #pragma unroll
           for (int off = 16; off > 0; off >>= 1)
             v += __shfl_down_sync(0xffffffffu, v, off);
@@ -634,23 +713,10 @@ namespace mpdg
     tiles_y      = (m[1] + TY - 1) / TY;
     // CTAs resident per SM from the shared memory footprint (227 KB usable per CTA, 228 KB per SM)
     const int per_sm = std::max(1, (int)(233472 / (smem_bytes() + 1024)));
-    const long long slots = (long long)sm_count * per_sm;
-    // segment length: the fewest waves of equal tiles, weighted by the halo layer each tile adds
-    double best = 1e300;
-    for (int tz = 2; tz <= 64; ++tz)
-      {
-        const long long segs  = (m[2] + tz - 1) / tz;
-        const long long tiles = (long long)tiles_x * tiles_y * segs;
-        const double    waves = std::ceil((double)tiles / (double)slots);
-        const double    cost  = waves * (std::min(tz, m[2]) + 1.5);
-        if (cost < best - 1e-9)
-          {
-            best = cost;
-            TZ   = tz;
-          }
-      }
-    segs   = (m[2] + TZ - 1) / TZ;
-    ntiles = tiles_x * tiles_y * segs;
+    // one CTA per resident slot, each with an equal share of the columns' layers; a share below
+    // four layers would spend more on its halo layer than it saves, so small lattices use fewer CTAs
+    layers = (long long)tiles_x * tiles_y * m[2];
+    ntiles = (int)std::max(1LL, std::min((long long)sm_count * per_sm, layers / 4));
   }
 
   template <typename T>
@@ -671,7 +737,7 @@ namespace mpdg
     a.faces   = faces;
     a.tiles_x = tiles_x;
     a.tiles_y = tiles_y;
-    a.TZ      = TZ;
+    a.layers  = layers;
     a.ty      = TY;
     a.alpha_m = (T)mass_coef;
     a.cx      = (T)geo[0];

@@ -30,7 +30,8 @@ namespace mpdg
     unsigned faces = 0;
     double   mass_coef = 0.0, geo[3]{}, kconst = 1.0;
     const T *kcell = nullptr;
-    int      tiles_x = 0, tiles_y = 0, TZ = 0, segs = 0, ntiles = 0;
+    int       tiles_x = 0, tiles_y = 0, ntiles = 0; // ntiles: CTAs of the sweep (one partial sum each)
+    long long layers  = 0;                          // columns x cell layers
 
     static int padded_pitch(int n0) { return (n0 + 8) / 8 * 8; }
     long long  padded_len() const { return (long long)P0 * n[1] * n[2]; }

@@ -431,6 +431,23 @@ namespace mpdg
       const long long cell = (long long)cx + (long long)a.g.m[0] * ((long long)cy + (long long)a.g.m[1] * cz);
       return a.kscale * (a.kcell ? a.kcell[cell] : a.kconst);
     }
+    // unscaled per-cell conductivity (nullptr: the constant kconst()) and the scale applied to it
+    __device__ __forceinline__ const T *
+    kcell_ptr(int cx, int cy, int cz) const
+    {
+      const long long cell = (long long)cx + (long long)a.g.m[0] * ((long long)cy + (long long)a.g.m[1] * cz);
+      return a.kcell ? a.kcell + cell : nullptr;
+    }
+    __device__ __forceinline__ T
+    kconst() const
+    {
+      return a.kconst;
+    }
+    __device__ __forceinline__ T
+    kscale() const
+    {
+      return a.kscale;
+    }
   };
 
   template <int K, typename T, OutMode MODE, bool DOT>

@@ -11,7 +11,11 @@
 //      place, the two face points of the cell into separate face buffers;
 //   3. each thread reads its x point back (face points add the results of both adjacent cells,
 //      so x faces inside the brick are combined without atomics), applies the backward y and z
-//      transforms and holds the (k+1)^2 output values of its pencil;
+//      transforms and holds the (k+1)^2 output values of its pencil; with MPDG_PENCIL_PREFETCH the
+//      thread then starts the asynchronous copy (cp.async) of its pencil of the next row step into
+//      its (now free) transposition-buffer column, with the next row's conductivities, so that the
+//      loads of step 1 are in flight during this step's backward transforms and stores (on for
+//      k = 3 and for FP32; at k = 4 in FP64 the plain loads measured faster);
 //   4. y faces between the rows of the brick are carried in registers to the next row step, z faces
 //      between layers in shared memory to the next layer (per thread, no synchronisation); points
 //      owned by the pencil are written with coalesced plain stores; points on the brick's faces
@@ -39,6 +43,9 @@
 #endif
 #ifndef MPDG_PENCIL_XPAIR
 #define MPDG_PENCIL_XPAIR 0
+#endif
+#ifndef MPDG_PENCIL_PREFETCH
+#define MPDG_PENCIL_PREFETCH -1 // -1: by degree and precision (measured); 0 off; 1 on
 #endif
 
 namespace mpdg
@@ -87,26 +94,49 @@ namespace mpdg
     T *kcs = xs + LAY::XS, *mus = kcs + LAY::KC;
     const int p = threadIdx.x, lane = p & 31, warp = p >> 5;
     BR        br;
+    constexpr bool PF = MPDG_PENCIL_PREFETCH < 0 ? (K == 3 || sizeof(T) == 4) : MPDG_PENCIL_PREFETCH != 0;
     if (!brick_begin<BR, T, MODE>(br, g, s, dst, bvec, s_ticket))
       return;
-    if constexpr (MODE != OutMode::Add)
-      if (br.has_lower_neighbour())
-        brick_wait_lower(br, g, s);
-    const T *we = op.we(), *wo = op.wo(), *lam = op.lam();
-    if (p < M)
-      mus[p] = op.cyg() * lam[p % N] + op.czg() * lam[p / N];
-    const T   alpha = op.alpha(), cxg = op.cxg();
     const int ncx = min(BX, g.m[0] - br.c0[0]), ncy = min(SH::BY, g.m[1] - br.c0[1]),
               ncz = min(SH::BZ, g.m[2] - br.c0[2]);
     const int  plast = K * ncx;               // brick's high x face (x point)
     const bool xin   = p <= plast;
+    const int  sy = br.sy, sz = br.sz;
+    const int  xbase = br.g0[0] + (xin ? p : plast); // clamped: every load stays inside the lattice
+    // asynchronous copy of row step (rr, ll): the thread's pencil into its own column of tb, the
+    // row's (unscaled) conductivities into kcs
+    auto prefetch = [&](int rr, int ll) {
+      const T *s0 = src + (xbase + (br.g0[1] + K * rr) * sy + (br.g0[2] + K * ll) * sz);
+#pragma unroll
+      for (int l = 0; l < N; ++l)
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+          cp_async_elem(tb + (l * N + j) * TP + p, s0 + (j * sy + l * sz), true);
+      if (p < ncx)
+        {
+          const T *kp = op.kcell_ptr(br.c0[0] + p, br.c0[1] + rr, br.c0[2] + ll);
+          if (kp != nullptr)
+            cp_async_elem(kcs + p, kp, true);
+          else
+            kcs[p] = op.kconst();
+        }
+    };
+    if constexpr (PF)
+      prefetch(0, 0);
+    if constexpr (MODE != OutMode::Add)
+      if (br.has_lower_neighbour())
+        brick_wait_lower(br, g, s);
+    const T *we = op.we(), *wo = op.wo(), *lam = op.lam();
+    // with the prefetch kcs holds unscaled conductivities: the scale goes into the geometry factors
+    const T kmul = PF ? op.kscale() : T(1);
+    if (p < M)
+      mus[p] = kmul * (op.cyg() * lam[p % N] + op.czg() * lam[p / N]);
+    const T   alpha = op.alpha(), cxg = kmul * op.cxg();
     const bool extra = ncx == BX;             // x point K*BX exists and is done cooperatively
     const bool xface = p == 0 || p == plast;
     const bool xcon  = (br.con_lo[0] && p == 0) || (br.con_hi[0] && p == plast);
     const bool zero_pencil = !xin || (mask_src && xcon);
     const int  qx = p % K, cxp = p / K;       // x point = K cxp + qx
-    const int  sy = br.sy, sz = br.sz;
-    const int  xbase = br.g0[0] + (xin ? p : plast); // clamped: every load stays inside the lattice
     // the cooperative pencil runs on warp 1, the extra round of x lines on the last warp and the x = 0
     // face atomics on warp 0, so that no warp carries two of these
     const bool exl   = extra && warp == 1 && lane < N; // lanes of the cooperative pencil
@@ -134,16 +164,24 @@ namespace mpdg
             const int  cy = br.c0[1] + r, cz = br.c0[2] + lz;
             // ---- 1. load and transform the pencil (z lines, then y lines)
             T u[M];
-            {
-              const T *s0 = src + (xbase + base);
+            if constexpr (PF)
+              {
+                cp_async_wait_all(); // this thread's copies; the barrier below publishes kcs
 #pragma unroll
-              for (int l = 0; l < N; ++l)
+                for (int m = 0; m < M; ++m)
+                  u[m] = tb[m * TP + p];
+              }
+            else
+              {
+                const T *s0 = src + (xbase + base);
 #pragma unroll
-                for (int j = 0; j < N; ++j)
-                  u[l * N + j] = s0[j * sy + l * sz];
-            }
-            if (p < ncx)
-              kcs[p] = op.kcell(br.c0[0] + p, cy, cz);
+                for (int l = 0; l < N; ++l)
+#pragma unroll
+                  for (int j = 0; j < N; ++j)
+                    u[l * N + j] = s0[j * sy + l * sz];
+                if (p < ncx)
+                  kcs[p] = op.kcell(br.c0[0] + p, cy, cz);
+              }
             if (zero_pencil)
 #pragma unroll
               for (int q = 0; q < M; ++q)
@@ -387,6 +425,13 @@ namespace mpdg
                 for (int m = 0; m < M; ++m)
                   u[m] = (h0 ? f0[m] : T(0)) + (h4 ? f4[m] : T(0));
               }
+            if constexpr (PF)
+              {
+                // the next row step's loads, in flight during the rest of this one
+                const bool nl = r + 1 == ncy;
+                if (!nl || lz + 1 < ncz)
+                  prefetch(nl ? 0 : r + 1, nl ? lz + 1 : lz);
+              }
 #pragma unroll
             for (int c = 0; c < N; ++c)
               bwd_line<T, N, 1>(u, c * N, we, wo);
@@ -530,7 +575,8 @@ namespace mpdg
               }
             // no barrier here: the next row's first barrier (after its pencil transforms) already
             // orders every shared buffer it reuses -- tb columns are rewritten only by their own
-            // thread before it, kcs and the face buffers only after it
+            // thread before it, the face buffers only after it, and kcs (nobody reads it between the
+            // x-line barrier of this row and the first barrier of the next) by its prefetch
           }
       }
     if constexpr (DOT)

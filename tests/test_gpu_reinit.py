@@ -187,13 +187,33 @@ def test_narrow_band_projection_and_rhs(degree, m, faces):
     g.level_set_curvature_rhs(kap, *(to_gpu(c) for c in normal), 1e-10)
     assert rel_err(kap.cpu().numpy(), curvature_rhs(om, cm, normal, 1e-10, level_set=psi, narrow_band=band)) <= 1e-12
     # projection solve: the banded operator is only semidefinite (rows outside the band are zero, and
-    # cells with few Gauss points in the band add low-rank terms), so the consistent system is solved
-    # to a moderate tolerance and checked against the oracle's operator
+    # cells with few Gauss points in the band add nearly singular terms), so CG converges slowly and
+    # amplifies rounding quickly (a 1e-15 perturbation of the right-hand side reaches 1e-3 after 20
+    # steps); a fixed number of Jacobi-CG steps (SolverCG's recurrence, restated here on the oracle's
+    # operator) must give the same iterate
+    from meltpooldg_b200._lib import NoConvergence
+
+    steps = 8
     rhs = nx.clone()
     sol = torch.zeros_like(rhs)
-    LinearSolver.solve(g, sol, rhs, LinearSolverData("CG", "Diagonal", rel_tolerance=1e-6, max_iterations=5000))
-    r = rhs.cpu().numpy() - projection_apply(om, cm, damping, sol.cpu().numpy(), level_set=psi, narrow_band=band)
-    assert np.linalg.norm(r) <= 1.01e-6 * np.linalg.norm(rhs.cpu().numpy())
+    try:  # a small system may converge within the steps: then compare after as many
+        steps = LinearSolver.solve(g, sol, rhs, LinearSolverData("CG", "Diagonal", rel_tolerance=1e-14,
+                                                                 max_iterations=steps)).iterations
+    except NoConvergence:
+        pass
+    b = rhs.cpu().numpy()
+    xo, r = np.zeros(n), b.copy()
+    z = inv * r
+    p, rz = z.copy(), float(r @ z)
+    for _ in range(steps):
+        v = projection_apply(om, cm, damping, p, level_set=psi, narrow_band=band)
+        alpha = rz / float(p @ v)
+        xo += alpha * p
+        r -= alpha * v
+        z = inv * r
+        rz, rz_old = float(r @ z), rz
+        p = z + (rz / rz_old) * p
+    assert rel_err(sol.cpu().numpy(), xo) <= 1e-8
     g.set_narrow_band(None, 0.0)
     g.vmult(y, to_gpu(x))
     assert rel_err(y.cpu().numpy(), projection_apply(om, cm, damping, x)) <= 1e-12

@@ -656,7 +656,13 @@ namespace
     T *R[2] = {op->vec<T>(t + "fR0", plen), op->vec<T>(t + "fR1", plen)};
     T *P[2] = {op->vec<T>(t + "fP0", plen), op->vec<T>(t + "fP1", plen)};
     T *V[2] = {op->vec<T>(t + "fV0", plen), op->vec<T>(t + "fV1", plen)};
-    double *part = op->vec<double>(t + "fpart", (size_t)5 * f.ntiles);
+    double    *part  = op->vec<double>(t + "fpart", (size_t)5 * f.ntiles);
+    long long *range = op->vec<long long>(t + "frange", f.range.size());
+    if (!range)
+      return fail(MPDG_ERR_NOMEM, "fused CG ranges");
+    MPDG_CUDA(cudaMemcpyAsync(range, f.range.data(), sizeof(long long) * f.range.size(), cudaMemcpyHostToDevice,
+                              op->stream));
+    f.d_range = range;
     double *hist = op->vec<double>(t + "hist", (size_t)max_it + 2);
     if (!X || !D || !R[0] || !R[1] || !P[0] || !P[1] || !V[0] || !V[1] || !part || !hist)
       return fail(MPDG_ERR_NOMEM, "fused CG work vectors");

@@ -16,9 +16,11 @@
 // forms z_0, p_0 = z_0 and v_0 only.  Per iteration the sweep reads x, r, p, v, d and writes x, r,
 // p, v: s (9 N + N_c) bytes, against s (13 N + N_c) for separate update / apply / update passes.
 //
-// Tiles.  The lattice is cut into columns of 32 x TY cells in x, y; the columns' cell layers, taken
-// column after column, are dealt out in equal contiguous ranges to a grid of one CTA per resident
-// slot, so every SM gets the same number of layers.  A CTA's range is one or a few pieces (a segment
+// Tiles.  The lattice is cut into columns of 32 x TY cells in x, y and into slabs of cell layers in
+// z; the (column, layer) pairs, taken slab by slab and column by column within a slab, are dealt out
+// in equal contiguous ranges to a grid of one CTA per resident slot, so every SM gets the same
+// number of layers and the CTAs running side by side work on neighbouring columns at nearly the same
+// layers (their halo planes are shared through L2).  A CTA's range is one or a few pieces (a segment
 // of z layers of one column); it owns the lattice points of each piece and marches through it
 // layer by layer.  It also computes the cells of one halo layer
 // on its low side in x, y and z (a halo column warp, a halo row warp, a halo cell layer), so every
@@ -86,7 +88,9 @@ namespace mpdg
       int           P0;          // padded x pitch (elements)
       unsigned      faces;       // Dirichlet faces (bit 2d low, 2d+1 high of dim d)
       int           tiles_x, tiles_y, ty;
-      long long     layers;      // columns x cell layers, dealt out in equal ranges to the CTAs
+      long long     layers;      // columns x cell layers
+      int           slab;        // layers of a slab: the sequence is slab by slab, column by column
+      const long long *range;    // CTA b takes sequence positions [range[b], range[b + 1])
       T             alpha_m, cx, cy, cz; // mass coefficient, stiffness geometry factors
       T             kconst;
       const T      *kcell;
@@ -221,23 +225,22 @@ namespace mpdg
       unsigned       phase[2]  = {0u, 0u}; // mbarrier parities, carried across the pieces
       bool           failed    = false;
 
-      // fast-diagonalisation tables (k = 2: even block 2 x 2, odd block 1 x 1)
-      T we[NE * NE], wo[NO * NO], lam[N];
-#pragma unroll
-      for (int i = 0; i < NE * NE; ++i)
-        we[i] = a.we[i];
-      wo[0] = a.wo[0];
-#pragma unroll
-      for (int i = 0; i < N; ++i)
-        lam[i] = a.lam[i];
+      // fast-diagonalisation tables (k = 2: even block 2 x 2, odd block 1 x 1), read in place from
+      // the kernel parameters (constant bank operands, no registers)
+      const T *we = a.we, *wo = a.wo, *lam = a.lam;
 
-      // this CTA's equal share of the (column, cell layer) sequence, as pieces of single columns
-      const long long g_end = a.layers * (tile + 1) / gridDim.x;
-      for (long long gcur = a.layers * tile / gridDim.x; gcur < g_end;)
+      // this CTA's range of the (column, cell layer) sequence, as pieces of single columns
+      const long long g_end = a.range[tile + 1];
+      for (long long gcur = a.range[tile]; gcur < g_end;)
         {
-          const long long col = gcur / a.m[2];
-          const int       cz0 = (int)(gcur - col * a.m[2]);
-          const int       cz1 = (int)min((long long)a.m[2], (long long)cz0 + (g_end - gcur));
+          // sequence position -> (slab, column, layer); only the last slab may be lower
+          const long long ncol = (long long)a.tiles_x * a.tiles_y;
+          const int       sl   = (int)(gcur / (ncol * a.slab));
+          const int       hs   = min(a.slab, a.m[2] - sl * a.slab); // height of this slab
+          const long long off  = gcur - (long long)sl * ncol * a.slab;
+          const long long col  = off / hs;
+          const int       cz0  = sl * a.slab + (int)(off - col * hs);
+          const int       cz1  = (int)min((long long)(sl * a.slab + hs), (long long)cz0 + (g_end - gcur));
           gcur += cz1 - cz0;
           const int  txi = (int)(col % a.tiles_x), tyi = (int)(col / a.tiles_x);
           const int  cx0 = TX * txi, cy0 = TY * tyi;
@@ -278,22 +281,20 @@ namespace mpdg
                    ((f & 8u) && J == n1 - 1);
           };
 
-          // the thread's pairs of a staged plane, plane-independent parts (at most PR pairs): the
-          // in-plane global offset, and packed into one word the staged index (11 bits), the window
-          // index of z / d (11 bits) and the flags (10 bits)
+          // the thread's pairs of a staged plane, plane-independent parts (at most PR pairs), packed
+          // into one word: the staged index (11 bits), the window index of z / d (11 bits) and the
+          // flags (10 bits)
           constexpr int PR = (S::NPAIR + S::NT - 1) / S::NT;
           constexpr unsigned F_VALID = 1u, F_JOWN = 2u, F_IN = 4u, F_CON = 16u, F_OWN = 64u, F_WIN = 256u;
           static_assert(S::PLANE < 2048 && S::OPL < 2048, "staged and window indices must fit 11 bits");
-          int      pr_g[PR];
-          unsigned pr_w[PR];
-#pragma unroll
-          for (int k = 0; k < PR; ++k)
-            {
+          // FP64 keeps the words in registers (it has spare ones at one CTA per SM); FP32, held to
+          // two CTAs per SM, recomputes them per plane
+          constexpr bool KEEP = sizeof(T) == 8;
+          auto pair_word = [&](int k) {
               const int q   = tid + k * S::NT;
               const int row = q / (SX / 2 - 2), pp = q - row * (SX / 2 - 2);
               const int xi  = 2 + 2 * pp;            // staged x index (even)
               const int I   = XB + xi, J = Y0 + row; // lattice coordinates of the pair's first point
-              pr_g[k]  = J * a.P0 + I;
               unsigned   f   = q < S::NPAIR ? F_VALID : 0u;
               const bool Jin = J >= 0 && J < n1;
               if (J >= 2 * cy0 && J < n1 && (J < 2 * cy0 + 2 * TY || J == n1 - 1))
@@ -313,8 +314,13 @@ namespace mpdg
               if (win)
                 f |= F_WIN;
               const unsigned zi = win ? (unsigned)((J - 2 * cy0) * OXW + (I - 2 * cx0)) : 0u;
-              pr_w[k]           = (f & F_VALID) ? (unsigned)(row * SX + xi) | (zi << 11) | (f << 22) : 0u;
-            }
+              return (f & F_VALID) ? (unsigned)(row * SX + xi) | (zi << 11) | (f << 22) : 0u;
+          };
+          unsigned pr_w[KEEP ? PR : 1];
+          if constexpr (KEEP)
+#pragma unroll
+            for (int k = 0; k < PR; ++k)
+              pr_w[k] = pair_word(k);
 
           // ---- U stage of plane L: vector updates on every staged point the cells read; owned points
           // are written back and summed
@@ -334,7 +340,7 @@ namespace mpdg
 #pragma unroll
             for (int k = 0; k < PR; ++k)
               {
-                const unsigned w = pr_w[k], f = w >> 22;
+                const unsigned w = KEEP ? pr_w[KEEP ? k : 0] : pair_word(k), f = w >> 22;
                 if (!(f & F_VALID))
                   continue;
                 const int si = (int)(w & 2047u), zi = (int)((w >> 11) & 2047u);
@@ -364,7 +370,8 @@ namespace mpdg
                 if (Lown && (f & F_JOWN))
                   {
                     // I and P0 are even: the pair is one aligned vector in global and shared memory
-                    const long long g = gL + pr_g[k];
+                    const int       row = si / SX, xi = si - row * SX;
+                    const long long g   = gL + (long long)(Y0 + row) * a.P0 + (XB + xi);
                     const PV        xn{x2.x + alpha * p2.x, x2.y + alpha * p2.y};
                     if ((f & (F_OWN | (F_OWN << 1))) == (F_OWN | (F_OWN << 1)))
                       {
@@ -717,6 +724,70 @@ namespace mpdg
     // four layers would spend more on its halo layer than it saves, so small lattices use fewer CTAs
     layers = (long long)tiles_x * tiles_y * m[2];
     ntiles = (int)std::max(1LL, std::min((long long)sm_count * per_sm, layers / 4));
+    // slabs about one share high, so that the CTAs working at the same time hold neighbouring
+    // columns at about the same layers and read each other's halo planes from L2
+    slab = (int)std::max(1LL, std::min((long long)m[2], (layers + ntiles / 2) / ntiles));
+    // ranges of equal cost: a piece costs its layers plus about 1.5 (its halo layer and the
+    // staging ramp), so CTAs whose range is cut into short pieces (the last, lower slab) take
+    // fewer layers; the smallest cost bound that needs at most ntiles ranges, by bisection
+    const long long ncol = (long long)tiles_x * tiles_y;
+    auto greedy = [&](double bound, std::vector<long long> *out) {
+      long long n = 0, pos = 0;
+      double    cost = 0.0;
+      bool      open = false;
+      if (out)
+        out->assign(1, 0);
+      for (int z0 = 0; z0 < m[2]; z0 += slab)
+        {
+          const int hs = std::min(slab, m[2] - z0);
+          for (long long c = 0; c < ncol; ++c)
+            {
+              long long left = hs;
+              while (left > 0)
+                {
+                  long long take = (long long)std::floor(bound - cost - 1.5);
+                  if (take <= 0)
+                    {
+                      if (!open) // a bound below one layer per piece: take one anyway
+                        take = 1;
+                      else
+                        {
+                          ++n;
+                          if (out)
+                            out->push_back(pos);
+                          cost = 0.0;
+                          open = false;
+                          continue;
+                        }
+                    }
+                  take = std::min(take, left);
+                  cost += (double)take + 1.5;
+                  open = true;
+                  pos += take;
+                  left -= take;
+                }
+            }
+        }
+      if (open)
+        {
+          ++n;
+          if (out)
+            out->push_back(pos);
+        }
+      return n;
+    };
+    double lo = (double)layers / ntiles, hi = lo + 3.0 * (1.5 + slab);
+    for (int it = 0; it < 60; ++it)
+      {
+        const double mid = 0.5 * (lo + hi);
+        if (greedy(mid, nullptr) <= ntiles)
+          hi = mid;
+        else
+          lo = mid;
+      }
+    greedy(hi, &range);
+    while ((long long)range.size() < ntiles + 1LL) // fewer ranges than CTAs: empty ranges at the end
+      range.push_back(layers);
   }
 
   template <typename T>
@@ -738,6 +809,8 @@ namespace mpdg
     a.tiles_x = tiles_x;
     a.tiles_y = tiles_y;
     a.layers  = layers;
+    a.slab    = slab;
+    a.range   = d_range;
     a.ty      = TY;
     a.alpha_m = (T)mass_coef;
     a.cx      = (T)geo[0];

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "kernels.h"
 
@@ -32,6 +33,9 @@ namespace mpdg
     const T *kcell = nullptr;
     int       tiles_x = 0, tiles_y = 0, ntiles = 0; // ntiles: CTAs of the sweep (one partial sum each)
     long long layers  = 0;                          // columns x cell layers
+    int       slab    = 1;                          // cell layers per slab of the CTA sequence
+    std::vector<long long> range;                   // CTA b: sequence positions [range[b], range[b+1])
+    const long long       *d_range = nullptr;       // the same on the device (uploaded by the caller)
 
     static int padded_pitch(int n0) { return (n0 + 8) / 8 * 8; }
     long long  padded_len() const { return (long long)P0 * n[1] * n[2]; }

@@ -176,7 +176,7 @@ namespace mpdg
     }
 
     template <typename T, int TY, bool FIRST>
-    __global__ void __launch_bounds__(Shape<T, TY>::NT, sizeof(T) == 4 ? 2 : 1)
+    __global__ void __launch_bounds__(Shape<T, TY>::NT, Shape<T, TY>::BYTES <= 112 * 1024 ? 2 : 1)
     heat_cg_sweep_kernel(const __grid_constant__ Sweep<T> a, const __grid_constant__ CUtensorMap tm_r,
                          const __grid_constant__ CUtensorMap tm_v, const __grid_constant__ CUtensorMap tm_p,
                          const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_d)
@@ -282,14 +282,14 @@ namespace mpdg
           };
 
           // the thread's pairs of a staged plane, plane-independent parts (at most PR pairs), packed
-          // into one word: the staged index (11 bits), the window index of z / d (11 bits) and the
-          // flags (10 bits)
+          // into one word: the staged index (12 bits) and the flags (10 bits); the window index of z
+          // and d follows from the staged index, (row - 2) OXW + (x - XOFF)
           constexpr int PR = (S::NPAIR + S::NT - 1) / S::NT;
           constexpr unsigned F_VALID = 1u, F_JOWN = 2u, F_IN = 4u, F_CON = 16u, F_OWN = 64u, F_WIN = 256u;
-          static_assert(S::PLANE < 2048 && S::OPL < 2048, "staged and window indices must fit 11 bits");
-          // FP64 keeps the words in registers (it has spare ones at one CTA per SM); FP32, held to
-          // two CTAs per SM, recomputes them per plane
-          constexpr bool KEEP = sizeof(T) == 8;
+          static_assert(S::PLANE < 4096, "staged indices must fit 12 bits");
+          // a tile that takes a whole SM keeps the words in registers; at two CTAs per SM (FP32,
+          // 8 rows) the registers are short and the words are recomputed per plane
+          constexpr bool KEEP = S::BYTES > 112 * 1024;
           auto pair_word = [&](int k) {
               const int q   = tid + k * S::NT;
               const int row = q / (SX / 2 - 2), pp = q - row * (SX / 2 - 2);
@@ -313,8 +313,7 @@ namespace mpdg
               const bool win = I - 2 * cx0 >= 0 && I - 2 * cx0 <= OXW - 2 && (f & F_JOWN);
               if (win)
                 f |= F_WIN;
-              const unsigned zi = win ? (unsigned)((J - 2 * cy0) * OXW + (I - 2 * cx0)) : 0u;
-              return (f & F_VALID) ? (unsigned)(row * SX + xi) | (zi << 11) | (f << 22) : 0u;
+              return (f & F_VALID) ? (unsigned)(row * SX + xi) | (f << 12) : 0u;
           };
           unsigned pr_w[KEEP ? PR : 1];
           if constexpr (KEEP)
@@ -340,10 +339,10 @@ namespace mpdg
 #pragma unroll
             for (int k = 0; k < PR; ++k)
               {
-                const unsigned w = KEEP ? pr_w[KEEP ? k : 0] : pair_word(k), f = w >> 22;
+                const unsigned w = KEEP ? pr_w[KEEP ? k : 0] : pair_word(k), f = w >> 12;
                 if (!(f & F_VALID))
                   continue;
-                const int si = (int)(w & 2047u), zi = (int)((w >> 11) & 2047u);
+                const int si = (int)(w & 4095u);
                 const PV  r2 = *reinterpret_cast<const PV *>(sr + si);
                 const PV  d2 = *reinterpret_cast<const PV *>(sd + si);
                 PV        v2{}, p2{}, x2{};
@@ -372,6 +371,7 @@ namespace mpdg
                     // I and P0 are even: the pair is one aligned vector in global and shared memory
                     const int       row = si / SX, xi = si - row * SX;
                     const long long g   = gL + (long long)(Y0 + row) * a.P0 + (XB + xi);
+                    const int       zi  = (row - 2) * OXW + (xi - XOFF);
                     const PV        xn{x2.x + alpha * p2.x, x2.y + alpha * p2.y};
                     if ((f & (F_OWN | (F_OWN << 1))) == (F_OWN | (F_OWN << 1)))
                       {

@@ -54,7 +54,7 @@ namespace mpdg
     constexpr int TX   = 32;  // owned cells per tile in x (lanes)
     constexpr int SX   = 72;  // staged x points per row: lattice x from 2 cx0 - 4 (TMA x alignment)
     constexpr int XOFF = 4;   // staged x index of lattice point 2 cx0
-    constexpr int OXW  = 66;  // owned window in x: lattice x from 2 cx0 to 2 cx0 + 65
+    constexpr int OXW  = 68;  // owned window in x: lattice x from 2 cx0 (66 points used, rows of 16 bytes x k)
     constexpr int NV   = 5;   // staged vectors: r, v, p, x, d
 
     template <typename T, int TY>
@@ -66,7 +66,6 @@ namespace mpdg
       static constexpr int OPL   = OXW * OYW;   // owned window points per plane
       static constexpr int NW    = TY + 2;      // warps: TY main rows, halo row, halo column
       static constexpr int NT    = 32 * NW;
-      static constexpr int NPAIR = (SX / 2 - 2) * RY; // point pairs per plane that cells read
       // shared memory layout (bytes, 128-byte aligned sections)
       static constexpr size_t align(size_t b) { return (b + 127) / 128 * 128; }
       static constexpr size_t STAGE_B = align(sizeof(T) * PLANE);      // one vector, one plane
@@ -162,6 +161,37 @@ namespace mpdg
     {
       using V = float2;
     };
+
+    // W consecutive values of T as one aligned vector access (W * sizeof(T) = 16 bytes, or a pair)
+    template <typename T, int W>
+    struct Vec;
+    template <>
+    struct Vec<double, 2>
+    {
+      using V = double2;
+    };
+    template <>
+    struct Vec<float, 2>
+    {
+      using V = float2;
+    };
+    template <>
+    struct Vec<float, 4>
+    {
+      using V = float4;
+    };
+    template <typename T, int W>
+    __device__ __forceinline__ void
+    vload(T (&e)[W], const T *p)
+    {
+      *reinterpret_cast<typename Vec<T, W>::V *>(e) = *reinterpret_cast<const typename Vec<T, W>::V *>(p);
+    }
+    template <typename T, int W>
+    __device__ __forceinline__ void
+    vstore(T *p, const T (&e)[W])
+    {
+      *reinterpret_cast<typename Vec<T, W>::V *>(p) = *reinterpret_cast<const typename Vec<T, W>::V *>(e);
+    }
 
     __device__ __forceinline__ int
     control_check(const CGState &st, int step, double value)
@@ -281,37 +311,43 @@ namespace mpdg
                    ((f & 8u) && J == n1 - 1);
           };
 
-          // the thread's pairs of a staged plane, plane-independent parts (at most PR pairs), packed
-          // into one word: the staged index (12 bits) and the flags (10 bits); the window index of z
-          // and d follows from the staged index, (row - 2) OXW + (x - XOFF)
-          constexpr int PR = (S::NPAIR + S::NT - 1) / S::NT;
-          constexpr unsigned F_VALID = 1u, F_JOWN = 2u, F_IN = 4u, F_CON = 16u, F_OWN = 64u, F_WIN = 256u;
-          static_assert(S::PLANE < 4096, "staged indices must fit 12 bits");
-          // a tile that takes a whole SM keeps the words in registers; at two CTAs per SM (FP32,
-          // 8 rows) the registers are short and the words are recomputed per plane
+          // The update works on units of W consecutive staged points, one aligned vector per vector
+          // and unit: pairs in FP64, quads (16 bytes) in FP32.  The thread's units of a staged plane
+          // and their plane-independent parts (at most PR units) are packed into one word: the staged
+          // index (12 bits) and the flags; the window index of z and d follows from the staged index,
+          // (row - 2) OXW + (x - XOFF).
+          constexpr int W  = sizeof(T) == 4 ? 4 : 2;
+          constexpr int UR = W == 4 ? SX / 4 : SX / 2 - 2; // units per staged row (quads: all 72 x)
+          constexpr int NU = UR * S::RY;
+          constexpr int PR = (NU + S::NT - 1) / S::NT;
+          constexpr unsigned F_VALID = 1u, F_JOWN = 2u, F_WIN = 4u, F_IN = 8u, F_CON = 8u << W, F_OWN = 8u << (2 * W);
+          static_assert(S::PLANE < 4096 && 12 + 3 + 3 * W <= 32, "staged index and flags must fit one word");
+          // a tile that takes a whole SM keeps the words in registers; at two CTAs per SM the
+          // registers are short and the words are recomputed per plane
           constexpr bool KEEP = S::BYTES > 112 * 1024;
-          auto pair_word = [&](int k) {
+          auto unit_word = [&](int k) {
               const int q   = tid + k * S::NT;
-              const int row = q / (SX / 2 - 2), pp = q - row * (SX / 2 - 2);
-              const int xi  = 2 + 2 * pp;            // staged x index (even)
-              const int I   = XB + xi, J = Y0 + row; // lattice coordinates of the pair's first point
-              unsigned   f   = q < S::NPAIR ? F_VALID : 0u;
+              const int row = q / UR, uu = q - row * UR;
+              const int xi  = W == 4 ? 4 * uu : 2 + 2 * uu; // staged x index of the unit's first point
+              const int I   = XB + xi, J = Y0 + row;         // lattice coordinates of that point
+              unsigned   f   = q < NU ? F_VALID : 0u;
               const bool Jin = J >= 0 && J < n1;
               if (J >= 2 * cy0 && J < n1 && (J < 2 * cy0 + 2 * TY || J == n1 - 1))
                 f |= F_JOWN;
 #pragma unroll
-              for (int h = 0; h < 2; ++h)
+              for (int h = 0; h < W; ++h)
                 {
                   const int Ih = I + h;
                   if (Jin && Ih >= 0 && Ih < n0)
                     f |= F_IN << h;
                   if (constrained_xy(Ih, J))
                     f |= F_CON << h;
-                  if (Ih >= 2 * cx0 && Ih < n0 && (Ih < 2 * cx0 + 2 * TX || Ih == n0 - 1))
+                  // the lattice's last point belongs to the tile whose cells end there (a quad of the
+                  // tile to its left may reach it too)
+                  if (Ih >= 2 * cx0 && Ih < n0 && (Ih < 2 * cx0 + 2 * TX || (Ih == n0 - 1 && Ih == 2 * cx0 + 2 * TX)))
                     f |= F_OWN << h;
                 }
-              const bool win = I - 2 * cx0 >= 0 && I - 2 * cx0 <= OXW - 2 && (f & F_JOWN);
-              if (win)
+              if (I - 2 * cx0 >= 0 && I - 2 * cx0 <= OXW - W && (f & F_JOWN))
                 f |= F_WIN;
               return (f & F_VALID) ? (unsigned)(row * SX + xi) | (f << 12) : 0u;
           };
@@ -319,7 +355,7 @@ namespace mpdg
           if constexpr (KEEP)
 #pragma unroll
             for (int k = 0; k < PR; ++k)
-              pr_w[k] = pair_word(k);
+              pr_w[k] = unit_word(k);
 
           // ---- U stage of plane L: vector updates on every staged point the cells read; owned points
           // are written back and summed
@@ -339,57 +375,59 @@ namespace mpdg
 #pragma unroll
             for (int k = 0; k < PR; ++k)
               {
-                const unsigned w = KEEP ? pr_w[KEEP ? k : 0] : pair_word(k), f = w >> 12;
+                const unsigned w = KEEP ? pr_w[KEEP ? k : 0] : unit_word(k), f = w >> 12;
                 if (!(f & F_VALID))
                   continue;
                 const int si = (int)(w & 4095u);
-                const PV  r2 = *reinterpret_cast<const PV *>(sr + si);
-                const PV  d2 = *reinterpret_cast<const PV *>(sd + si);
-                PV        v2{}, p2{}, x2{};
+                T         rv[W], dv[W], vv[W], pv[W], xv[W];
+                vload<T, W>(rv, sr + si);
+                vload<T, W>(dv, sd + si);
                 if constexpr (!FIRST)
                   {
-                    v2 = *reinterpret_cast<const PV *>(sv + si);
-                    p2 = *reinterpret_cast<const PV *>(sp + si);
-                    x2 = *reinterpret_cast<const PV *>(sxv + si);
+                    vload<T, W>(vv, sv + si);
+                    vload<T, W>(pv, sp + si);
+                    vload<T, W>(xv, sxv + si);
                   }
-                T pn[2], rn[2], zn[2];
+                T pn[W], rn[W], zn[W];
 #pragma unroll
-                for (int h = 0; h < 2; ++h)
+                for (int h = 0; h < W; ++h)
                   {
-                    const T    rv   = h ? r2.y : r2.x, dv = h ? d2.y : d2.x;
-                    const T    vv   = h ? v2.y : v2.x, pv = h ? p2.y : p2.x;
                     const bool free = Lin && (f & (F_IN << h)) && !Lcon && !(f & (F_CON << h));
-                    const T    r    = FIRST ? rv : rv - alpha * vv;
-                    const T    z    = dv * r;
+                    const T    r    = FIRST ? rv[h] : rv[h] - alpha * vv[h];
+                    const T    z    = dv[h] * r;
                     rn[h]           = r;
                     zn[h]           = free ? z : T(0);
-                    pn[h]           = free ? (FIRST ? z : z + beta * pv) : T(0);
+                    pn[h]           = free ? (FIRST ? z : z + beta * pv[h]) : T(0);
                   }
-                *reinterpret_cast<PV *>(pr + si) = PV{pn[0], pn[1]};
+                vstore<T, W>(pr + si, pn);
                 if (Lown && (f & F_JOWN))
                   {
-                    // I and P0 are even: the pair is one aligned vector in global and shared memory
+                    // I and P0 are multiples of W: the unit is one aligned vector in global memory
                     const int       row = si / SX, xi = si - row * SX;
                     const long long g   = gL + (long long)(Y0 + row) * a.P0 + (XB + xi);
                     const int       zi  = (row - 2) * OXW + (xi - XOFF);
-                    const PV        xn{x2.x + alpha * p2.x, x2.y + alpha * p2.y};
-                    if ((f & (F_OWN | (F_OWN << 1))) == (F_OWN | (F_OWN << 1)))
+                    constexpr unsigned ALL = ((1u << W) - 1u) * F_OWN;
+                    T xn[W];
+#pragma unroll
+                    for (int h = 0; h < W; ++h)
+                      xn[h] = xv[h] + alpha * pv[h];
+                    if ((f & ALL) == ALL)
                       {
                         if constexpr (!FIRST)
                           {
-                            *reinterpret_cast<PV *>(a.x + g)     = xn;
-                            *reinterpret_cast<PV *>(a.r_out + g) = PV{rn[0], rn[1]};
+                            vstore<T, W>(a.x + g, xn);
+                            vstore<T, W>(a.r_out + g, rn);
                           }
-                        *reinterpret_cast<PV *>(a.p_out + g) = PV{pn[0], pn[1]};
+                        vstore<T, W>(a.p_out + g, pn);
                       }
                     else
 #pragma unroll
-                      for (int h = 0; h < 2; ++h)
+                      for (int h = 0; h < W; ++h)
                         if (f & (F_OWN << h))
                           {
                             if constexpr (!FIRST)
                               {
-                                a.x[g + h]     = h ? xn.y : xn.x;
+                                a.x[g + h]     = xn[h];
                                 a.r_out[g + h] = rn[h];
                               }
                             a.p_out[g + h] = pn[h];
@@ -397,11 +435,11 @@ namespace mpdg
                     // z and d of the owned window (points outside it are never read)
                     if (f & F_WIN)
                       {
-                        *reinterpret_cast<PV *>(zr + zi) = PV{zn[0], zn[1]};
-                        *reinterpret_cast<PV *>(dr + zi) = d2;
+                        vstore<T, W>(zr + zi, zn);
+                        vstore<T, W>(dr + zi, dv);
                       }
 #pragma unroll
-                    for (int h = 0; h < 2; ++h)
+                    for (int h = 0; h < W; ++h)
                       if (f & (F_OWN << h))
                         {
                           acc[0] = fma(rn[h], zn[h], acc[0]);

@@ -42,7 +42,10 @@
 #include <cmath>
 #include <mutex>
 
+#include <type_traits>
+
 #include "cgfused.h"
+#include "pack2.cuh"
 #include "sumfac.cuh"
 #include "tables.h"
 
@@ -51,15 +54,18 @@ namespace mpdg
   namespace cgf
   {
     constexpr int K = 2, N = 3, NE = 2, NO = 1;
-    constexpr int TX   = 32;  // owned cells per tile in x (lanes)
-    constexpr int SX   = 72;  // staged x points per row: lattice x from 2 cx0 - 4 (TMA x alignment)
     constexpr int XOFF = 4;   // staged x index of lattice point 2 cx0
-    constexpr int OXW  = 68;  // owned window in x: lattice x from 2 cx0 (66 points used, rows of 16 bytes x k)
     constexpr int NV   = 5;   // staged vectors: r, v, p, x, d
 
     template <typename T, int TY>
     struct Shape
     {
+      // cells per lane in x: two adjacent cells per thread in FP32, computed as packed pairs
+      static constexpr int C     = sizeof(T) == 4 ? FUSED_C_F32 : 1;
+      using LV                   = std::conditional_t<C == 2, F2, T>; // a lane's values of one point
+      static constexpr int TX    = 32 * C;      // owned cells per tile in x
+      static constexpr int SX    = 2 * TX + 8;  // staged x points per row: lattice x from 2 cx0 - 4 (TMA x alignment)
+      static constexpr int OXW   = 2 * TX + 4;  // owned window in x: lattice x from 2 cx0 (2 TX + 2 used; rows of 16 bytes x k)
       static constexpr int RY    = 2 * TY + 3;  // staged rows: lattice y from 2 cy0 - 2
       static constexpr int PLANE = SX * RY;     // staged points per plane
       static constexpr int OYW   = 2 * TY + 1;  // owned window rows: lattice y from 2 cy0
@@ -74,7 +80,7 @@ namespace mpdg
       static constexpr size_t O_ZS    = O_PRING + 3 * STAGE_B;          // [3] owned planes of z
       static constexpr size_t O_DS    = O_ZS + align(3 * sizeof(T) * OPL); // [3] owned planes of d
       static constexpr size_t O_YX    = O_DS + align(3 * sizeof(T) * OPL);
-      static constexpr size_t O_HX    = O_YX + align(sizeof(T) * (TY + 1) * 9 * 32);
+      static constexpr size_t O_HX    = O_YX + align(sizeof(LV) * (TY + 1) * 9 * 32);
       static constexpr size_t O_RED   = O_HX + align(sizeof(T) * (TY + 1) * 9);
       static constexpr size_t O_BAR   = O_RED + align(sizeof(double) * NW * 5);
       static constexpr size_t BYTES   = O_BAR + 128;
@@ -213,12 +219,14 @@ namespace mpdg
     {
       using S  = Shape<T, TY>;
       using PV = typename Pair<T>::V;
+      using LV = typename S::LV;
+      constexpr int C = S::C, TX = S::TX, SX = S::SX, OXW = S::OXW;
       extern __shared__ __align__(128) unsigned char smem[];
       T                  *stage = reinterpret_cast<T *>(smem + S::O_STAGE);
       T                  *pring = reinterpret_cast<T *>(smem + S::O_PRING);
       T                  *zs    = reinterpret_cast<T *>(smem + S::O_ZS);
       T                  *ds    = reinterpret_cast<T *>(smem + S::O_DS);
-      T                  *yx    = reinterpret_cast<T *>(smem + S::O_YX);
+      LV                 *yx    = reinterpret_cast<LV *>(smem + S::O_YX);
       T                  *hx    = reinterpret_cast<T *>(smem + S::O_HX);
       double             *red   = reinterpret_cast<double *>(smem + S::O_RED);
       unsigned long long *bar   = reinterpret_cast<unsigned long long *>(smem + S::O_BAR);
@@ -235,7 +243,7 @@ namespace mpdg
 
       // thread's cell: main rows (warp < TY), halo row (warp == TY), halo column (warp == TY + 1)
       const int  role = warp < TY ? 0 : (warp == TY ? 1 : 2);
-      const int  cxl = role == 2 ? -1 : lane, cyl = role == 0 ? warp : (role == 1 ? -1 : lane - 1);
+      const int  cxl = role == 2 ? -1 : C * lane, cyl = role == 0 ? warp : (role == 1 ? -1 : lane - 1);
       const bool active = role != 2 || lane <= TY;
       const int  sxi = XOFF + 2 * cxl, syi = 2 + 2 * cyl; // staged index of the cell's first point
 
@@ -279,6 +287,8 @@ namespace mpdg
           const int  cx = cx0 + cxl, cy = cy0 + cyl;
           const bool vxy    = active && cx >= 0 && cx < a.m[0] && cy >= 0 && cy < a.m[1];
           const bool last_x = cx == a.m[0] - 1, last_y = cy == a.m[1] - 1;
+          // the second cell of the lane (two cells per lane; the halo column has one)
+          const bool vx1 = C == 2 && role != 2 && vxy && cx + 1 < a.m[0];
 
           auto issue = [&](int slot, int L) {
             // one thread: the plane L of every staged vector into slot
@@ -460,18 +470,39 @@ namespace mpdg
           __syncthreads();
           refill(Pfirst);
 
-          T carry[N * N];
+          // a scalar as the lane's value type, and one cell's component of a lane value
+          auto bc = [](T x) -> LV {
+            if constexpr (C == 2)
+              return f2(x);
+            else
+              return x;
+          };
+          auto comp = [](const LV &v, int c) -> T {
+            if constexpr (C == 2)
+              return c ? v.v.y : v.v.x;
+            else
+              return v;
+          };
+          LV carry[N * N];
 #pragma unroll
           for (int q = 0; q < N * N; ++q)
-            carry[q] = T(0);
+            carry[q] = bc(T(0));
 
           for (int lz = lz_begin; lz < cz1; ++lz)
             {
               const bool halo_layer = lz < cz0;
-              T          kc         = T(0);
-              if (vxy)
-                kc = a.kcell ? a.kcell[(long long)cx + (long long)a.m[0] * ((long long)cy + (long long)a.m[1] * lz)]
-                             : a.kconst;
+              // conductivity of the lane's cells
+              auto kload = [&](int x, bool v) -> T {
+                if (!v)
+                  return T(0);
+                return a.kcell ? a.kcell[(long long)x + (long long)a.m[0] * ((long long)cy + (long long)a.m[1] * lz)]
+                               : a.kconst;
+              };
+              LV kc;
+              if constexpr (C == 2)
+                kc = f2(kload(cx, vxy), kload(cx + 1, vx1));
+              else
+                kc = kload(cx, vxy);
               update_plane(2 * lz + 1);
               __syncthreads();
               refill(2 * lz + 1);
@@ -479,8 +510,8 @@ namespace mpdg
               __syncthreads();
               refill(2 * lz + 2);
 
-              // ---- cell stage: u = A_c p_c for the thread's cell
-              T u[N * N * N];
+              // ---- cell stage: u = A_c p_c for the lane's cells
+              LV u[N * N * N];
 #pragma unroll
               for (int l = 0; l < N; ++l)
                 {
@@ -488,51 +519,82 @@ namespace mpdg
 #pragma unroll
                   for (int j = 0; j < N; ++j)
                     {
-                      // sxi and SX are even: points 0, 1 of the row are one aligned pair
                       const T *row = pl + (syi + j) * SX + sxi;
-                      const PV p01 = vxy ? *reinterpret_cast<const PV *>(row) : PV{T(0), T(0)};
-                      u[(l * N + j) * N + 0] = p01.x;
-                      u[(l * N + j) * N + 1] = p01.y;
-                      u[(l * N + j) * N + 2] = vxy ? row[2] : T(0);
+                      if constexpr (C == 2)
+                        {
+                          // the two cells' 5 points of the row: one aligned quad and one more (the
+                          // halo column: its single cell, an aligned pair and one more)
+                          T r[5] = {T(0), T(0), T(0), T(0), T(0)};
+                          if (vxy)
+                            {
+                              if (role != 2)
+                                {
+                                  const float4 q4 = *reinterpret_cast<const float4 *>(row);
+                                  r[0] = q4.x, r[1] = q4.y, r[2] = q4.z, r[3] = q4.w;
+                                  r[4] = row[4];
+                                }
+                              else
+                                {
+                                  const PV q2 = *reinterpret_cast<const PV *>(row);
+                                  r[0] = q2.x, r[1] = q2.y, r[2] = row[2];
+                                }
+                            }
+#pragma unroll
+                          for (int i = 0; i < N; ++i)
+                            u[(l * N + j) * N + i] = f2(r[i], vx1 ? r[i + 2] : T(0));
+                        }
+                      else
+                        {
+                          // sxi and SX are even: points 0, 1 of the row are one aligned pair
+                          const PV p01 = vxy ? *reinterpret_cast<const PV *>(row) : PV{T(0), T(0)};
+                          u[(l * N + j) * N + 0] = p01.x;
+                          u[(l * N + j) * N + 1] = p01.y;
+                          u[(l * N + j) * N + 2] = vxy ? row[2] : T(0);
+                        }
                     }
                 }
               {
-                const T kcx = kc * a.cx, kcy = kc * a.cy, kcz = kc * a.cz, am = a.alpha_m;
-                xy_planes<T, N, N, true>(u, we, wo);
+                const LV kcx = kc * bc(a.cx), kcy = kc * bc(a.cy), kcz = kc * bc(a.cz), am = bc(a.alpha_m);
+                xy_planes<LV, N, N, true, T>(u, we, wo);
 #pragma unroll
                 for (int q = 0; q < N * N; ++q)
-                  fwd_line<T, N, N * N>(u, q, we, wo);
-                T form = T(0);
+                  fwd_line<LV, N, N * N, T>(u, q, we, wo);
+                LV form = bc(T(0));
 #pragma unroll
                 for (int c = 0; c < N; ++c)
                   {
-                    const T tz = fma(kcz, lam[c], am);
+                    const LV tz = fma(kcz, bc(lam[c]), am);
 #pragma unroll
                     for (int b = 0; b < N; ++b)
                       {
-                        const T tyz = fma(kcy, lam[b], tz);
+                        const LV tyz = fma(kcy, bc(lam[b]), tz);
 #pragma unroll
                         for (int aa = 0; aa < N; ++aa)
                           {
-                            const T d = fma(kcx, lam[aa], tyz);
-                            T      &v = u[(c * N + b) * N + aa];
-                            form      = fma(d * v, v, form);
+                            const LV d = fma(kcx, bc(lam[aa]), tyz);
+                            LV      &v = u[(c * N + b) * N + aa];
+                            form       = fma(d * v, v, form);
                             v *= d;
                           }
                       }
                   }
-                if (role == 0 && !halo_layer && vxy)
-                  acc[2] += form;
+                if (role == 0 && !halo_layer)
+                  {
+                    if (vxy)
+                      acc[2] += comp(form, 0);
+                    if (C == 2 && vx1)
+                      acc[2] += comp(form, 1);
+                  }
 #pragma unroll
                 for (int q = 0; q < N * N; ++q)
-                  bwd_line<T, N, N * N>(u, q, we, wo);
-                xy_planes<T, N, N, false>(u, we, wo);
+                  bwd_line<LV, N, N * N, T>(u, q, we, wo);
+                xy_planes<LV, N, N, false, T>(u, we, wo);
               }
               // ---- x faces: the halo column hands its x = 2 face to lane 0 of every other row
               if (role == 2 && active)
 #pragma unroll
                 for (int q = 0; q < N * N; ++q)
-                  hx[lane * 9 + q] = u[q * N + K];
+                  hx[lane * 9 + q] = comp(u[q * N + K], 0);
               __syncthreads();
               if (role != 2)
                 {
@@ -540,8 +602,19 @@ namespace mpdg
 #pragma unroll
                   for (int q = 0; q < N * N; ++q)
                     {
-                      const T v = __shfl_up_sync(0xffffffffu, u[q * N + K], 1);
-                      u[q * N] += lane > 0 ? v : hx[hrow * 9 + q];
+                      if constexpr (C == 2)
+                        {
+                          // the lane's second cell takes its first cell's x = 2 face; the first cell
+                          // takes the x = 2 face of the left lane's second cell
+                          const T v = __shfl_up_sync(0xffffffffu, u[q * N + K].v.y, 1);
+                          u[q * N].v.y += u[q * N + K].v.x;
+                          u[q * N].v.x += lane > 0 ? v : hx[hrow * 9 + q];
+                        }
+                      else
+                        {
+                          const T v = __shfl_up_sync(0xffffffffu, u[q * N + K], 1);
+                          u[q * N] += lane > 0 ? v : hx[hrow * 9 + q];
+                        }
                     }
                   // y faces: main rows and the halo row hand their y = 2 face to the next row
                   const int slot = role == 0 ? warp : TY;
@@ -581,33 +654,41 @@ namespace mpdg
                             {
                               if (j == K && !last_y)
                                 continue;
-                              const int J = 2 * cy + j;
-                              T        *vrow = a.v_out + (long long)L * plane_stride + (long long)J * a.P0;
-                              const int o0 = (J - 2 * cy0) * OXW + 2 * (cx - cx0); // even: aligned pairs
-                              const PV  z01 = *reinterpret_cast<const PV *>(zl + o0);
-                              const PV  d01 = *reinterpret_cast<const PV *>(dl + o0);
-                              const T   zz[N] = {z01.x, z01.y, last_x ? zl[o0 + 2] : T(0)};
-                              const T   dd[N] = {d01.x, d01.y, last_x ? dl[o0 + 2] : T(0)};
+                              const int  J    = 2 * cy + j;
+                              T         *vrow = a.v_out + (long long)L * plane_stride + (long long)J * a.P0;
                               const bool Jcon = Lcon || ((a.faces & 4u) && J == 0) || ((a.faces & 8u) && J == n1 - 1);
-                              T          vv[N];
-                              T          s2 = T(0), s3 = T(0);
 #pragma unroll
-                              for (int i = 0; i < N; ++i)
+                              for (int c = 0; c < C; ++c)
                                 {
-                                  const int  I   = 2 * cx + i;
-                                  const bool con = Jcon || ((a.faces & 1u) && I == 0) || ((a.faces & 2u) && I == n0 - 1);
-                                  vv[i]          = con ? T(0) : u[(l * N + j) * N + i];
-                                  if (i < K || last_x)
+                                  if (c == 1 && !vx1)
+                                    continue;
+                                  const int  xc = cx + c;
+                                  const bool lx = xc == a.m[0] - 1;
+                                  const int  o0 = (J - 2 * cy0) * OXW + 2 * (xc - cx0); // even: aligned pairs
+                                  const PV   z01 = *reinterpret_cast<const PV *>(zl + o0);
+                                  const PV   d01 = *reinterpret_cast<const PV *>(dl + o0);
+                                  const T    zz[N] = {z01.x, z01.y, lx ? zl[o0 + 2] : T(0)};
+                                  const T    dd[N] = {d01.x, d01.y, lx ? dl[o0 + 2] : T(0)};
+                                  T          vv[N];
+                                  T          s2 = T(0), s3 = T(0);
+#pragma unroll
+                                  for (int i = 0; i < N; ++i)
                                     {
-                                      s2 = fma(zz[i], vv[i], s2);
-                                      s3 = fma(dd[i] * vv[i], vv[i], s3);
+                                      const int  I   = 2 * xc + i;
+                                      const bool con = Jcon || ((a.faces & 1u) && I == 0) || ((a.faces & 2u) && I == n0 - 1);
+                                      vv[i]          = con ? T(0) : comp(u[(l * N + j) * N + i], c);
+                                      if (i < K || lx)
+                                        {
+                                          s2 = fma(zz[i], vv[i], s2);
+                                          s3 = fma(dd[i] * vv[i], vv[i], s3);
+                                        }
                                     }
+                                  acc[3] += s2;
+                                  acc[4] += s3;
+                                  *reinterpret_cast<PV *>(vrow + 2 * xc) = PV{vv[0], vv[1]};
+                                  if (lx)
+                                    vrow[2 * xc + 2] = vv[2];
                                 }
-                              acc[3] += s2;
-                              acc[4] += s3;
-                              *reinterpret_cast<PV *>(vrow + 2 * cx) = PV{vv[0], vv[1]};
-                              if (last_x)
-                                vrow[2 * cx + 2] = vv[2];
                             }
                         }
                     }
@@ -726,7 +807,8 @@ namespace mpdg
     const int       TY   = sizeof(T) == 8 ? FUSED_TY_F64 : FUSED_TY_F32;
     cuuint64_t      dims[3]    = {(cuuint64_t)n[0], (cuuint64_t)n[1], (cuuint64_t)n[2]};
     cuuint64_t      strides[2] = {(cuuint64_t)P0 * sizeof(T), (cuuint64_t)P0 * n[1] * sizeof(T)};
-    cuuint32_t      box[3]     = {(cuuint32_t)cgf::SX, (cuuint32_t)(2 * TY + 3), 1u};
+    cuuint32_t      box[3]     = {(cuuint32_t)cgf::Shape<T, sizeof(T) == 8 ? FUSED_TY_F64 : FUSED_TY_F32>::SX,
+                                  (cuuint32_t)(2 * TY + 3), 1u};
     cuuint32_t      estr[3]    = {1u, 1u, 1u};
     const CUresult  r = fn(map, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
                           const_cast<T *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -754,7 +836,8 @@ namespace mpdg
   FusedCG<T>::plan(int sm_count)
   {
     const int TY = sizeof(T) == 8 ? FUSED_TY_F64 : FUSED_TY_F32;
-    tiles_x      = (m[0] + cgf::TX - 1) / cgf::TX;
+    constexpr int TXC = cgf::Shape<T, sizeof(T) == 8 ? FUSED_TY_F64 : FUSED_TY_F32>::TX;
+    tiles_x      = (m[0] + TXC - 1) / TXC;
     tiles_y      = (m[1] + TY - 1) / TY;
     // CTAs resident per SM from the shared memory footprint (227 KB usable per CTA, 228 KB per SM)
     const int per_sm = std::max(1, (int)(233472 / (smem_bytes() + 1024)));

@@ -15,14 +15,24 @@ namespace mpdg
 #ifndef MPDG_FUSED_TY_F64
 #define MPDG_FUSED_TY_F64 8
 #endif
+#ifndef MPDG_FUSED_C_F32
+#define MPDG_FUSED_C_F32 1
+#endif
 #ifndef MPDG_FUSED_TY_F32
-#define MPDG_FUSED_TY_F32 16
+#define MPDG_FUSED_TY_F32 (MPDG_FUSED_C_F32 == 2 ? 8 : 16)
 #endif
   constexpr int FUSED_TY_F64 = MPDG_FUSED_TY_F64; // owned cell rows per tile (FP64)
   // owned cell rows per tile (FP32): 16 rows take one SM each (200 KB of shared memory, 18 warps) and
   // halve the share of halo rows against two CTAs of 8 rows per SM (215 against 246 us per iteration
   // on 128^3)
   constexpr int FUSED_TY_F32 = MPDG_FUSED_TY_F32;
+  // cells per lane in x (FP32): 2 computes two adjacent cells per thread as packed FP32 pairs
+  // (tiles of 64 x 8 cells, one CTA per SM, 10 warps); it measured slower than one cell per lane
+  // with 16-row tiles (215 against 206 us per iteration on 128^3: half the resident warps, and the
+  // register cap of a 320-thread CTA spills), so 1 is the default and 2 stays selectable
+  // (-DMPDG_FUSED_C_F32=2)
+  constexpr int FUSED_C_F32 = MPDG_FUSED_C_F32;
+  static_assert(FUSED_C_F32 == 1 || FUSED_C_F32 == 2, "one or two cells per lane");
 
   // Problem description and tiling of the fused sweep; vectors in the padded layout (x rows of P0
   // entries, P0 = n0 rounded up to a multiple of 8 and > n0).

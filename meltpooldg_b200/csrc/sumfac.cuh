@@ -23,10 +23,11 @@ namespace mpdg
     T                    lam3[N * N * N];               // cx lam_a + cy lam_b + cz lam_c (modal order)
   };
 
-  // nodal -> modal along one line v[b + k*S], k < N; modal order: even modes, then odd modes
-  template <typename T, int N, int S>
+  // nodal -> modal along one line v[b + k*S], k < N; modal order: even modes, then odd modes.
+  // The values may be packed pairs (TT the scalar type of the tables, T the value type).
+  template <typename T, int N, int S, typename TT = T>
   __device__ __forceinline__ void
-  fwd_line(T *v, const int b, const T *we, const T *wo)
+  fwd_line(T *v, const int b, const TT *we, const TT *wo)
   {
     constexpr int NE = (N + 1) / 2, NO = N / 2;
     T             e[NE], o[NO > 0 ? NO : 1];
@@ -60,9 +61,9 @@ namespace mpdg
   }
 
   // modal -> nodal along one line (transpose of fwd_line)
-  template <typename T, int N, int S>
+  template <typename T, int N, int S, typename TT = T>
   __device__ __forceinline__ void
-  bwd_line(T *v, const int b, const T *we, const T *wo)
+  bwd_line(T *v, const int b, const TT *we, const TT *wo)
   {
     constexpr int NE = (N + 1) / 2, NO = N / 2;
     T             ev[NE], od[NO > 0 ? NO : 1];
@@ -97,9 +98,9 @@ namespace mpdg
   }
 
   // Apply fwd/bwd in x and y to P planes of N x N values (plane stride N*N, x fastest).
-  template <typename T, int N, int P, bool FWD>
+  template <typename T, int N, int P, bool FWD, typename TT = T>
   __device__ __forceinline__ void
-  xy_planes(T *v, const T *we, const T *wo)
+  xy_planes(T *v, const TT *we, const TT *wo)
   {
     if constexpr (FWD)
       {
@@ -108,10 +109,10 @@ namespace mpdg
           {
 #pragma unroll
             for (int j = 0; j < N; ++j)
-              fwd_line<T, N, 1>(v, p * N * N + j * N, we, wo);
+              fwd_line<T, N, 1, TT>(v, p * N * N + j * N, we, wo);
 #pragma unroll
             for (int i = 0; i < N; ++i)
-              fwd_line<T, N, N>(v, p * N * N + i, we, wo);
+              fwd_line<T, N, N, TT>(v, p * N * N + i, we, wo);
           }
       }
     else
@@ -121,10 +122,10 @@ namespace mpdg
           {
 #pragma unroll
             for (int i = 0; i < N; ++i)
-              bwd_line<T, N, N>(v, p * N * N + i, we, wo);
+              bwd_line<T, N, N, TT>(v, p * N * N + i, we, wo);
 #pragma unroll
             for (int j = 0; j < N; ++j)
-              bwd_line<T, N, 1>(v, p * N * N + j * N, we, wo);
+              bwd_line<T, N, 1, TT>(v, p * N * N + j * N, we, wo);
           }
       }
   }

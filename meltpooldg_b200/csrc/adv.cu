@@ -31,12 +31,13 @@
 
 namespace mpdg
 {
-  // Per degree (1, 2) in constant memory, uploaded once per device:
+  // Per degree (1..3) in constant memory, uploaded once per device:
   //   [B (n*n): phi_i(x_q) | D (n*n): collocation derivative on the Gauss points |
   //    qp (n): Gauss points | qw3 (n^3): tensor Gauss weights]
-  constexpr int ADV_TAB = 48;
-  __constant__ double c_adv_d[3][ADV_TAB];
-  __constant__ float  c_adv_f[3][ADV_TAB];
+  constexpr int ADV_KMAX = 3;
+  constexpr int ADV_TAB  = 2 * 16 + 4 + 64;
+  __constant__ double c_adv_d[ADV_KMAX + 1][ADV_TAB];
+  __constant__ float  c_adv_f[ADV_KMAX + 1][ADV_TAB];
 
   template <typename T>
   __device__ __forceinline__ const T *
@@ -67,7 +68,7 @@ namespace mpdg
     // cell-independent factors per direction d and Gauss point q (N^3 <= 27 used):
     //   pa = th_adv det / h_d w_q,  pb = pa (G_d. (h (x) qp_q)),  pd = th_dif det / h_d^2 w_q;
     // pm = det inv_dt w_q.  The velocity term of a cell is (vd0 pa + pb) g, vd0 = v_d(cell origin).
-    T pa[3][27], pb[3][27], pd[3][27], pm[27];
+    T pa[3][64], pb[3][64], pd[3][64], pm[64];
   };
 
   // out = M in along a line (in place), M[a*N+b], TR: transpose
@@ -297,11 +298,12 @@ namespace mpdg
   struct AdvLayout
   {
     static constexpr int  N  = K + 1;
-    static constexpr int  BX = 8, BY = 8, BZ = (K == 1 ? 8 : 4);
+    static constexpr int  BX = 8, BY = 8, BZ = (K == 1 ? 8 : (K == 2 ? 4 : 2));
     static constexpr int  NT = BX * BY * BZ;
     using BR                 = Brick<K, BX, BY, BZ, NT>;
     static constexpr size_t bytes = sizeof(T) * 2 * (size_t)BR::NPTS; // staged input + accumulator
-    static constexpr int    MINB  = sizeof(T) == 8 ? MPDG_ADV_MINB_F64 : MPDG_ADV_MINB_F32; // CTAs per SM
+    // CTAs per SM (k = 3: two CTAs of 128 threads, so that the two 64-value cell arrays fit registers)
+    static constexpr int    MINB  = K == 3 ? 2 : (sizeof(T) == 8 ? MPDG_ADV_MINB_F64 : MPDG_ADV_MINB_F32);
   };
 
   // The SUPG form keeps a third cell array (the strong residual).  At k = 2 it is held to half the
@@ -456,9 +458,9 @@ namespace mpdg
     std::lock_guard<std::mutex> lock(mtx);
     if (done.count(dev))
       return cudaSuccess;
-    double hd[3][ADV_TAB] = {};
-    float  hf[3][ADV_TAB] = {};
-    for (int K = 1; K <= 2; ++K)
+    double hd[ADV_KMAX + 1][ADV_TAB] = {};
+    float  hf[ADV_KMAX + 1][ADV_TAB] = {};
+    for (int K = 1; K <= ADV_KMAX; ++K)
       {
         const Tables1D &t = tables(K);
         const int       n = t.n;
@@ -542,8 +544,13 @@ namespace mpdg
     const bool vdof = h.p.vfield[0] != nullptr;
     if (vdof && h.p.supg)
       return cudaErrorInvalidValue; // SUPG with a DoF-vector velocity is not built
-    auto kern = h.p.supg ? adv_apply_kernel<K, T, MODE, true>
-                         : (vdof ? adv_apply_kernel<K, T, MODE, false, true> : adv_apply_kernel<K, T, MODE, false>);
+    // SUPG and the DoF-vector velocity keep a third cell array and are built for k <= 2 only
+    auto kern = adv_apply_kernel<K, T, MODE, false>;
+    if constexpr (K <= 2)
+      kern = h.p.supg ? adv_apply_kernel<K, T, MODE, true>
+                      : (vdof ? adv_apply_kernel<K, T, MODE, false, true> : adv_apply_kernel<K, T, MODE, false>);
+    else if (h.p.supg || vdof)
+      return cudaErrorInvalidValue;
     static std::atomic<unsigned long long> devices{0}, devices_supg{0}, devices_vdof{0};
     if (cudaError_t e = ensure_smem(kern, LAY::bytes, h.p.supg ? devices_supg : (vdof ? devices_vdof : devices));
         e != cudaSuccess)
@@ -573,6 +580,7 @@ namespace mpdg
       {
         case 1: return adv_mode<1, T>(h, s);
         case 2: return adv_mode<2, T>(h, s);
+        case 3: return adv_mode<3, T>(h, s);
         default: return cudaErrorInvalidValue;
       }
   }
@@ -587,11 +595,17 @@ namespace mpdg
         shape[1] = AdvLayout<1, T>::BY;
         shape[2] = AdvLayout<1, T>::BZ;
       }
-    else
+    else if (K == 2)
       {
         shape[0] = AdvLayout<2, T>::BX;
         shape[1] = AdvLayout<2, T>::BY;
         shape[2] = AdvLayout<2, T>::BZ;
+      }
+    else
+      {
+        shape[0] = AdvLayout<3, T>::BX;
+        shape[1] = AdvLayout<3, T>::BY;
+        shape[2] = AdvLayout<3, T>::BZ;
       }
   }
 
@@ -683,7 +697,7 @@ namespace mpdg
   cudaError_t
   adv_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, cudaStream_t s)
   {
-    if (K < 1 || K > 2)
+    if (K < 1 || K > ADV_KMAX)
       return cudaErrorInvalidValue;
     AdvDiagArgs<T>   a{};
     const Tables1D &t = tables(K);
@@ -719,8 +733,10 @@ namespace mpdg
     const int       threads = std::min(1024, std::max(32, (g.n[0] + 31) / 32 * 32));
     if (K == 1)
       adv_diag_kernel<1, T><<<blocks, threads, 0, s>>>(a);
-    else
+    else if (K == 2)
       adv_diag_kernel<2, T><<<blocks, threads, 0, s>>>(a);
+    else
+      adv_diag_kernel<3, T><<<blocks, threads, 0, s>>>(a);
     return cudaGetLastError();
   }
 
@@ -789,10 +805,10 @@ namespace mpdg
   cudaError_t
   adv_supg_diagonal(const GridDesc &g, int K, const AdvParams &p, T *diag, cudaStream_t s)
   {
-    if (K < 1 || K > 2)
-      return cudaErrorInvalidValue;
     if (!p.supg)
       return cudaSuccess;
+    if (K < 1 || K > 2)
+      return cudaErrorInvalidValue;
     AdvSupgDiagArgs<T> a{};
     const Tables1D    &t = tables(K);
     const int          n = t.n;

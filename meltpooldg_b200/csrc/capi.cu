@@ -1020,8 +1020,8 @@ mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op
     return fail(MPDG_ERR_UNSUPPORTED, "reinitialisation operator: FE_Q degree must be 1..2");
   if (params->kind == MPDG_HEAT && (mesh->degree < 1 || mesh->degree > 4))
     return fail(MPDG_ERR_UNSUPPORTED, "heat operator: FE_Q degree must be 1..4");
-  if (params->kind == MPDG_ADVDIFF && (mesh->degree < 1 || mesh->degree > 2))
-    return fail(MPDG_ERR_UNSUPPORTED, "advection-diffusion operator: FE_Q degree must be 1..2");
+  if (params->kind == MPDG_ADVDIFF && (mesh->degree < 1 || mesh->degree > 3))
+    return fail(MPDG_ERR_UNSUPPORTED, "advection-diffusion operator: FE_Q degree must be 1..3");
   for (int d = 0; d < 3; ++d)
     if (mesh->cells[d] < 1 || !(mesh->length[d] > 0.0))
       return fail(MPDG_ERR_ARG, "mesh cells and lengths must be positive");
@@ -1365,6 +1365,8 @@ mpdg_op_set_velocity_field(mpdg_op *op, const double *vx, const double *vy, cons
     return fail(MPDG_ERR_ARG, "a velocity field needs all three components");
   if (vx && op->supg)
     return fail(MPDG_ERR_UNSUPPORTED, "SUPG with a DoF-vector velocity is not supported");
+  if (vx && op->degree > 2)
+    return fail(MPDG_ERR_UNSUPPORTED, "a DoF-vector velocity is supported for FE_Q degree 1..2");
   op->d_vfield[0] = vx;
   op->d_vfield[1] = vy;
   op->d_vfield[2] = vz;
@@ -1416,6 +1418,8 @@ mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient)
     return fail(MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator");
   if (enabled && op->d_vfield[0])
     return fail(MPDG_ERR_UNSUPPORTED, "SUPG with a DoF-vector velocity is not supported");
+  if (enabled && op->degree > 2)
+    return fail(MPDG_ERR_UNSUPPORTED, "SUPG is supported for FE_Q degree 1..2");
   op->supg      = enabled ? 1 : 0;
   op->supg_coef = coefficient;
   return MPDG_OK;

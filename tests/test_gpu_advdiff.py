@@ -22,7 +22,8 @@ def adv_pair(degree, m, faces=0, mask=None, dt=5e-3, theta=1.0, eps=1e-3, vel=VE
     return o, g, om, cm
 
 
-@pytest.mark.parametrize("degree,m", [(1, (9, 8, 9)), (1, (17, 5, 3)), (2, (9, 8, 5)), (2, (16, 16, 16))])
+@pytest.mark.parametrize("degree,m", [(1, (9, 8, 9)), (1, (17, 5, 3)), (2, (9, 8, 5)), (2, (16, 16, 16)), (3, (6, 5, 4)),
+                                      (3, (9, 8, 3))])
 @pytest.mark.parametrize("theta,eps", [(1.0, 1e-3), (0.5, 0.0)])
 def test_vmult_matches_oracle(degree, m, theta, eps):
     import torch
@@ -41,7 +42,7 @@ def test_vmult_matches_oracle(degree, m, theta, eps):
     assert g.device_errors() == 0
 
 
-@pytest.mark.parametrize("degree,m", [(1, (7, 6, 9)), (2, (5, 7, 4))])
+@pytest.mark.parametrize("degree,m", [(1, (7, 6, 9)), (2, (5, 7, 4)), (3, (5, 4, 6))])
 @pytest.mark.parametrize("theta,eps", [(1.0, 1e-3), (0.5, 0.2)])
 def test_inverse_diagonal_closed_form(degree, m, theta, eps):
     """The closed-form diagonal (1-D quadrature moments) against the oracle's unit-vector applies."""
@@ -69,9 +70,10 @@ def test_per_dof_mask_and_diagonal():
     assert rel_err(d.cpu().numpy(), o.inverse_diagonal()) <= 1e-12
 
 
+@pytest.mark.parametrize("degree,m", [(2, (9, 8, 5)), (3, (5, 6, 4))])
 @pytest.mark.parametrize("theta", [1.0, 0.5])
-def test_create_rhs(theta):
-    o, g, om, cm = adv_pair(2, (9, 8, 5), faces=0b000011, theta=theta)
+def test_create_rhs(degree, m, theta):
+    o, g, om, cm = adv_pair(degree, m, faces=0b000011, theta=theta)
     u_old = uniform_dofs(om, seed=13)
     ref = uniform_dofs(om, seed=14)
     dst = to_gpu(ref)
@@ -80,12 +82,13 @@ def test_create_rhs(theta):
     assert rel_err(dst.cpu().numpy(), ref) <= 1e-12
 
 
-def test_gmres_solve():
+@pytest.mark.parametrize("degree,m", [(2, (12, 12, 12)), (3, (7, 6, 8))])
+def test_gmres_solve(degree, m):
     import torch
 
     from meltpooldg_b200.operators import LinearSolver, LinearSolverData
 
-    o, g, om, cm = adv_pair(2, (12, 12, 12), vel=VEL_ROT)
+    o, g, om, cm = adv_pair(degree, m, vel=VEL_ROT)
     b = uniform_dofs(om, seed=15)
     x_ref = np.zeros(om.ndofs)
     it_ref, _ = osolve(o, x_ref, b, "gmres", inv_diag=o.inverse_diagonal(), rel_tol=1e-10)
@@ -145,3 +148,19 @@ def test_velocity_field_matches_oracle(degree, m, faces):
     gf.vmult(yf, to_gpu(u))
     assert rel_err(yf.cpu().numpy(), ya.cpu().numpy()) <= 1e-12
     assert om0.ndofs == om.ndofs and g.device_errors() == 0
+
+
+def test_degree_three_limits():
+    """FE_Q(3) covers the plain advection-diffusion operator; SUPG and a DoF-vector velocity are k <= 2."""
+    import torch
+
+    from meltpooldg_b200 import _lib as L
+
+    o, g, om, cm = adv_pair(3, (4, 4, 4))
+    with pytest.raises(L.MpdgError) as exc:
+        g.set_convection_stabilization("SUPG", -1.0)
+    assert exc.value.code == L.MPDG_ERR_UNSUPPORTED
+    v = torch.zeros(om.ndofs, dtype=torch.float64, device="cuda")
+    with pytest.raises(L.MpdgError) as exc:
+        g.set_velocity_field(v, v, v)
+    assert exc.value.code == L.MPDG_ERR_UNSUPPORTED

@@ -61,7 +61,7 @@ enum mpdg_op_kind
   MPDG_HEAT    = 0, /* (rho c_p/dt) M + div(k grad), source/heat/heat_diffuse_operator.cpp      */
   MPDG_ADVDIFF = 1, /* M/dt + theta (v.grad + eps K), source/level_set/advection_diffusion_operator.cpp */
   MPDG_REINIT  = 2  /* M/dt + div(D grad), D = eps_t I + (eps_n - eps_t) n n^T: conservative level-set
-                       reinitialisation, source/level_set/olsson_CG_operator.cpp (FE_Q(1, 2); set the
+                       reinitialisation, source/level_set/olsson_CG_operator.cpp (FE_Q(1..3); set the
                        normal field with mpdg_op_set_reinit) */
 };
 
@@ -80,7 +80,7 @@ enum mpdg_precond_kind
 typedef struct mpdg_mesh_desc
 {
   int32_t        degree;          /* FE_Q degree: heat 1..4, advection-diffusion 1..3 (SUPG and a
-                                     DoF-vector velocity 1..2), reinitialisation 1..2 */
+                                     DoF-vector velocity 1..2), reinitialisation 1..3 */
   int32_t        cells[3];        /* cells per direction                                */
   double         origin[3];       /* lower corner of the box                            */
   double         length[3];       /* box edge lengths                                   */
@@ -222,7 +222,7 @@ MPDG_API int mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient);
 MPDG_API int mpdg_op_set_reinit(mpdg_op *op, double eps_normal, double eps_tangential, double normal_tolerance,
                                 const double *nx, const double *ny, const double *nz);
 
-/* Right-hand sides of the level set's projections, FE_Q(1, 2), on the lattice and constraint set of
+/* Right-hand sides of the level set's projections, FE_Q(1..3), on the lattice and constraint set of
    op (any kind; the projection itself is M + damping K, a heat operator with rho_cp = dt = 1 and
    conductivity = the reference's cell-size-dependent damping, solved per component), no narrow band:
    - NormalVectorOperator::create_rhs (source/level_set/normal_vector_operator.cpp:160-240):

@@ -1016,8 +1016,8 @@ mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op
   *out = nullptr;
   if (params->kind != MPDG_HEAT && params->kind != MPDG_ADVDIFF && params->kind != MPDG_REINIT)
     return fail(MPDG_ERR_ARG, "unknown operator kind");
-  if (params->kind == MPDG_REINIT && (mesh->degree < 1 || mesh->degree > 2))
-    return fail(MPDG_ERR_UNSUPPORTED, "reinitialisation operator: FE_Q degree must be 1..2");
+  if (params->kind == MPDG_REINIT && (mesh->degree < 1 || mesh->degree > 3))
+    return fail(MPDG_ERR_UNSUPPORTED, "reinitialisation operator: FE_Q degree must be 1..3");
   if (params->kind == MPDG_HEAT && (mesh->degree < 1 || mesh->degree > 4))
     return fail(MPDG_ERR_UNSUPPORTED, "heat operator: FE_Q degree must be 1..4");
   if (params->kind == MPDG_ADVDIFF && (mesh->degree < 1 || mesh->degree > 3))
@@ -1330,8 +1330,8 @@ mpdg_level_set_normal_rhs(mpdg_op *op, const double *psi, int normalized, double
     return e;
   if (!psi || !nx || !ny || !nz)
     return fail(MPDG_ERR_ARG, "null argument to mpdg_level_set_normal_rhs");
-  if (op->degree > 2)
-    return fail(MPDG_ERR_UNSUPPORTED, "the level-set right-hand sides support FE_Q degree 1..2");
+  if (op->degree > 3)
+    return fail(MPDG_ERR_UNSUPPORTED, "the level-set right-hand sides support FE_Q degree 1..3");
   // the normal's narrow band masks with the level set psi itself (normal_vector_operator.cpp:184-189)
   MPDG_CUDA(level_set_rhs(op->grid(), op->degree, op->h, 0, normalized ? 1 : 0, 0.0, psi, nullptr, nullptr, nx, ny,
                           nz, op->stream, op->banded() ? psi : nullptr, op->band));
@@ -1346,8 +1346,8 @@ mpdg_level_set_curvature_rhs(mpdg_op *op, const double *nx, const double *ny, co
     return e;
   if (!nx || !ny || !nz || !dst || !(normal_tolerance > 0.0))
     return fail(MPDG_ERR_ARG, "invalid argument to mpdg_level_set_curvature_rhs");
-  if (op->degree > 2)
-    return fail(MPDG_ERR_UNSUPPORTED, "the level-set right-hand sides support FE_Q degree 1..2");
+  if (op->degree > 3)
+    return fail(MPDG_ERR_UNSUPPORTED, "the level-set right-hand sides support FE_Q degree 1..3");
   MPDG_CUDA(vec_fill<double>(dst, 0.0, op->ndofs, op->stream));
   MPDG_CUDA(level_set_rhs(op->grid(), op->degree, op->h, 1, 0, normal_tolerance, nx, ny, nz, dst, nullptr, nullptr,
                           op->stream, op->banded() ? op->d_band_ls : nullptr, op->band));
@@ -1399,8 +1399,8 @@ mpdg_op_set_narrow_band(mpdg_op *op, const double *level_set, double threshold)
       op->band      = 0.0;
       return MPDG_OK;
     }
-  if (op->degree > 2)
-    return fail(MPDG_ERR_UNSUPPORTED, "the narrow band supports FE_Q degree 1..2");
+  if (op->degree > 3)
+    return fail(MPDG_ERR_UNSUPPORTED, "the narrow band supports FE_Q degree 1..3");
   if (op->d_k64 || op->d_mask || op->solid || heat_faces_active(op->fbc, 0) || heat_faces_active(op->fbc, 1))
     return fail(MPDG_ERR_UNSUPPORTED, "the narrow band takes a constant damping, Dirichlet faces only and no "
                                       "boundary-face terms or temperature-dependent material");

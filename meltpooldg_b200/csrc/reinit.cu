@@ -1,4 +1,4 @@
-// Conservative level-set reinitialisation operator (Olsson), FE_Q(1, 2).
+// Conservative level-set reinitialisation operator (Olsson), FE_Q(1..3).
 //
 // Reference: source/level_set/olsson_CG_operator.cpp, default configuration (no wetting boundary
 // faces, no interface penalty):
@@ -565,7 +565,7 @@ namespace mpdg
   {
     if (!(band > 0.0))
       band_ls = nullptr;
-    if (K < 1 || K > 2)
+    if (K < 1 || K > 3)
       return cudaErrorInvalidValue;
     const double *tab = level_set_tables(K);
     if (!tab)
@@ -578,8 +578,12 @@ namespace mpdg
       level_set_rhs_kernel<1><<<blocks, 128, 0, s>>>(g, tab, tab + n * n, tab + 2 * n * n, det, 1.0 / hlen[0],
                                                       1.0 / hlen[1], 1.0 / hlen[2], mode, normalized, tol, in0, in1,
                                                       in2, out0, out1, out2, band_ls, band);
-    else
+    else if (K == 2)
       level_set_rhs_kernel<2><<<blocks, 128, 0, s>>>(g, tab, tab + n * n, tab + 2 * n * n, det, 1.0 / hlen[0],
+                                                      1.0 / hlen[1], 1.0 / hlen[2], mode, normalized, tol, in0, in1,
+                                                      in2, out0, out1, out2, band_ls, band);
+    else
+      level_set_rhs_kernel<3><<<blocks, 128, 0, s>>>(g, tab, tab + n * n, tab + 2 * n * n, det, 1.0 / hlen[0],
                                                       1.0 / hlen[1], 1.0 / hlen[2], mode, normalized, tol, in0, in1,
                                                       in2, out0, out1, out2, band_ls, band);
     return cudaGetLastError();
@@ -593,6 +597,7 @@ namespace mpdg
       {
         case 1: return launch_reinit<1, T>(h, mode, s);
         case 2: return launch_reinit<2, T>(h, mode, s);
+        case 3: return launch_reinit<3, T>(h, mode, s);
         default: return cudaErrorInvalidValue;
       }
   }

@@ -10,7 +10,8 @@ from tests.gpu_util import meshes, rel_err, to_gpu
 
 pytestmark = pytest.mark.gpu
 
-CASES = [(1, (9, 7, 5), 0b000001), (2, (9, 8, 5), 0b010011), (2, (16, 16, 16), 0), (1, (17, 5, 3), 0)]
+CASES = [(1, (9, 7, 5), 0b000001), (2, (9, 8, 5), 0b010011), (2, (16, 16, 16), 0), (1, (17, 5, 3), 0),
+         (3, (5, 4, 3), 0b001100)]
 EPS_N, EPS_T, DT, TOL = 0.05, 0.01, 1e-2, 1e-3
 
 
@@ -85,7 +86,7 @@ def test_reinit_argument_checks():
     from meltpooldg_b200.operators import Mesh, OlssonOperator
 
     with pytest.raises(MpdgError) as e:
-        OlssonOperator(Mesh(3, (2, 2, 2)), dt=1e-2, eps_normal=0.1, eps_tangential=0.1)
+        OlssonOperator(Mesh(4, (2, 2, 2)), dt=1e-2, eps_normal=0.1, eps_tangential=0.1)
     assert e.value.code == MPDG_ERR_UNSUPPORTED
     g = OlssonOperator(Mesh(1, (4, 4, 4)), dt=1e-2, eps_normal=0.1, eps_tangential=0.1)
     x = torch.zeros(g.n_dofs, dtype=torch.float64, device="cuda")
@@ -97,7 +98,8 @@ def test_reinit_argument_checks():
     g.vmult(y, x)
 
 
-@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0), (2, (9, 8, 5), 0b010011), (2, (16, 16, 16), 0)])
+@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0), (2, (9, 8, 5), 0b010011), (2, (16, 16, 16), 0),
+                                            (3, (4, 5, 3), 0b000011)])
 def test_level_set_rhs_and_normal_projection(degree, m, faces):
     """The normal-vector and curvature right-hand sides against the oracle, and the normal projection
     (M + damping K) n_d = rhs_d solved with a heat operator (rho_cp = dt = 1, k = damping)."""
@@ -141,7 +143,7 @@ def test_level_set_rhs_and_normal_projection(degree, m, faces):
     assert rel_err(c.cpu().numpy(), c_ref) <= 1e-12
 
 
-@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0), (2, (8, 7, 6), 0b000011)])
+@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0), (2, (8, 7, 6), 0b000011), (3, (5, 4, 4), 0)])
 def test_narrow_band_projection_and_rhs(degree, m, faces):
     """Narrow band of the normal-vector / curvature projections (level_set_tools.hpp:357-368) on a
     heat handle used as the projection operator: vmult (FP64, FP32), the inverse diagonal with the
@@ -220,7 +222,7 @@ def test_narrow_band_projection_and_rhs(degree, m, faces):
 
 
 @pytest.mark.parametrize("degree,m,faces,wet", [(1, (6, 5, 4), 0, 0b000101), (2, (5, 4, 6), 0b100000, 0b011010),
-                                                (2, (7, 6, 5), 0, 0b111111)])
+                                                (2, (7, 6, 5), 0, 0b111111), (3, (4, 3, 4), 0, 0b010110)])
 def test_wetting_faces_match_oracle(degree, m, faces, wet):
     """Wetting boundary faces of the reinitialisation operator (olsson_CG_operator.cpp:550-716):
     vmult, create_rhs and the inverse diagonal with the face terms, against oracle/reinit.py."""

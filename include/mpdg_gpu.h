@@ -290,7 +290,7 @@ MPDG_API int     mpdg_op_distribute_inflow(mpdg_op *op, double *x);
 MPDG_API int mpdg_op_set_temperature(mpdg_op *op, const double *temperature);
 
 /* Temperature-dependent material of the heat operator, MaterialTypes::liquid_solid without latent
-   heat (include/meltpooldg/core/material.templates.hpp:296-360, :540-620, :748-765), FE_Q(1, 2):
+   heat (include/meltpooldg/core/material.templates.hpp:296-360, :540-620, :748-765), FE_Q(1..3):
    solid fraction f_s = clamp((T_liquidus - T) / (T_liquidus - T_solidus), 0, 1) (mushy zone) or
    T < T_solidus (sharp); rho, c_p and k blend cubically, v_l + (v_s - v_l)(3 f_s^2 - 2 f_s^3).
    With it vmult applies the solidification tangent (source/heat/heat_diffuse_operator.cpp:1029-1050)

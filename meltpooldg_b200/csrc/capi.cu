@@ -1251,8 +1251,8 @@ mpdg_op_set_solidification(mpdg_op *op, const mpdg_solid_liquid *mat)
       op->solid = false;
       return MPDG_OK;
     }
-  if (op->degree > 2)
-    return fail(MPDG_ERR_UNSUPPORTED, "temperature-dependent material supports FE_Q degree 1..2");
+  if (op->degree > 3)
+    return fail(MPDG_ERR_UNSUPPORTED, "temperature-dependent material supports FE_Q degree 1..3");
   if (!(mat->liquid_density > 0 && mat->liquid_specific_heat > 0 && mat->liquid_conductivity > 0 &&
         mat->solid_density > 0 && mat->solid_specific_heat > 0 && mat->solid_conductivity > 0) ||
       (!mat->sharp && !(mat->liquidus_temperature > mat->solidus_temperature)) || !(mat->latent_heat >= 0.0) ||

@@ -174,11 +174,12 @@ namespace mpdg
     template <int K, typename T>
     struct SolidLayout
     {
-      static constexpr int BX = 8, BY = 8, BZ = (K == 1 ? 8 : 4);
+      static constexpr int BX = 8, BY = 8, BZ = (K == 1 ? 8 : (K == 2 ? 4 : 2));
       static constexpr int NT = BX * BY * BZ;
       using BR                = Brick<K, BX, BY, BZ, NT>;
       static constexpr size_t bytes = sizeof(T) * 4 * (size_t)BR::NPTS; // u, T, T_old, accumulator
-      static constexpr int    MINB  = sizeof(T) == 8 ? MPDG_SOLID_MINB_F64 : MPDG_SOLID_MINB_F32; // CTAs per SM
+      // CTAs per SM (k = 3: 128-thread CTAs, 140 KB of staging in FP64, one per SM)
+      static constexpr int    MINB  = K == 3 ? 1 : (sizeof(T) == 8 ? MPDG_SOLID_MINB_F64 : MPDG_SOLID_MINB_F32);
     };
 
     // v = M v along direction D of an N^3 array (TR: M^T)
@@ -502,7 +503,7 @@ namespace mpdg
   {
     shape[0] = 8;
     shape[1] = 8;
-    shape[2] = K == 1 ? SolidLayout<1, T>::BZ : SolidLayout<2, T>::BZ;
+    shape[2] = K == 1 ? SolidLayout<1, T>::BZ : (K == 2 ? SolidLayout<2, T>::BZ : SolidLayout<3, T>::BZ);
   }
 
   template <typename T>
@@ -513,6 +514,7 @@ namespace mpdg
       {
         case 1: return solid_mode<1, T>(h, s);
         case 2: return solid_mode<2, T>(h, s);
+        case 3: return solid_mode<3, T>(h, s);
         default: return cudaErrorInvalidValue;
       }
   }
@@ -521,7 +523,7 @@ namespace mpdg
   heat_solid_diagonal(const GridDesc &g, int K, const SolidMaterial &mat, double dt, const double hlen[3],
                       const double *temp, const double *temp_old, double *diag, cudaStream_t s)
   {
-    if (K < 1 || K > 2)
+    if (K < 1 || K > 3)
       return cudaErrorInvalidValue;
     const Tables1D &t      = tables(K);
     const long long ncell  = (long long)g.m[0] * g.m[1] * g.m[2];
@@ -550,11 +552,17 @@ namespace mpdg
         fill(a, 2);
         heat_solid_diag_kernel<1, double><<<blocks, 128, 0, s>>>(a);
       }
-    else
+    else if (K == 2)
       {
         SolidDiagArgs<double, 3> a{};
         fill(a, 3);
         heat_solid_diag_kernel<2, double><<<blocks, 128, 0, s>>>(a);
+      }
+    else
+      {
+        SolidDiagArgs<double, 4> a{};
+        fill(a, 4);
+        heat_solid_diag_kernel<3, double><<<blocks, 128, 0, s>>>(a);
       }
     return cudaGetLastError();
   }

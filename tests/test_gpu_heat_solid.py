@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 LIQ, SOL, TL, TS = (7.4, 0.8, 30.0), (7.9, 0.6, 20.0), 1700.0, 1600.0
 CASES = [(1, (9, 7, 5), 0b000001, False, False), (2, (9, 8, 5), 0b010011, False, False),
          (2, (16, 16, 16), 0, False, False), (2, (6, 5, 7), 0b000001, True, False),
-         (1, (5, 6, 4), 0b100000, False, True), (2, (7, 4, 6), 0, False, True)]
+         (1, (5, 6, 4), 0b100000, False, True), (2, (7, 4, 6), 0, False, True),
+         (3, (5, 4, 3), 0b000101, False, False), (3, (4, 3, 5), 0b000001, True, True)]
 
 
 def setup(degree, m, faces, use_mask, sharp, dt=1e-3):
@@ -103,7 +104,7 @@ def test_solid_argument_checks():
     from meltpooldg_b200._lib import MPDG_ERR_ARG, MPDG_ERR_UNSUPPORTED, MpdgError
     from meltpooldg_b200.operators import HeatDiffuseOperator, Mesh
 
-    g = HeatDiffuseOperator(Mesh(3, (2, 2, 2)), dt=1e-3)
+    g = HeatDiffuseOperator(Mesh(4, (2, 2, 2)), dt=1e-3)
     with pytest.raises(MpdgError) as e:
         g.set_solidification(LIQ, SOL, TL, TS)
     assert e.value.code == MPDG_ERR_UNSUPPORTED
@@ -125,7 +126,7 @@ def test_solid_argument_checks():
     g.vmult(y, x)
 
 
-@pytest.mark.parametrize("degree,capacity", [(1, "qlq"), (2, "qlq"), (2, "poly4_bell"), (2, "constant")])
+@pytest.mark.parametrize("degree,capacity", [(1, "qlq"), (2, "qlq"), (2, "poly4_bell"), (2, "constant"), (3, "qlq")])
 def test_solid_latent_heat_matches_oracle(degree, capacity):
     """Latent heat of fusion as the reference's apparent capacity (material.templates.hpp:561-614):
     vmult, the residual part of create_rhs and the inverse diagonal against the oracle, with the

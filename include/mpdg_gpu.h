@@ -261,7 +261,12 @@ MPDG_API int mpdg_op_set_wetting(mpdg_op *op, uint32_t faces);
    reference (the caller keeps them alive and current) and read plainly per cell; they replace the
    affine velocity of mpdg_op_params in vmult, create_rhs, the inverse diagonal and the inflow
    detection of mpdg_op_set_inflow_outflow.  All NULL returns to the affine velocity.  Not with
-   SUPG. */
+   SUPG.  FE_Q degree 1..2.
+   On a heat operator the field is its convection velocity (HeatDiffuseOperator with velocity,
+   source/heat/heat_diffuse_operator.cpp:448-453, 499-500, 1038-1041): vmult adds
+   int rho c_p (v . grad u) phi, create_rhs subtracts int rho c_p (v . grad T) phi, and the inverse
+   diagonal includes the term (heat inversion rule); with a constant conductivity and material only
+   (no per-cell k, no temperature-dependent material, no narrow band). */
 MPDG_API int mpdg_op_set_velocity_field(mpdg_op *op, const double *vx, const double *vy, const double *vz);
 /* Inflow/outflow condition of the advection-diffusion operator
    (AdvectionDiffusionOperation::create_inflow_outflow_constraints,

@@ -243,6 +243,36 @@ namespace
     return p;
   }
 
+  // The heat tangent with a convection velocity (heat_diffuse_operator.cpp:1029-1044, velocity a DoF
+  // vector): rho c_p / dt u + rho c_p v . grad u tested with phi plus k grad u . grad phi, i.e. the
+  // advection-diffusion form with 1/dt -> rho c_p / dt, theta -> rho c_p, theta eps -> k (the
+  // velocity term alone for create_rhs: adv = -rho c_p, no mass, no diffusion).
+  // the lattice of a heat operator with the brick counts of the advection-form kernels
+  template <typename T>
+  GridDesc
+  heat_velocity_grid(const mpdg_op *op)
+  {
+    GridDesc g = op->grid<T>();
+    int      sh[3];
+    adv_brick_shape<T>(op->degree, sh);
+    for (int d = 0; d < 3; ++d)
+      g.nbr[d] = (op->m[d] + sh[d] - 1) / sh[d];
+    return g;
+  }
+
+  AdvParams
+  heat_velocity_params(const mpdg_op *op, bool rhs_term)
+  {
+    AdvParams p = adv_params(op, 0.0, false);
+    p.inv_dt    = rhs_term ? 0.0 : op->rho_cp / op->dt;
+    p.theta_adv = rhs_term ? -op->rho_cp : op->rho_cp;
+    p.theta_dif = rhs_term ? 0.0 : op->k;
+    for (int i = 0; i < 12; ++i)
+      p.vel[i] = 0.0;
+    p.supg = 0;
+    return p;
+  }
+
   template <typename T>
   ReinitLaunch<T>
   reinit_launch(const mpdg_op *op, double scale, const T *src, T *dst, int mask_src)
@@ -390,6 +420,22 @@ namespace
             if (int e = solid_apply<T>(op, mode, scale, dst, src, b, mask_src, skip, false))
               return e;
           }
+        else if (which == 0 && op->d_vfield[0])
+          {
+            AdvLaunch<T> a;
+            a.degree   = op->degree;
+            a.mode     = mode;
+            a.scale    = scale;
+            a.p        = heat_velocity_params(op, false);
+            a.grid     = heat_velocity_grid<T>(op);
+            a.sync     = op->sync();
+            a.src      = src;
+            a.dst      = dst;
+            a.b        = b;
+            a.mask_src = mask_src;
+            a.skip     = skip;
+            MPDG_CUDA(adv_apply<T>(a, op->stream));
+          }
         else
           MPDG_CUDA(heat_apply<T>(h, op->stream));
         if (which == 0 && op->tangent_faces())
@@ -526,6 +572,20 @@ namespace
         if (!std::is_same<T, double>::value)
           MPDG_CUDA(vec_convert<T, double>(diag, d64, op->ndofs, op->stream));
       }
+    else if (op->kind == MPDG_HEAT && op->d_vfield[0])
+      {
+        // with a convection velocity: the per-cell diagonal of the whole tangent in FP64, then the
+        // heat operator's inversion rule (|d| > 1e-10 ? 1/d : 1, constrained rows 1)
+        double *f64 = std::is_same<T, double>::value ? reinterpret_cast<double *>(diag) : op->vec<double>("vf_diag");
+        if (!f64)
+          return fail(MPDG_ERR_NOMEM, "diagonal work vector");
+        MPDG_CUDA(vec_fill<double>(f64, 0.0, op->ndofs, op->stream));
+        MPDG_CUDA(adv_field_diagonal(g, op->degree, heat_velocity_params(op, false), f64, op->stream));
+        MPDG_CUDA(vec_set_constrained<double>(f64, 1.0, g, op->stream));
+        MPDG_CUDA(vec_invert<double>(f64, 1.0e-10, op->ndofs, op->stream));
+        if (!std::is_same<T, double>::value)
+          MPDG_CUDA(vec_convert<T, double>(diag, f64, op->ndofs, op->stream));
+      }
     else if (op->kind == MPDG_HEAT)
       {
         MPDG_CUDA(heat_diagonal<T>(g, op->degree, heat_geom(op, op->rho_cp / op->dt), op->k, op->kcell<T>(), diag,
@@ -621,7 +681,7 @@ namespace
   fused_cg_applies(const mpdg_op *op)
   {
     return op->fused_cg && op->kind == MPDG_HEAT && op->degree == 2 && op->d_mask == nullptr && op->with_bc &&
-           !op->tangent_faces() && !op->solid && !op->banded();
+           !op->tangent_faces() && !op->solid && !op->banded() && !op->d_vfield[0];
   }
 
   // Preconditioned CG with one launch per iteration (cgfused.cu): the same iterates as cg_solve in
@@ -786,7 +846,7 @@ namespace
     // heat operators without a per-DoF mask fuse p^T A p into the apply and set alpha on the device
     // (not the narrow-band projection, whose apply is the point-wise kernel)
     const bool fused = op->kind == MPDG_HEAT && op->d_part != nullptr && !op->tangent_faces() && !op->solid &&
-                       !op->banded() && heat_apply_fuses_dot(op->degree, op->d_mask != nullptr, true);
+                       !op->banded() && !op->d_vfield[0] && heat_apply_fuses_dot(op->degree, op->d_mask != nullptr, true);
     DotSink    sink;
     sink.part  = op->d_part;
     sink.alpha = &op->d_cg->alpha;
@@ -1069,9 +1129,23 @@ mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op
     }
   op->ndofs             = n0 * n1 * n2;
   op->ncells            = (long long)op->m[0] * op->m[1] * op->m[2];
-  // brick flags and fused-dot partials serve the FP64 and the FP32 apply
-  const long long nbrk  = std::max((long long)op->nbr[0] * op->nbr[1] * op->nbr[2],
-                                   (long long)op->nbr32[0] * op->nbr32[1] * op->nbr32[2]);
+  // brick flags and fused-dot partials serve the FP64 and the FP32 apply (and, for a heat operator
+  // at k <= 3, the advection-form kernels of its convection velocity, on their own bricks)
+  long long nbrk = std::max((long long)op->nbr[0] * op->nbr[1] * op->nbr[2],
+                            (long long)op->nbr32[0] * op->nbr32[1] * op->nbr32[2]);
+  if (op->kind == MPDG_HEAT && op->degree <= 3)
+    for (int prec = 0; prec < 2; ++prec)
+      {
+        int sh[3];
+        if (prec == 0)
+          adv_brick_shape<double>(op->degree, sh);
+        else
+          adv_brick_shape<float>(op->degree, sh);
+        long long nb = 1;
+        for (int d = 0; d < 3; ++d)
+          nb *= (op->m[d] + sh[d] - 1) / sh[d];
+        nbrk = std::max(nbrk, nb);
+      }
   auto            clean = [&](int code, const std::string &msg) {
     mpdg_op_destroy(op);
     return fail(code, msg);
@@ -1200,6 +1274,8 @@ mpdg_op_set_conductivity(mpdg_op *op, const double *k_cells)
     return e;
   if (op->kind != MPDG_HEAT || !k_cells)
     return fail(MPDG_ERR_ARG, "conductivity applies to the heat operator");
+  if (op->d_vfield[0])
+    return fail(MPDG_ERR_UNSUPPORTED, "a per-cell conductivity with a convection velocity is not supported");
   if (!op->d_k64)
     {
       if (cudaMalloc(&op->d_k64, sizeof(double) * op->ncells) != cudaSuccess ||
@@ -1251,6 +1327,8 @@ mpdg_op_set_solidification(mpdg_op *op, const mpdg_solid_liquid *mat)
       op->solid = false;
       return MPDG_OK;
     }
+  if (op->d_vfield[0])
+    return fail(MPDG_ERR_UNSUPPORTED, "temperature-dependent material with a convection velocity is not supported");
   if (op->degree > 3)
     return fail(MPDG_ERR_UNSUPPORTED, "temperature-dependent material supports FE_Q degree 1..3");
   if (!(mat->liquid_density > 0 && mat->liquid_specific_heat > 0 && mat->liquid_conductivity > 0 &&
@@ -1359,10 +1437,13 @@ mpdg_op_set_velocity_field(mpdg_op *op, const double *vx, const double *vy, cons
 {
   if (int e = check_op(op))
     return e;
-  if (op->kind != MPDG_ADVDIFF)
-    return fail(MPDG_ERR_ARG, "a velocity field belongs to the advection-diffusion operator");
+  if (op->kind != MPDG_ADVDIFF && op->kind != MPDG_HEAT)
+    return fail(MPDG_ERR_ARG, "a velocity field belongs to the advection-diffusion or the heat operator");
   if ((vx || vy || vz) && !(vx && vy && vz))
     return fail(MPDG_ERR_ARG, "a velocity field needs all three components");
+  if (vx && op->kind == MPDG_HEAT && (op->d_k64 || op->solid || op->banded()))
+    return fail(MPDG_ERR_UNSUPPORTED, "the heat operator's convection velocity takes a constant conductivity and "
+                                      "material and no narrow band");
   if (vx && op->supg)
     return fail(MPDG_ERR_UNSUPPORTED, "SUPG with a DoF-vector velocity is not supported");
   if (vx && op->degree > 2)
@@ -1401,9 +1482,10 @@ mpdg_op_set_narrow_band(mpdg_op *op, const double *level_set, double threshold)
     }
   if (op->degree > 3)
     return fail(MPDG_ERR_UNSUPPORTED, "the narrow band supports FE_Q degree 1..3");
-  if (op->d_k64 || op->d_mask || op->solid || heat_faces_active(op->fbc, 0) || heat_faces_active(op->fbc, 1))
+  if (op->d_k64 || op->d_mask || op->solid || op->d_vfield[0] || heat_faces_active(op->fbc, 0) ||
+      heat_faces_active(op->fbc, 1))
     return fail(MPDG_ERR_UNSUPPORTED, "the narrow band takes a constant damping, Dirichlet faces only and no "
-                                      "boundary-face terms or temperature-dependent material");
+                                      "boundary-face terms, convection velocity or temperature-dependent material");
   op->d_band_ls = level_set;
   op->band      = threshold;
   return MPDG_OK;
@@ -1776,6 +1858,23 @@ mpdg_op_create_rhs(mpdg_op *op, double *dst, const double *a, const double *b, c
         return e;
       if (int e = apply<double>(op, (int)OutMode::Add, -1.0, dst, a, nullptr, 0, 2))
         return e;
+      if (op->d_vfield[0])
+        {
+          // dst -= int rho c_p (v . grad T) phi (heat_diffuse_operator.cpp:499-500), plain reads
+          AdvLaunch<double> h;
+          h.degree   = op->degree;
+          h.mode     = (int)OutMode::Add;
+          h.scale    = 1.0;
+          h.p        = heat_velocity_params(op, true);
+          h.grid     = heat_velocity_grid<double>(op);
+          h.sync     = op->sync();
+          h.src      = a;
+          h.dst      = dst;
+          h.b        = nullptr;
+          h.mask_src = 0;
+          h.skip     = nullptr;
+          MPDG_CUDA(adv_apply<double>(h, op->stream));
+        }
       if (heat_faces_active(op->fbc, 1))
         {
           HeatFaceLaunch<double> f;

@@ -260,6 +260,16 @@ class HeatDiffuseOperator(OperatorMatrixFree):
         self._temperature = temperature_device
         check(lib().mpdg_op_set_temperature(self._h, self._v(temperature_device)))
 
+    def set_velocity_field(self, vx, vy, vz) -> None:
+        """Convection velocity as a DoF vector (three device vectors on the lattice, kept by
+        reference), as the reference heat operator's velocity (heat_diffuse_operator.cpp:448-453,
+        1038-1041); constant conductivity and material only; None removes it."""
+        self._vfield = (vx, vy, vz)
+        if vx is None:
+            check(lib().mpdg_op_set_velocity_field(self._h, None, None, None))
+        else:
+            check(lib().mpdg_op_set_velocity_field(self._h, self._v(vx), self._v(vy), self._v(vz)))
+
 
 class AdvectionDiffusionOperator(OperatorMatrixFree):
     """M/dt + theta (v.grad + eps K) with an affine velocity v(x) = v0 + G x."""

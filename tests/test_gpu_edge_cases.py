@@ -88,7 +88,7 @@ def test_op_create_argument_checks():
 
     assert code(lambda: HeatDiffuseOperator(Mesh(5, (2, 2, 2)), dt=1e-2)) == L.MPDG_ERR_UNSUPPORTED
     assert code(lambda: HeatDiffuseOperator(Mesh(0, (2, 2, 2)), dt=1e-2)) == L.MPDG_ERR_UNSUPPORTED
-    assert code(lambda: AdvectionDiffusionOperator(Mesh(3, (2, 2, 2)), dt=1e-2)) == L.MPDG_ERR_UNSUPPORTED
+    assert code(lambda: AdvectionDiffusionOperator(Mesh(4, (2, 2, 2)), dt=1e-2)) == L.MPDG_ERR_UNSUPPORTED
     assert code(lambda: HeatDiffuseOperator(Mesh(2, (2, 0, 2)), dt=1e-2)) == L.MPDG_ERR_ARG
     assert code(lambda: HeatDiffuseOperator(Mesh(2, (2, 2, 2), length=(1, -1, 1)), dt=1e-2)) == L.MPDG_ERR_ARG
     assert code(lambda: HeatDiffuseOperator(Mesh(2, (2, 2, 2)), dt=0.0)) == L.MPDG_ERR_ZERO_DT

@@ -79,8 +79,8 @@ enum mpdg_precond_kind
 
 typedef struct mpdg_mesh_desc
 {
-  int32_t        degree;          /* FE_Q degree: heat 1..4, advection-diffusion 1..3 (SUPG and a
-                                     DoF-vector velocity 1..2), reinitialisation 1..3 */
+  int32_t        degree;          /* FE_Q degree: heat 1..4, advection-diffusion 1..3 (SUPG 1..2),
+                                     reinitialisation 1..3 */
   int32_t        cells[3];        /* cells per direction                                */
   double         origin[3];       /* lower corner of the box                            */
   double         length[3];       /* box edge lengths                                   */
@@ -261,7 +261,7 @@ MPDG_API int mpdg_op_set_wetting(mpdg_op *op, uint32_t faces);
    reference (the caller keeps them alive and current) and read plainly per cell; they replace the
    affine velocity of mpdg_op_params in vmult, create_rhs, the inverse diagonal and the inflow
    detection of mpdg_op_set_inflow_outflow.  All NULL returns to the affine velocity.  Not with
-   SUPG.  FE_Q degree 1..2.
+   SUPG.  FE_Q degree 1..3.
    On a heat operator the field is its convection velocity (HeatDiffuseOperator with velocity,
    source/heat/heat_diffuse_operator.cpp:448-453, 499-500, 1038-1041): vmult adds
    int rho c_p (v . grad u) phi, create_rhs subtracts int rho c_p (v . grad T) phi, and the inverse

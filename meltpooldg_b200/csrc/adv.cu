@@ -544,12 +544,14 @@ namespace mpdg
     const bool vdof = h.p.vfield[0] != nullptr;
     if (vdof && h.p.supg)
       return cudaErrorInvalidValue; // SUPG with a DoF-vector velocity is not built
-    // SUPG and the DoF-vector velocity keep a third cell array and are built for k <= 2 only
-    auto kern = adv_apply_kernel<K, T, MODE, false>;
+    // SUPG keeps a third cell array and is built for k <= 2 only
+    auto kern = vdof ? adv_apply_kernel<K, T, MODE, false, true> : adv_apply_kernel<K, T, MODE, false>;
     if constexpr (K <= 2)
-      kern = h.p.supg ? adv_apply_kernel<K, T, MODE, true>
-                      : (vdof ? adv_apply_kernel<K, T, MODE, false, true> : adv_apply_kernel<K, T, MODE, false>);
-    else if (h.p.supg || vdof)
+      {
+        if (h.p.supg)
+          kern = adv_apply_kernel<K, T, MODE, true>;
+      }
+    else if (h.p.supg)
       return cudaErrorInvalidValue;
     static std::atomic<unsigned long long> devices{0}, devices_supg{0}, devices_vdof{0};
     if (cudaError_t e = ensure_smem(kern, LAY::bytes, h.p.supg ? devices_supg : (vdof ? devices_vdof : devices));
@@ -909,7 +911,7 @@ namespace mpdg
   cudaError_t
   adv_field_diagonal(const GridDesc &g, int K, const AdvParams &p, double *diag, cudaStream_t s)
   {
-    if (K < 1 || K > 2 || !p.vfield[0] || !p.vfield[1] || !p.vfield[2])
+    if (K < 1 || K > ADV_KMAX || !p.vfield[0] || !p.vfield[1] || !p.vfield[2])
       return cudaErrorInvalidValue;
     AdvFieldDiagArgs a{};
     const Tables1D  &t = tables(K);
@@ -938,8 +940,10 @@ namespace mpdg
     const int       blocks = (int)std::max<long long>(1, std::min<long long>((ncell + 127) / 128, 148LL * 16));
     if (K == 1)
       adv_field_diag_kernel<1><<<blocks, 128, 0, s>>>(a);
-    else
+    else if (K == 2)
       adv_field_diag_kernel<2><<<blocks, 128, 0, s>>>(a);
+    else
+      adv_field_diag_kernel<3><<<blocks, 128, 0, s>>>(a);
     return cudaGetLastError();
   }
 

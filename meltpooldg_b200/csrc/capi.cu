@@ -1446,8 +1446,8 @@ mpdg_op_set_velocity_field(mpdg_op *op, const double *vx, const double *vy, cons
                                       "material and no narrow band");
   if (vx && op->supg)
     return fail(MPDG_ERR_UNSUPPORTED, "SUPG with a DoF-vector velocity is not supported");
-  if (vx && op->degree > 2)
-    return fail(MPDG_ERR_UNSUPPORTED, "a DoF-vector velocity is supported for FE_Q degree 1..2");
+  if (vx && op->degree > 3)
+    return fail(MPDG_ERR_UNSUPPORTED, "a DoF-vector velocity is supported for FE_Q degree 1..3");
   op->d_vfield[0] = vx;
   op->d_vfield[1] = vy;
   op->d_vfield[2] = vz;

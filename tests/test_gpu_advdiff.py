@@ -98,7 +98,8 @@ def test_gmres_solve(degree, m):
     assert rel_err(xd.cpu().numpy(), x_ref) <= 1e-8
 
 
-@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0), (2, (8, 9, 6), 0b010011), (2, (33, 5, 4), 0)])
+@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0), (2, (8, 9, 6), 0b010011), (2, (33, 5, 4), 0),
+                                            (3, (5, 4, 3), 0b000011)])
 def test_velocity_field_matches_oracle(degree, m, faces):
     """Advection velocity as a DoF vector (advection_diffusion_operator.cpp:461-466, 475-479): vmult
     (FP64, FP32), create_rhs, the inverse diagonal and a GMRES solve against oracle/advection_field.py,
@@ -151,16 +152,10 @@ def test_velocity_field_matches_oracle(degree, m, faces):
 
 
 def test_degree_three_limits():
-    """FE_Q(3) covers the plain advection-diffusion operator; SUPG and a DoF-vector velocity are k <= 2."""
-    import torch
-
+    """FE_Q(3) covers the advection-diffusion operator with affine or DoF-vector velocity; SUPG is k <= 2."""
     from meltpooldg_b200 import _lib as L
 
     o, g, om, cm = adv_pair(3, (4, 4, 4))
     with pytest.raises(L.MpdgError) as exc:
         g.set_convection_stabilization("SUPG", -1.0)
-    assert exc.value.code == L.MPDG_ERR_UNSUPPORTED
-    v = torch.zeros(om.ndofs, dtype=torch.float64, device="cuda")
-    with pytest.raises(L.MpdgError) as exc:
-        g.set_velocity_field(v, v, v)
     assert exc.value.code == L.MPDG_ERR_UNSUPPORTED

@@ -33,7 +33,8 @@ def velocity_term(om, cm, field, u, plain):
     return AF._form(om, cm, field, 0.0, RHO_CP, 0.0, u, plain=plain)
 
 
-@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0b111111), (2, (9, 8, 5), 0b010011), (2, (12, 10, 9), 0)])
+@pytest.mark.parametrize("degree,m,faces", [(1, (9, 7, 5), 0b111111), (2, (9, 8, 5), 0b010011), (2, (12, 10, 9), 0),
+                                            (3, (5, 4, 4), 0b000011)])
 def test_heat_velocity_vmult_rhs_diagonal(degree, m, faces):
     import torch
 

@@ -79,8 +79,8 @@ enum mpdg_precond_kind
 
 typedef struct mpdg_mesh_desc
 {
-  int32_t        degree;          /* FE_Q degree: heat 1..4, advection-diffusion 1..3 (SUPG 1..2),
-                                     reinitialisation 1..3 */
+  int32_t        degree;          /* FE_Q degree: heat 1..4, advection-diffusion 1..3, reinitialisation
+                                     1..3 */
   int32_t        cells[3];        /* cells per direction                                */
   double         origin[3];       /* lower corner of the box                            */
   double         length[3];       /* box edge lengths                                   */

@@ -544,15 +544,8 @@ namespace mpdg
     const bool vdof = h.p.vfield[0] != nullptr;
     if (vdof && h.p.supg)
       return cudaErrorInvalidValue; // SUPG with a DoF-vector velocity is not built
-    // SUPG keeps a third cell array and is built for k <= 2 only
-    auto kern = vdof ? adv_apply_kernel<K, T, MODE, false, true> : adv_apply_kernel<K, T, MODE, false>;
-    if constexpr (K <= 2)
-      {
-        if (h.p.supg)
-          kern = adv_apply_kernel<K, T, MODE, true>;
-      }
-    else if (h.p.supg)
-      return cudaErrorInvalidValue;
+    auto kern = h.p.supg ? adv_apply_kernel<K, T, MODE, true>
+                         : (vdof ? adv_apply_kernel<K, T, MODE, false, true> : adv_apply_kernel<K, T, MODE, false>);
     static std::atomic<unsigned long long> devices{0}, devices_supg{0}, devices_vdof{0};
     if (cudaError_t e = ensure_smem(kern, LAY::bytes, h.p.supg ? devices_supg : (vdof ? devices_vdof : devices));
         e != cudaSuccess)
@@ -809,7 +802,7 @@ namespace mpdg
   {
     if (!p.supg)
       return cudaSuccess;
-    if (K < 1 || K > 2)
+    if (K < 1 || K > ADV_KMAX)
       return cudaErrorInvalidValue;
     AdvSupgDiagArgs<T> a{};
     const Tables1D    &t = tables(K);
@@ -847,8 +840,10 @@ namespace mpdg
     const int       blocks = (int)std::max<long long>(1, std::min<long long>((ncell + 127) / 128, 148LL * 16));
     if (K == 1)
       adv_supg_diag_kernel<1, T><<<blocks, 128, 0, s>>>(a);
-    else
+    else if (K == 2)
       adv_supg_diag_kernel<2, T><<<blocks, 128, 0, s>>>(a);
+    else
+      adv_supg_diag_kernel<3, T><<<blocks, 128, 0, s>>>(a);
     return cudaGetLastError();
   }
 

@@ -1500,8 +1500,6 @@ mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient)
     return fail(MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator");
   if (enabled && op->d_vfield[0])
     return fail(MPDG_ERR_UNSUPPORTED, "SUPG with a DoF-vector velocity is not supported");
-  if (enabled && op->degree > 2)
-    return fail(MPDG_ERR_UNSUPPORTED, "SUPG is supported for FE_Q degree 1..2");
   op->supg      = enabled ? 1 : 0;
   op->supg_coef = coefficient;
   return MPDG_OK;

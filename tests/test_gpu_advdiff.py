@@ -149,13 +149,3 @@ def test_velocity_field_matches_oracle(degree, m, faces):
     gf.vmult(yf, to_gpu(u))
     assert rel_err(yf.cpu().numpy(), ya.cpu().numpy()) <= 1e-12
     assert om0.ndofs == om.ndofs and g.device_errors() == 0
-
-
-def test_degree_three_limits():
-    """FE_Q(3) covers the advection-diffusion operator with affine or DoF-vector velocity; SUPG is k <= 2."""
-    from meltpooldg_b200 import _lib as L
-
-    o, g, om, cm = adv_pair(3, (4, 4, 4))
-    with pytest.raises(L.MpdgError) as exc:
-        g.set_convection_stabilization("SUPG", -1.0)
-    assert exc.value.code == L.MPDG_ERR_UNSUPPORTED

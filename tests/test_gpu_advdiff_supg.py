@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 VEL = [0.1, 0.2, -0.3, 0.0, -1.0, 0.3, 1.0, 0.1, 0.0, 0.2, 0.1, -0.2]
 CASES = [(1, (9, 8, 9), 0b010011, 1.0, 1e-3, -1.0), (1, (17, 5, 3), 0, 0.5, 0.0, 0.3),
          (2, (9, 8, 5), 0b010011, 1.0, 1e-3, -1.0), (2, (16, 16, 16), 0b001001, 0.5, 2e-3, 0.25),
-         (2, (6, 7, 5), 0, 1.0, 1e-2, -1.0)]
+         (2, (6, 7, 5), 0, 1.0, 1e-2, -1.0), (3, (5, 4, 3), 0b000011, 1.0, 1e-3, -1.0)]
 
 
 def supg_pair(degree, m, faces, theta, eps, coef, dt=5e-3):

@@ -207,7 +207,8 @@ MPDG_API int mpdg_op_set_heat_bc(mpdg_op *op, const mpdg_heat_bc *bc);
    conv_stab, source/level_set/advection_diffusion_operator.cpp:455-533): vmult, create_rhs and the
    inverse diagonal add int tau_c (v.grad phi)(u/dt + theta v.grad u - theta eps lap u) (theta - 1 in
    create_rhs), tau_c = (coefficient < 0 ? 1 / max_q |v| (0 if below 1e-6) : coefficient) times the
-   cell diameter / sqrt(3).  enabled = 0 switches it off (ConvectionStabilizationType::none). */
+   cell diameter / sqrt(3), with the affine velocity or the DoF-vector field of
+   mpdg_op_set_velocity_field.  enabled = 0 switches it off (ConvectionStabilizationType::none). */
 MPDG_API int mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient);
 /* Reinitialisation operator (MPDG_REINIT; source/level_set/olsson_CG_operator.cpp, no wetting
    boundary faces, no interface penalty): normal and tangential diffusion lengths (the reference's
@@ -260,8 +261,8 @@ MPDG_API int mpdg_op_set_wetting(mpdg_op *op, uint32_t faces);
    DEVICE arrays of n_dofs, the components of an FE_Q(k) field on the operator's lattice, kept by
    reference (the caller keeps them alive and current) and read plainly per cell; they replace the
    affine velocity of mpdg_op_params in vmult, create_rhs, the inverse diagonal and the inflow
-   detection of mpdg_op_set_inflow_outflow.  All NULL returns to the affine velocity.  Not with
-   SUPG.  FE_Q degree 1..3.
+   detection of mpdg_op_set_inflow_outflow, and in the SUPG terms of mpdg_op_set_supg (tau_c's
+   max_q |v| included, :510-520).  All NULL returns to the affine velocity.  FE_Q degree 1..3.
    On a heat operator the field is its convection velocity (HeatDiffuseOperator with velocity,
    source/heat/heat_diffuse_operator.cpp:448-453, 499-500, 1038-1041): vmult adds
    int rho c_p (v . grad u) phi, create_rhs subtracts int rho c_p (v . grad T) phi, and the inverse

@@ -186,10 +186,11 @@ namespace mpdg
   }
 
   // SUPG, direction D of the strong residual: s += theta_adv v_d (D_d u_q) / h_d - theta_dif (D_d D_d u_q) / h_d^2
+  // (v_d from the affine field, or vq = v_d at the Gauss points of a DoF-vector field)
   template <typename T, int N, int D>
   __device__ __forceinline__ void
   supg_residual(const T *uq, T *sres, const T *tD, const T *tqp, T inv_h, T vd0, T gx, T gy, T gz, T th_adv,
-                T th_dif)
+                T th_dif, const T *vq = nullptr)
   {
     constexpr int S = D == 0 ? 1 : (D == 1 ? N : N * N);
 #pragma unroll
@@ -217,7 +218,7 @@ namespace mpdg
                 gg = fma(tD[r * N + k], g[k], gg);
               const int q  = base + r * S;
               const int qx = q % N, qy = (q / N) % N, qz = q / (N * N);
-              const T   vd = vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
+              const T   vd = vq ? vq[q] : vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
               sres[q] += th_adv * vd * g[r] * inv_h - th_dif * gg * inv_h * inv_h;
             }
         }
@@ -226,7 +227,8 @@ namespace mpdg
   // SUPG, direction D of the test with tau v.grad phi: R += D_d^T (c_t w3 v_d s), c_t = tau det / h_d
   template <typename T, int N, int D>
   __device__ __forceinline__ void
-  supg_test(const T *sres, T *R, const T *tD, const T *tqp, const T *tw3, T c_t, T vd0, T gx, T gy, T gz)
+  supg_test(const T *sres, T *R, const T *tD, const T *tqp, const T *tw3, T c_t, T vd0, T gx, T gy, T gz,
+            const T *vq = nullptr)
   {
     constexpr int S = D == 0 ? 1 : (D == 1 ? N : N * N);
 #pragma unroll
@@ -241,7 +243,7 @@ namespace mpdg
             {
               const int q  = base + r * S;
               const int qx = q % N, qy = (q / N) % N, qz = q / (N * N);
-              const T   vd = vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
+              const T   vd = vq ? vq[q] : vd0 + gx * tqp[qx] + gy * tqp[qy] + gz * tqp[qz];
               t[r]         = c_t * tw3[q] * vd * sres[q];
             }
 #pragma unroll
@@ -399,11 +401,68 @@ namespace mpdg
     else                                                                                                        \
       adv_direction<T, N, d>(uq, R, tD, a.pa[d], a.pb[d], a.pd[d], vd0, th_dif != T(0));                       \
   }
-          MPDG_ADV_DIR(0)
-          MPDG_ADV_DIR(1)
-          MPDG_ADV_DIR(2)
+          if constexpr (SUPG && VDOF)
+            {
+              // SUPG with a DoF-vector velocity: one component at the Gauss points at a time (four
+              // cell arrays live: u_q, R, the strong residual and the component).  Pass 1: the
+              // advection terms and |v|^2 at the points (kept in the residual's array) for tau_c
+              // (advection_diffusion_operator.cpp:510-520); pass 2: the strong residual; pass 3 its test
+              // with tau_c v.grad phi.
+              T sres[N * N * N], vq[N * N * N];
+#pragma unroll
+              for (int q = 0; q < N * N * N; ++q)
+                sres[q] = T(0);
+#pragma unroll
+              for (int d = 0; d < 3; ++d)
+                {
+                  field_at_points<T, N>(a.vfield[d], a.g, cx, cy, cz, tB, vq);
+                  if (d == 0)
+                    adv_direction<T, N, 0>(uq, R, tD, a.pa[0], a.pb[0], a.pd[0], T(0), th_dif != T(0), vq);
+                  else if (d == 1)
+                    adv_direction<T, N, 1>(uq, R, tD, a.pa[1], a.pb[1], a.pd[1], T(0), th_dif != T(0), vq);
+                  else
+                    adv_direction<T, N, 2>(uq, R, tD, a.pa[2], a.pb[2], a.pd[2], T(0), th_dif != T(0), vq);
+#pragma unroll
+                  for (int q = 0; q < N * N * N; ++q)
+                    sres[q] = fma(vq[q], vq[q], sres[q]);
+                }
+              T tau = a.supg_coef;
+              if (tau < T(0))
+                {
+                  T vmax = T(0);
+#pragma unroll
+                  for (int q = 0; q < N * N * N; ++q)
+                    vmax = fmax(vmax, sqrt(sres[q]));
+                  tau = vmax >= T(1e-6) ? T(1) / vmax : T(0);
+                }
+              tau *= a.cell_size;
+#pragma unroll
+              for (int q = 0; q < N * N * N; ++q)
+                sres[q] = a.inv_dt * uq[q];
+              const T ih[3] = {T(1) / a.h[0], T(1) / a.h[1], T(1) / a.h[2]};
+              const T z     = T(0);
+              field_at_points<T, N>(a.vfield[0], a.g, cx, cy, cz, tB, vq);
+              supg_residual<T, N, 0>(uq, sres, tD, tqp, ih[0], z, z, z, z, th_adv, th_dif, vq);
+              field_at_points<T, N>(a.vfield[1], a.g, cx, cy, cz, tB, vq);
+              supg_residual<T, N, 1>(uq, sres, tD, tqp, ih[1], z, z, z, z, th_adv, th_dif, vq);
+              field_at_points<T, N>(a.vfield[2], a.g, cx, cy, cz, tB, vq);
+              supg_residual<T, N, 2>(uq, sres, tD, tqp, ih[2], z, z, z, z, th_adv, th_dif, vq);
+              const T td = tau * a.det;
+              field_at_points<T, N>(a.vfield[0], a.g, cx, cy, cz, tB, vq);
+              supg_test<T, N, 0>(sres, R, tD, tqp, tw3, td * ih[0], z, z, z, z, vq);
+              field_at_points<T, N>(a.vfield[1], a.g, cx, cy, cz, tB, vq);
+              supg_test<T, N, 1>(sres, R, tD, tqp, tw3, td * ih[1], z, z, z, z, vq);
+              field_at_points<T, N>(a.vfield[2], a.g, cx, cy, cz, tB, vq);
+              supg_test<T, N, 2>(sres, R, tD, tqp, tw3, td * ih[2], z, z, z, z, vq);
+            }
+          else
+            {
+              MPDG_ADV_DIR(0)
+              MPDG_ADV_DIR(1)
+              MPDG_ADV_DIR(2)
+            }
 #undef MPDG_ADV_DIR
-          if constexpr (SUPG)
+          if constexpr (SUPG && !VDOF)
             {
               const T tau = supg_tau<T, N>(a.vel, a.h, tqp, x0, y0, z0, a.supg_coef, a.cell_size);
               T       sres[N * N * N];
@@ -542,12 +601,11 @@ namespace mpdg
             }
     }
     const bool vdof = h.p.vfield[0] != nullptr;
-    if (vdof && h.p.supg)
-      return cudaErrorInvalidValue; // SUPG with a DoF-vector velocity is not built
-    auto kern = h.p.supg ? adv_apply_kernel<K, T, MODE, true>
+    auto kern = h.p.supg ? (vdof ? adv_apply_kernel<K, T, MODE, true, true> : adv_apply_kernel<K, T, MODE, true>)
                          : (vdof ? adv_apply_kernel<K, T, MODE, false, true> : adv_apply_kernel<K, T, MODE, false>);
-    static std::atomic<unsigned long long> devices{0}, devices_supg{0}, devices_vdof{0};
-    if (cudaError_t e = ensure_smem(kern, LAY::bytes, h.p.supg ? devices_supg : (vdof ? devices_vdof : devices));
+    static std::atomic<unsigned long long> devices{0}, devices_supg{0}, devices_vdof{0}, devices_sv{0};
+    if (cudaError_t e = ensure_smem(kern, LAY::bytes,
+                                    h.p.supg ? (vdof ? devices_sv : devices_supg) : (vdof ? devices_vdof : devices));
         e != cudaSuccess)
       return e;
     const unsigned nbricks = (unsigned)h.grid.nbr[0] * h.grid.nbr[1] * h.grid.nbr[2];
@@ -745,21 +803,42 @@ namespace mpdg
     T        B[MAX_N * MAX_N], G[MAX_N * MAX_N], H[MAX_N * MAX_N], qp[MAX_N], qw[MAX_N];
     T        inv_dt, th_adv, th_dif, coef, cell_size, det;
     T        vel[12], origin[3], h[3];
+    const double *f[3]; // DoF-vector velocity (FIELD kernels)
     T       *diag;
   };
 
-  template <int K, typename T>
+  // FIELD: the velocity is a DoF vector, evaluated at the cell's Gauss points from its nodal values
+  template <int K, typename T, bool FIELD>
   __global__ void
   adv_supg_diag_kernel(const __grid_constant__ AdvSupgDiagArgs<T> a)
   {
-    constexpr int   N     = K + 1;
+    constexpr int   N     = K + 1, N3 = N * N * N;
     const int       m0    = a.g.m[0], m1 = a.g.m[1];
     const long long ncell = (long long)m0 * m1 * a.g.m[2];
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
       {
         const int cx = (int)(c % m0), cy = (int)((c / m0) % m1), cz = (int)(c / ((long long)m0 * m1));
         const T   x0 = a.origin[0] + a.h[0] * cx, y0 = a.origin[1] + a.h[1] * cy, z0 = a.origin[2] + a.h[2] * cz;
-        const T   tau = supg_tau<T, N>(a.vel, a.h, a.qp, x0, y0, z0, a.coef, a.cell_size);
+        T         vq[FIELD ? 3 : 1][FIELD ? N3 : 1];
+        T         tau;
+        if constexpr (FIELD)
+          {
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+              field_at_points<T, N>(a.f[d], a.g, cx, cy, cz, a.B, vq[d]);
+            tau = a.coef;
+            if (tau < T(0))
+              {
+                T vmax = T(0);
+#pragma unroll
+                for (int q = 0; q < N3; ++q)
+                  vmax = fmax(vmax, sqrt(vq[0][q] * vq[0][q] + vq[1][q] * vq[1][q] + vq[2][q] * vq[2][q]));
+                tau = vmax >= T(1e-6) ? T(1) / vmax : T(0);
+              }
+            tau *= a.cell_size;
+          }
+        else
+          tau = supg_tau<T, N>(a.vel, a.h, a.qp, x0, y0, z0, a.coef, a.cell_size);
         if (tau == T(0))
           continue;
         const T ih[3] = {T(1) / a.h[0], T(1) / a.h[1], T(1) / a.h[2]};
@@ -788,7 +867,14 @@ namespace mpdg
                         T       vg = T(0);
 #pragma unroll
                         for (int d = 0; d < 3; ++d)
-                          vg += (a.vel[d] + a.vel[3 + 3 * d] * x + a.vel[4 + 3 * d] * y + a.vel[5 + 3 * d] * z) * dp[d];
+                          {
+                            T vd;
+                            if constexpr (FIELD)
+                              vd = vq[d][(qz * N + qy) * N + qx];
+                            else
+                              vd = a.vel[d] + a.vel[3 + 3 * d] * x + a.vel[4 + 3 * d] * y + a.vel[5 + 3 * d] * z;
+                            vg += vd * dp[d];
+                          }
                         sum += a.qw[qx] * a.qw[qy] * a.qw[qz] * vg * (a.inv_dt * phi + a.th_adv * vg - a.th_dif * lap);
                       }
                 atomicAdd(a.diag + idx, tau * a.det * sum);
@@ -836,14 +922,17 @@ namespace mpdg
         a.h[d]      = (T)p.h[d];
       }
     a.diag                 = diag;
+    for (int d = 0; d < 3; ++d)
+      a.f[d] = p.vfield[d];
+    const bool      field  = p.vfield[0] != nullptr;
     const long long ncell  = (long long)g.m[0] * g.m[1] * g.m[2];
     const int       blocks = (int)std::max<long long>(1, std::min<long long>((ncell + 127) / 128, 148LL * 16));
     if (K == 1)
-      adv_supg_diag_kernel<1, T><<<blocks, 128, 0, s>>>(a);
+      (field ? adv_supg_diag_kernel<1, T, true> : adv_supg_diag_kernel<1, T, false>)<<<blocks, 128, 0, s>>>(a);
     else if (K == 2)
-      adv_supg_diag_kernel<2, T><<<blocks, 128, 0, s>>>(a);
+      (field ? adv_supg_diag_kernel<2, T, true> : adv_supg_diag_kernel<2, T, false>)<<<blocks, 128, 0, s>>>(a);
     else
-      adv_supg_diag_kernel<3, T><<<blocks, 128, 0, s>>>(a);
+      (field ? adv_supg_diag_kernel<3, T, true> : adv_supg_diag_kernel<3, T, false>)<<<blocks, 128, 0, s>>>(a);
     return cudaGetLastError();
   }
 

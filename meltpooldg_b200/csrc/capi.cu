@@ -619,6 +619,7 @@ namespace
               return fail(MPDG_ERR_NOMEM, "diagonal work vector");
             MPDG_CUDA(vec_fill<double>(f64, 0.0, op->ndofs, op->stream));
             MPDG_CUDA(adv_field_diagonal(g, op->degree, adv_params(op, 0, false), f64, op->stream));
+            MPDG_CUDA(adv_supg_diagonal<double>(g, op->degree, adv_params(op, 0, false), f64, op->stream));
             MPDG_CUDA(vec_set_constrained<double>(f64, 1.0, g, op->stream));
             MPDG_CUDA(vec_absmax<double>(f64, op->ndofs, op->d_scal, op->reducer(), op->stream));
             MPDG_CUDA(vec_invert_rel<double>(f64, op->d_scal, op->ndofs, op->stream));
@@ -1444,8 +1445,6 @@ mpdg_op_set_velocity_field(mpdg_op *op, const double *vx, const double *vy, cons
   if (vx && op->kind == MPDG_HEAT && (op->d_k64 || op->solid || op->banded()))
     return fail(MPDG_ERR_UNSUPPORTED, "the heat operator's convection velocity takes a constant conductivity and "
                                       "material and no narrow band");
-  if (vx && op->supg)
-    return fail(MPDG_ERR_UNSUPPORTED, "SUPG with a DoF-vector velocity is not supported");
   if (vx && op->degree > 3)
     return fail(MPDG_ERR_UNSUPPORTED, "a DoF-vector velocity is supported for FE_Q degree 1..3");
   op->d_vfield[0] = vx;
@@ -1498,8 +1497,6 @@ mpdg_op_set_supg(mpdg_op *op, int enabled, double coefficient)
     return e;
   if (op->kind != MPDG_ADVDIFF)
     return fail(MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator");
-  if (enabled && op->d_vfield[0])
-    return fail(MPDG_ERR_UNSUPPORTED, "SUPG with a DoF-vector velocity is not supported");
   op->supg      = enabled ? 1 : 0;
   op->supg_coef = coefficient;
   return MPDG_OK;

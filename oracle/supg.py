@@ -12,6 +12,11 @@ Restates source/level_set/advection_diffusion_operator.cpp for ConvectionStabili
   (source/core/scratch_data.cpp:262-277).
 Per cell with QGauss(k+1); the second derivatives of the 1-D basis come from differentiating the
 Lagrange polynomials on the Gauss-Lobatto nodes twice.  Vectorised over all cells with numpy.
+
+The velocity is the affine field vel (12 coefficients, v = vel[0:3] + G x) or, when `field` is
+given, a DoF vector: three FE_Q(k) components on the lattice read plainly per cell and evaluated at
+the Gauss points (the reference's advection_velocity, advection_diffusion_operator.cpp:461-466,
+:475-479), which also gives tau_c's max_q |v| (:510-520).
 """
 from __future__ import annotations
 
@@ -59,23 +64,31 @@ def _velocity(mesh: Mesh, vel, cx, cy, cz, qp):
     return [vel[d] + vel[3 + 3 * d] * X + vel[4 + 3 * d] * Y + vel[5 + 3 * d] * Z for d in range(3)]
 
 
-def supg_tau(mesh: Mesh, vel: Sequence[float], coefficient: float) -> np.ndarray:
+def _qvel(mesh: Mesh, vel, field, cx, cy, cz):
+    """The velocity at the Gauss points of every cell, (cells, qz, qy, qx) per component."""
+    qp, _, B, _, _ = tables(mesh.degree)
+    if field is None:
+        return _velocity(mesh, vel, cx, cy, cz, qp)
+    idx = _dof_index(mesh, cx, cy, cz)
+    return [np.einsum("al,bj,ci,xlji->xabc", B, B, B, np.asarray(c, dtype=np.float64)[idx]) for c in field]
+
+
+def supg_tau(mesh: Mesh, vel: Sequence[float], coefficient: float, field=None) -> np.ndarray:
     h = [mesh.length[d] / mesh.m[d] for d in range(3)]
     size = np.sqrt(sum(x * x for x in h)) / np.sqrt(3.0)
     cx, cy, cz = _cells(mesh)
     if coefficient >= 0:
         return np.full(cx.size, coefficient * size)
-    qp = tables(mesh.degree)[0]
-    v = _velocity(mesh, vel, cx, cy, cz, qp)
+    v = _qvel(mesh, vel, field, cx, cy, cz)
     vmax = np.sqrt(v[0] ** 2 + v[1] ** 2 + v[2] ** 2).reshape(cx.size, -1).max(axis=1)
     tau = np.where(vmax >= 1e-6, 1.0 / np.where(vmax > 0, vmax, 1.0), 0.0)
     return tau * size
 
 
 def supg_apply(mesh: Mesh, cmask: Optional[np.ndarray], vel, coefficient: float, inv_dt: float, th_adv: float,
-               th_dif: float, u: np.ndarray, plain: bool = False) -> np.ndarray:
+               th_dif: float, u: np.ndarray, plain: bool = False, field=None) -> np.ndarray:
     """sum_c tau_c int (v.grad phi_i)(u/dt + th_adv v.grad u - th_dif lap u) over the free rows;
-    u read with Dirichlet entries as 0 unless plain."""
+    u read with Dirichlet entries as 0 unless plain; v the affine vel or the DoF-vector field."""
     qp, qw, B, G, H = tables(mesh.degree)
     h = [mesh.length[d] / mesh.m[d] for d in range(3)]
     det = h[0] * h[1] * h[2]
@@ -88,10 +101,10 @@ def supg_apply(mesh: Mesh, cmask: Optional[np.ndarray], vel, coefficient: float,
     uq = ev(B, B, B, uc)
     g = [ev(B, B, G, uc) / h[0], ev(B, G, B, uc) / h[1], ev(G, B, B, uc) / h[2]]
     lap = ev(B, B, H, uc) / h[0] ** 2 + ev(B, H, B, uc) / h[1] ** 2 + ev(H, B, B, uc) / h[2] ** 2
-    v = _velocity(mesh, vel, cx, cy, cz, qp)
+    v = _qvel(mesh, vel, field, cx, cy, cz)
     s = inv_dt * uq + th_adv * (v[0] * g[0] + v[1] * g[1] + v[2] * g[2]) - th_dif * lap
     W = det * np.einsum("a,b,c->abc", qw, qw, qw)
-    tau = supg_tau(mesh, vel, coefficient)[:, None, None, None]
+    tau = supg_tau(mesh, vel, coefficient, field)[:, None, None, None]
     f = [tau * W[None] * v[d] * s for d in range(3)]
     te = lambda Z, Y, X, F: np.einsum("al,bj,ci,xabc->xlji", Z, Y, X, F)  # noqa: E731
     loc = te(B, B, G, f[0]) / h[0] + te(B, G, B, f[1]) / h[1] + te(G, B, B, f[2]) / h[2]
@@ -102,7 +115,7 @@ def supg_apply(mesh: Mesh, cmask: Optional[np.ndarray], vel, coefficient: float,
 
 
 def supg_diagonal(mesh: Mesh, cmask: Optional[np.ndarray], vel, coefficient: float, inv_dt: float,
-                  th_adv: float, th_dif: float) -> np.ndarray:
+                  th_adv: float, th_dif: float, field=None) -> np.ndarray:
     """Diagonal of supg_apply's operator (0 on constrained rows)."""
     qp, qw, B, G, H = tables(mesh.degree)
     h = [mesh.length[d] / mesh.m[d] for d in range(3)]
@@ -114,10 +127,10 @@ def supg_diagonal(mesh: Mesh, cmask: Optional[np.ndarray], vel, coefficient: flo
     phi = o(B, B, B)
     dphi = [o(B, B, G) / h[0], o(B, G, B) / h[1], o(G, B, B) / h[2]]
     lap = o(B, B, H) / h[0] ** 2 + o(B, H, B) / h[1] ** 2 + o(H, B, B) / h[2] ** 2
-    v = _velocity(mesh, vel, cx, cy, cz, qp)  # (cells, a, b, c)
+    v = _qvel(mesh, vel, field, cx, cy, cz)  # (cells, a, b, c)
     vg = sum(v[d][..., None, None, None] * dphi[d][None] for d in range(3))  # (cells, abc, lji)
     W = det * np.einsum("a,b,c->abc", qw, qw, qw)[None, :, :, :, None, None, None]
-    tau = supg_tau(mesh, vel, coefficient)[:, None, None, None]
+    tau = supg_tau(mesh, vel, coefficient, field)[:, None, None, None]
     loc = tau * np.sum(W * vg * (inv_dt * phi[None] + th_adv * vg - th_dif * lap[None]), axis=(1, 2, 3))
     out = np.zeros(mesh.ndofs)
     keep = free[idx]

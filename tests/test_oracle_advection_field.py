@@ -37,3 +37,40 @@ def test_nonaffine_field_diagonal_by_unit_vectors():
     e = np.array([AF.tangent_apply(mesh, None, field, 1e-2, 1.0, 1e-3, np.eye(1, mesh.ndofs, i).ravel())[i]
                   for i in range(mesh.ndofs)])
     assert np.max(np.abs(d - e)) <= 1e-12 * np.max(np.abs(e))
+
+
+@pytest.mark.parametrize("degree,m,coef", [(1, (4, 3, 3), -1.0), (2, (3, 4, 2), -1.0), (2, (3, 2, 3), 0.7),
+                                           (3, (2, 2, 2), -1.0)])
+def test_affine_field_reproduces_the_affine_supg_terms(degree, m, coef):
+    """oracle/supg.py with the velocity as a DoF vector: an affine field sampled at the support points
+    gives the affine form's tau, SUPG apply, rhs and diagonal."""
+    from oracle import supg as S
+
+    mesh = Mesh(degree, m, origin=(0.1, -0.2, 0.3), length=(1.0, 0.7, 1.2))
+    cm = mesh.face_mask(0b100110)
+    vel = [0.3, -0.2, 0.1, 0.5, -1.0, 0.2, 1.0, 0.1, -0.3, 0.05, 0.2, -0.4]
+    X, Y, Z = mesh.coords()
+    field = [vel[d] + vel[3 + 3 * d] * X + vel[4 + 3 * d] * Y + vel[5 + 3 * d] * Z for d in range(3)]
+    u = uniform_dofs(mesh, seed=2)
+    tol = lambda r: 1e-12 * np.max(np.abs(r))  # noqa: E731
+    t0, t1 = S.supg_tau(mesh, vel, coef), S.supg_tau(mesh, None, coef, field=field)
+    assert np.max(np.abs(t1 - t0)) <= tol(t0)
+    for plain in (False, True):
+        r0 = S.supg_apply(mesh, cm, vel, coef, 50.0, 0.5, 1e-3, u, plain=plain)
+        r1 = S.supg_apply(mesh, cm, None, coef, 50.0, 0.5, 1e-3, u, plain=plain, field=field)
+        assert np.max(np.abs(r1 - r0)) <= tol(r0)
+    d0 = S.supg_diagonal(mesh, cm, vel, coef, 50.0, 0.5, 1e-3)
+    d1 = S.supg_diagonal(mesh, cm, None, coef, 50.0, 0.5, 1e-3, field=field)
+    assert np.max(np.abs(d1 - d0)) <= tol(d0)
+
+
+def test_nonaffine_field_supg_diagonal_by_unit_vectors():
+    from oracle import supg as S
+
+    mesh = Mesh(2, (3, 2, 2))
+    X, Y, Z = mesh.coords()
+    field = [np.sin(3 * Y) * Z + 0.4, np.cos(2 * X) - Z * Z, X * Y - 0.3]
+    d = S.supg_diagonal(mesh, None, None, -1.0, 50.0, 1.0, 1e-3, field=field)
+    e = np.array([S.supg_apply(mesh, None, None, -1.0, 50.0, 1.0, 1e-3, np.eye(1, mesh.ndofs, i).ravel(),
+                               field=field)[i] for i in range(mesh.ndofs)])
+    assert np.max(np.abs(d - e)) <= 1e-12 * np.max(np.abs(e))

@@ -118,6 +118,9 @@ namespace mpdg
       }
     if ((e = cudaMemcpyToSymbol(c_adj_tab, h, sizeof(h))) != cudaSuccess)
       return e;
+    // the copy ran on the legacy stream: complete it before kernels on other streams read the table
+    if ((e = cudaStreamSynchronize(cudaStreamLegacy)) != cudaSuccess)
+      return e;
     done.insert(dev);
     return cudaSuccess;
   }

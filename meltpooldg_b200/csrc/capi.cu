@@ -659,6 +659,16 @@ namespace
     return MPDG_OK;
   }
 
+  // Copies between the operator's device data and the host, ordered on the operator's stream (which
+  // may be a non-blocking stream: a plain cudaMemcpy on the legacy stream would not wait for its work)
+  int
+  stream_copy(const mpdg_op *op, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind)
+  {
+    MPDG_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, op->stream));
+    MPDG_CUDA(cudaStreamSynchronize(op->stream));
+    return MPDG_OK;
+  }
+
   // Iterations to enqueue before the next convergence check of the CG loop.  The residual reduction
   // rate of the previous batch, extrapolated to the tolerance, bounds it from above, so that few of
   // the enqueued iterations run after convergence (each costs its launches, which return at once);
@@ -796,12 +806,14 @@ namespace
         if (info->history && info->history_capacity > 0)
           {
             const int cnt = std::min(info->history_capacity, fin.it + 1);
-            MPDG_CUDA(cudaMemcpy(info->history, hist, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            if (int e = stream_copy(op, info->history, hist, sizeof(double) * cnt, cudaMemcpyDeviceToHost))
+              return e;
           }
       }
     MPDG_CUDA(cudaStreamSynchronize(op->stream));
     int dev_err = 0;
-    MPDG_CUDA(cudaMemcpy(&dev_err, op->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (int e = stream_copy(op, &dev_err, op->d_err, sizeof(int), cudaMemcpyDeviceToHost))
+      return e;
     if (dev_err)
       return fail(MPDG_ERR_TIMEOUT, "a bounded device wait gave up during the CG solve");
     if (fin.done != 1)
@@ -885,11 +897,13 @@ namespace
         if (info->history && info->history_capacity > 0)
           {
             const int cnt = std::min(info->history_capacity, f.it + 1);
-            MPDG_CUDA(cudaMemcpy(info->history, hist, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            if (int e = stream_copy(op, info->history, hist, sizeof(double) * cnt, cudaMemcpyDeviceToHost))
+              return e;
           }
       }
     int dev_err = 0;
-    MPDG_CUDA(cudaMemcpy(&dev_err, op->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (int e = stream_copy(op, &dev_err, op->d_err, sizeof(int), cudaMemcpyDeviceToHost))
+      return e;
     if (dev_err)
       return fail(MPDG_ERR_TIMEOUT, "a bounded device wait gave up during the CG solve");
     if (f.done != 1)
@@ -1186,6 +1200,9 @@ mpdg_op_create(const mpdg_mesh_desc *mesh, const mpdg_op_params *params, mpdg_op
         return clean(MPDG_ERR_CUDA, "conductivity copy");
     }
   (void)tables(op->degree); // build the 1-D tables once
+  // the set-up above ran on the legacy stream; the operator's stream may not wait for it
+  if (cudaDeviceSynchronize() != cudaSuccess)
+    return clean(MPDG_ERR_CUDA, "set-up synchronisation in mpdg_op_create");
   *out = op;
   return MPDG_OK;
 }
@@ -1349,7 +1366,7 @@ mpdg_op_set_solidification(mpdg_op *op, const mpdg_solid_liquid *mat)
       MPDG_CUDA(cudaStreamSynchronize(op->stream));
       if (cudaMalloc(&fresh, sizeof(unsigned) * (3 + nb)) != cudaSuccess)
         return fail(MPDG_ERR_NOMEM, "brick flags");
-      MPDG_CUDA(cudaMemset(fresh, 0, sizeof(unsigned) * (3 + nb)));
+      MPDG_CUDA(cudaMemsetAsync(fresh, 0, sizeof(unsigned) * (3 + nb), op->stream));
       MPDG_CUDA(cudaFree(op->d_sync));
       op->d_sync   = fresh;
       op->sync_cap = nb;
@@ -1541,7 +1558,8 @@ mpdg_op_set_inflow_outflow(mpdg_op *op, uint32_t faces, const double *values)
   if (op->d_mask)
     {
       dmask.resize(op->ndofs);
-      MPDG_CUDA(cudaMemcpy(dmask.data(), op->d_mask, op->ndofs, cudaMemcpyDeviceToHost));
+      if (int e = stream_copy(op, dmask.data(), op->d_mask, op->ndofs, cudaMemcpyDeviceToHost))
+        return e;
     }
   // a DoF-vector velocity is evaluated at the support points: its nodal values there
   std::vector<double> vf[3];
@@ -1549,7 +1567,8 @@ mpdg_op_set_inflow_outflow(mpdg_op *op, uint32_t faces, const double *values)
     for (int d = 0; d < 3; ++d)
       {
         vf[d].resize(op->ndofs);
-        MPDG_CUDA(cudaMemcpy(vf[d].data(), op->d_vfield[d], sizeof(double) * op->ndofs, cudaMemcpyDeviceToHost));
+        if (int e = stream_copy(op, vf[d].data(), op->d_vfield[d], sizeof(double) * op->ndofs, cudaMemcpyDeviceToHost))
+          return e;
       }
   std::vector<uint8_t>   flag(op->ndofs, 0);
   std::vector<long long> idx;
@@ -1590,10 +1609,12 @@ mpdg_op_set_inflow_outflow(mpdg_op *op, uint32_t faces, const double *values)
       cudaMalloc(&op->d_in_idx, sizeof(long long) * std::max<size_t>(1, idx.size())) != cudaSuccess ||
       cudaMalloc(&op->d_in_val, sizeof(double) * std::max<size_t>(1, idx.size())) != cudaSuccess)
     return fail(MPDG_ERR_NOMEM, "inflow/outflow constraint storage");
-  MPDG_CUDA(cudaMemcpy(op->d_mask_io, flag.data(), op->ndofs, cudaMemcpyHostToDevice));
+  if (int e = stream_copy(op, op->d_mask_io, flag.data(), op->ndofs, cudaMemcpyHostToDevice))
+    return e;
   if (!idx.empty())
     {
-      MPDG_CUDA(cudaMemcpy(op->d_in_idx, idx.data(), sizeof(long long) * idx.size(), cudaMemcpyHostToDevice));
+      if (int e = stream_copy(op, op->d_in_idx, idx.data(), sizeof(long long) * idx.size(), cudaMemcpyHostToDevice))
+        return e;
       MPDG_CUDA(idx_gather(op->d_in_val, values, op->d_in_idx, op->n_inflow, op->stream));
       MPDG_CUDA(cudaStreamSynchronize(op->stream));
     }
@@ -1925,7 +1946,8 @@ mpdg_solve_mixed(mpdg_op *op, double *x, const double *b, const mpdg_mixed_param
   MPDG_CUDA(vec_multidot<double>(&bb, &bb, 1, n, op->d_scal, op->reducer(), op->stream));
   // a zero initial guess (max |x| == 0) makes the first outer residual b itself
   MPDG_CUDA(vec_absmax<double>(x, n, op->d_scal + 1, op->reducer(), op->stream));
-  MPDG_CUDA(cudaMemcpy(op->h_scal, op->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (int e = stream_copy(op, op->h_scal, op->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost))
+    return e;
   const double bnorm  = std::sqrt(op->h_scal[0]);
   const bool   x_zero = op->h_scal[1] == 0.0;
   const double tol   = prm->outer_rel_tol * bnorm;
@@ -2358,9 +2380,10 @@ mpdg_op_device_errors(mpdg_op *op)
   if (!op)
     return -1;
   int v = 0;
-  if (cudaMemcpy(&v, op->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (cudaMemcpyAsync(&v, op->d_err, sizeof(int), cudaMemcpyDeviceToHost, op->stream) != cudaSuccess ||
+      cudaStreamSynchronize(op->stream) != cudaSuccess)
     return -1;
-  cudaMemset(op->d_err, 0, sizeof(int));
+  cudaMemsetAsync(op->d_err, 0, sizeof(int), op->stream);
   return v;
 }
 

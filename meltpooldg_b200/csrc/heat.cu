@@ -564,6 +564,9 @@ namespace mpdg
       return e;
     if ((e = cudaMemcpyToSymbol(c_fd_f, hf, sizeof(hf))) != cudaSuccess)
       return e;
+    // the copies ran on the legacy stream: complete them before kernels on other streams read the tables
+    if ((e = cudaStreamSynchronize(cudaStreamLegacy)) != cudaSuccess)
+      return e;
     done.insert(dev);
     return cudaSuccess;
   }

@@ -550,7 +550,9 @@ namespace mpdg
           for (int q = 0; q < n; ++q)
             h[2 * n * n + q] = t.qw[q];
           double *p = nullptr;
-          if (cudaMalloc(&p, sizeof(h)) != cudaSuccess || cudaMemcpy(p, h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess)
+          // a legacy-stream copy, completed before kernels on other streams read the table
+          if (cudaMalloc(&p, sizeof(h)) != cudaSuccess || cudaMemcpy(p, h, sizeof(h), cudaMemcpyHostToDevice) != cudaSuccess ||
+              cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess)
             return nullptr;
           dev[d][K] = p;
         }

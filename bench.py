@@ -349,11 +349,12 @@ def run_reference(args):
 
 
 SOLVE_TOL = 5e-10  # relative residual that keeps the solution error at or below 1e-8 on this problem
+INNER_TOL = 1e-5  # FP32 inner CG reduction per outer step (two outer steps reach SOLVE_TOL)
 
 
 def run_solves(torch, stream, repeats=5):
     """Jacobi-CG on the 128^3 FE_Q(2) problem (dt 1e-3, k = exp(N(0,0.5^2)) seed 3, b = U[-1,1] seed 3):
-    the plain FP64 solve against the FP32-inner / FP64-outer defect correction (inner CG to 1e-4).
+    the plain FP64 solve against the FP32-inner / FP64-outer defect correction (inner CG to INNER_TOL).
     Both arms stop at the relative residual SOLVE_TOL, which keeps their error against a 1e-12 FP64
     solution at or below 1e-8 (a residual of 1e-8 bounds the error only up to the condition number,
     about 15 here); each arm is timed `repeats` times (median, min, max).  One run of each at the
@@ -368,7 +369,7 @@ def run_solves(torch, stream, repeats=5):
     op = HeatDiffuseOperator(mesh, rho_cp=1.0, dt=1e-3, conductivity_cells=kc, stream=stream.cuda_stream)
     bd = torch.tensor(b, device="cuda")
     out = {"workload": "heat_cg_q2_128cube", "dofs": mesh.ndofs, "tol": SOLVE_TOL, "repeats": repeats,
-           "inner_rel_tol": 1e-4}
+           "inner_rel_tol": INNER_TOL}
 
     def one(mode, tol):
         x = torch.zeros_like(bd)
@@ -379,7 +380,7 @@ def run_solves(torch, stream, repeats=5):
             st = LinearSolver.solve(op, x, bd, LinearSolverData("CG", "Diagonal", rel_tolerance=tol))
             its, outer = st.iterations, None
         else:
-            st = LinearSolver.solve_mixed(op, x, bd, outer_rel_tol=tol, inner_rel_tol=1e-4,
+            st = LinearSolver.solve_mixed(op, x, bd, outer_rel_tol=tol, inner_rel_tol=INNER_TOL,
                                           inexact_last=(mode == "mixed_inexact"))
             its, outer = st.inner_iterations, st.iterations
         e1.record(stream)
@@ -411,7 +412,7 @@ def run_solves(torch, stream, repeats=5):
     out["speedup_mixed_vs_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
     out["speedup_mixed_inexact_vs_fp64"] = out["fp64"]["ms"] / out["mixed_inexact"]["ms"]
     at_1e8 = {}
-    for mode in ("fp64", "mixed"):
+    for mode in ("fp64", "mixed_inexact"):
         ms, its, outer, x = one(mode, 1e-8)
         at_1e8[mode] = {"ms": ms, "iterations": its,
                         "rel_error_vs_fp64_1e-12": torch.linalg.norm(x - xr).item() / nr}

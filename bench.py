@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--case", default=None,
                     help="run one named case for profiling and exit: apply_<degree>_<cells>_<f64|f32>, "
                          "faces_<degree>_<cells>_<f64|f32>, supg_<degree>_<cells>_<f64|f32>, solid_<degree>_<cells>_<f64|f32>, "
+                         "vfield_<degree>_<cells>_<f64|f32>, "
                          "(e.g. apply_2_128_f32), solve (128^3 FE_Q(2) FP64 vs mixed CG), cg_f64 / cg_f32 / cg_f64_3pass "
                          "(one CG solve), advection, adjoint")
     return ap.parse_args()
@@ -98,6 +99,37 @@ def run_case(name):
         e1.record(stream)
         torch.cuda.synchronize()
         print(json.dumps({"case": name, "us_per_inverse_diagonal": e0.elapsed_time(e1) / 10 * 1e3}), flush=True)
+    elif name.startswith("vfield_"):
+        # advection-diffusion apply with the velocity as a DoF vector (the rotation of the advection
+        # benchmark sampled at the lattice points), without and with SUPG (tau_c = h_c / max |v|)
+        from meltpooldg_b200.inputs import lattice_coords
+        from meltpooldg_b200.operators import AdvectionDiffusionOperator
+
+        _, deg, cells, prec = name.split("_")
+        dt = torch.float64 if prec == "f64" else torch.float32
+        mesh = Mesh(int(deg), (int(cells),) * 3, dirichlet_faces=0b000011)
+        op = AdvectionDiffusionOperator(mesh, dt=5e-3, theta=1.0, diffusivity=1e-3, stream=stream.cuda_stream)
+        X, Y, Z = lattice_coords(mesh)
+        field = [torch.tensor(c, device="cuda") for c in (0.5 - Y, X - 0.5, 0.0 * Z)]
+        op.set_velocity_field(*field)
+        x = torch.tensor(uniform_dofs(mesh, seed=1), dtype=dt, device="cuda")
+        y = torch.empty_like(x)
+        out = {"case": name, "dofs": mesh.ndofs}
+        for tag in ("field", "field_supg"):
+            if tag == "field_supg":
+                op.set_convection_stabilization("SUPG", -1.0)
+            for _ in range(3):
+                op.vmult(y, x)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(10):
+                op.vmult(y, x)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            us = e0.elapsed_time(e1) / 10 * 1e3
+            out[tag] = {"us_per_apply": us, "gdofs": mesh.ndofs / us / 1e3}
+        print(json.dumps(out), flush=True)
     elif name.startswith("faces_") or name.startswith("supg_") or name.startswith("solid_"):
         # one apply with and without the extra terms: heat with convection (x faces) and radiation
         # (y, z faces); advection-diffusion with SUPG (tau_c = h_c / max |v|)

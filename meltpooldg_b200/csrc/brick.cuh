@@ -394,8 +394,9 @@ namespace mpdg
       }
   }
 
-  // Stage the brick's lattice points of src into shared memory (row walk, cp.async).
-  template <class BR, typename T>
+  // Stage the brick's lattice points of src into shared memory (row walk, cp.async).  WAIT = false
+  // only issues the copies (a later staging call with WAIT waits for all of the thread's copies).
+  template <class BR, typename T, bool WAIT = true>
   __device__ __forceinline__ void
   brick_stage(const BR &br, const T *src, bool mask_src, T *s_src)
   {
@@ -418,8 +419,11 @@ namespace mpdg
           valid = false;
         cp_async_elem(s_src + row * BR::PX + px, src + idx, valid);
       }
-    cp_async_wait_all();
-    __syncthreads();
+    if constexpr (WAIT)
+      {
+        cp_async_wait_all();
+        __syncthreads();
+      }
   }
 
   // Write the brick's accumulated values: plain stores for brick-interior points, atomics on points
